@@ -1,0 +1,303 @@
+"""Benchmark of the B200 join-order DP (MPDP on the 25-relation snowflake).
+
+One step = one MPDP optimisation (gpuqo_algorithm=dpsub, gpuqo_dpsub_bicc=on)
+of one seeded synthetic 25-relation snowflake query per rank.  Multi-GPU runs
+are weak-scaled query sharding: every rank optimises its own queries, no
+collective on the data path; the barrier and the max-over-ranks timing are
+the only collectives.
+
+Printed (rank 0, one JSON line):
+  value  - ms per query of the device-resident DP: the planner info is on the
+           device, the captured DP graph is replayed, CUDA events on the
+           library's stream, L2 flushed (256 MB write) before every step;
+  e2e    - ms per query through the C ABI gpuqo_run with host structures
+           (conversion, H2D of the planner info, the DP, D2H of the plan);
+  roofline - the evaluate kernel (k_eval): algorithmic memo bytes per launch
+           (32 B per evaluated csg-cmp pair: two 16 B memo reads; 20 B per
+           connected set written) over its event-timed launch duration,
+           against the measured HBM copy bandwidth;
+  cpu_baseline - the reference's parallel_cpu_dpsub_bicc (its own code,
+           compiled from its sources into oracle/_ref) on the host cores.
+
+--impl reference times that reference CPU engine alone (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "postgres-gpuqo_b200"))
+
+METRIC = "MPDP ms/query @25-rel snowflake; batched queries/s vs plain GPU; p50/p99"
+WORKLOAD = ("MPDP (gpuqo_algorithm=dpsub, gpuqo_dpsub_bicc=on) of one 25-relation snowflake "
+            "query per step: root with 4-6 children, 0-3 children per node, depth <= 4, rows "
+            "log-uniform [1e2,1e8], FK-PK selectivity 1/rows(PK side), dense memo 2^25")
+N_RELS = 25
+SEEDS = [0, 1, 2, 3]
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per k_eval launch from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "k_eval_mpdp_snowflake25.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_sample(queries, steps=None, budget_s=20.0):
+    """The reference's parallel_cpu_dpsub_bicc on the host cores (bounded)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import harness
+    from gpuqo_b200 import capi
+    cores = os.cpu_count() or 1
+    harness.run_ref(queries[0], capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)  # warm-up
+    times = []
+    t_start = time.perf_counter()
+    i = 0
+    while True:
+        q = queries[i % len(queries)]
+        _, dt = harness.run_ref(q, capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)
+        times.append(dt * 1000.0)
+        i += 1
+        if steps is not None and i >= steps:
+            break
+        if steps is None and (time.perf_counter() - t_start > budget_s or i >= 40):
+            break
+    return statistics.mean(times), cores, len(times)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local_rank = dist_env()
+
+    from gpuqo_b200 import capi, query
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        qs = [query.snowflake(N_RELS, s) for s in SEEDS]
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import harness
+        cores = os.cpu_count() or 1
+        for i in range(args.warmup):
+            harness.run_ref(qs[i % len(qs)], capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)
+        times = []
+        for i in range(args.steps):
+            _, dt = harness.run_ref(qs[i % len(qs)], capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)
+            times.append(dt * 1000.0)
+        v = statistics.mean(times)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/query", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "seeds": SEEDS, "engine": "parallel_cpu_dpsub_bicc",
+                           "chunk": 256},
+                "cpu_baseline": {"value": v, "unit": "ms/query", "cores": cores, "kind": "reference",
+                                 "sample": f"{args.steps} snowflake-25 queries, gpuqo_dpe_n_threads={cores}"},
+                "e2e": {"value": v, "unit": "ms/query", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    from gpuqo_b200 import lib
+    lib.load()
+    qs = [query.snowflake(N_RELS, s + 1000 * rank) for s in SEEDS]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also captures the DP graph)
+    for i in range(args.warmup):
+        rc, _, _, _ = lib.time_resident(qs[i % len(qs)], capi.GPUQO_DPSUB, bicc=True, warmup=0, iters=1)
+        if rc:
+            raise RuntimeError(f"gpuqo_b200_time_resident failed: {rc}")
+
+    # ---- timed region: device-resident DP ----
+    tot_ms = 0.0
+    eval_ms = 0.0
+    eval_launches = 0
+    kernels = 0
+    pairs = 0
+    csgs = 0
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            rc, ms, tree, st = lib.time_resident(qs[i % len(qs)], capi.GPUQO_DPSUB, bicc=True,
+                                                 warmup=0, iters=1, flush_l2=True)
+            if rc or tree is None:
+                raise RuntimeError(f"gpuqo_b200_time_resident failed: {rc}")
+            tot_ms += ms
+            eval_ms += st["eval_kernel_ms"]
+            eval_launches += st["eval_kernel_launches"]
+            kernels += st["kernel_launches"]
+            pairs += st["evaluated_pairs"]
+            csgs += st["connected_sets"]
+    barrier()
+    max_ms = tot_ms
+    if dist is not None:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        max_ms = float(t.item())
+    value = max_ms / (args.steps * world)
+
+    # ---- e2e: the C ABI with host structures ----
+    for i in range(args.warmup):
+        lib.run(qs[i % len(qs)], capi.GPUQO_DPSUB, bicc=True)
+    barrier()
+    e2e_ms = 0.0
+    for i in range(args.steps):
+        r = lib.run(qs[i % len(qs)], capi.GPUQO_DPSUB, bicc=True)
+        if r.error or r.tree is None:
+            raise RuntimeError(f"gpuqo_run failed: {r.error}")
+        e2e_ms += r.seconds * 1000.0
+    barrier()
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = e2e_ms / (args.steps * world)
+    # bytes crossing the bus per step: the planner-info blob (header 208 words,
+    # 2 words per class, selectivities, 8 words per class member; staged in
+    # 512-word buckets) in; plan nodes + tree size + counters out
+    q0 = qs[0]
+    n_ec = len(q0.eq_classes)
+    n_sels = sum(len(e.sels) for e in q0.eq_classes)
+    n_fks = sum(len(e.members) for e in q0.eq_classes)
+    h2d = 4 * ((208 + 2 * n_ec + n_sels + 8 * n_fks + 511) // 512 * 512)
+    d2h = 64 * 28 + 4 + 8 + 33 * 16
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        alg_bytes = pairs * 32 + csgs * 20
+        per_launch_bytes = alg_bytes / max(1, eval_launches)
+        per_launch_s = (eval_ms / 1000.0) / max(1, eval_launches)
+        achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+        traffic = profiled_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": "ms/query", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "b200",
+            "config": {"workload": WORKLOAD, "seeds": SEEDS, "queries_per_step_per_gpu": 1,
+                       "l2": "flushed before every step (256 MB write)", "parallelism": f"query-sharded x{world}"},
+            "evaluated_pairs_per_step": pairs / args.steps,
+            "connected_sets_per_step": csgs / args.steps,
+            "pairs_per_s": pairs / (tot_ms / 1000.0) if tot_ms > 0 else None,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_eval<MPDP>", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None},
+            "e2e": {"value": e2e_value, "unit": "ms/query", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": kernels,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cv, cores, ns = cpu_reference_sample(qs)
+            line["cpu_baseline"] = {"value": cv, "unit": "ms/query", "cores": cores, "kind": "reference",
+                                    "sample": f"{ns} snowflake-25 queries, parallel_cpu_dpsub_bicc, "
+                                              f"{cores} threads, chunk 256"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

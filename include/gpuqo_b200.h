@@ -1,0 +1,235 @@
+/*
+ * gpuqo_b200.h - C ABI of libgpuqo_b200.so, the B200 (sm_100a) join-order
+ * dynamic programming library (DPsub / MPDP, IDP2 / UnionDP on top).
+ *
+ * Drop-in boundary.  The library replaces the reference's gpuqo object set
+ * (the gpuqo_*.cu files under src/backend/optimizer/gpuqo, linked into postgres per
+ * src/backend/Makefile:55-59) behind the same entry point and the same GUC
+ * variables; the planner glue gpuqo_main.c (the caller) is unchanged.
+ *
+ * Struct layouts are the reference's, byte for byte, so a backend compiled
+ * against src/include/optimizer/gpuqo_planner_info.h can call this library.
+ * When those headers are already included, the declarations below are skipped.
+ */
+#ifndef GPUQO_B200_H
+#define GPUQO_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Reference ABI types                                                     */
+/* ---------------------------------------------------------------------- */
+#if !defined(GPUQO_PLANNER_INFO_H) && !defined(GPUQO_COMMON_H)
+
+/* Postgres nodes/bitmapset.h; re-declared by the reference in
+ * src/backend/optimizer/gpuqo/gpuqo_postgres.cuh:29-33 */
+#ifndef BITMAPSET_H
+typedef uint64_t bitmapword;
+typedef struct Bitmapset {
+    int nwords;
+    bitmapword words[];
+} Bitmapset;
+#endif
+
+/* src/include/optimizer/gpuqo_common.h:13-29 */
+typedef enum GpuqoAlgorithm {
+    GPUQO_DPSIZE = 0,
+    GPUQO_DPSUB,
+    GPUQO_CPU_DPSIZE,
+    GPUQO_CPU_DPSUB,
+    GPUQO_CPU_DPSUB_PARALLEL,
+    GPUQO_CPU_DPSUB_BICC,
+    GPUQO_CPU_DPSUB_BICC_PARALLEL,
+    GPUQO_CPU_DPCCP,
+    GPUQO_DPE_DPSIZE,
+    GPUQO_DPE_DPSUB,
+    GPUQO_DPE_DPCCP,
+    GPUQO_CPU_GOO,
+    GPUQO_CPU_IKKBZ,
+    GPUQO_CPU_LINEARIZED_DP,
+    GPUQO_CPU_DPLIN
+} GpuqoAlgorithm;
+
+/* gpuqo_common.h:31-36 */
+typedef enum GpuqoIDPType {
+    GPUQO_IDP1 = 0,
+    GPUQO_IDP2,
+    GPUQO_UNION
+} GpuqoIDPType;
+
+/* gpuqo_common.h:92-120 */
+typedef struct PathCost { float startup; float total; } PathCost;
+typedef struct GpuqoIndexInfo { bool available; bool unique; float rows; PathCost cost; } GpuqoIndexInfo;
+typedef struct VarStats { float stadistinct; float stanullfrac; float mcvfreq; } VarStats;
+typedef struct VarInfo { VarStats stats; GpuqoIndexInfo index; } VarInfo;
+
+/* src/include/optimizer/gpuqo_planner_info.h:158-198 */
+typedef Bitmapset *EdgeMask;
+typedef Bitmapset *RelationID;
+
+typedef struct EqClassInfo {
+    void *eclass;                 /* EquivalenceClass*, unused here */
+    RelationID relids;
+    float *sels;                  /* size*(size-1)/2, eqClassIndex order */
+    VarInfo *vars;                /* one per member */
+    RelationID *fk;               /* one per member, may be NULL */
+    struct EqClassInfo *next;
+} EqClassInfo;
+
+typedef struct BaseRelationC {
+    RelationID id;
+    float rows;
+    float tuples;
+    PathCost cost;
+    int width;
+} BaseRelationC;
+
+typedef struct GpuqoPlannerInfoC {
+    int n_rels;
+    BaseRelationC *base_rels;
+    EdgeMask *edge_table;
+    EqClassInfo *eq_classes;
+    int n_eq_classes;
+    int n_eq_class_sels;
+    int n_eq_class_fks;
+    int n_eq_class_vars;
+} GpuqoPlannerInfoC;
+
+typedef struct QueryTreeC {
+    RelationID id;
+    float rows;
+    PathCost cost;
+    int width;
+    struct QueryTreeC *left;
+    struct QueryTreeC *right;
+} QueryTreeC;
+
+#endif /* reference headers not included */
+
+/* ---------------------------------------------------------------------- */
+/* Entry point                                                             */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * Replaces: extern "C" QueryTreeC *gpuqo_run(int, GpuqoPlannerInfoC*)
+ *   src/include/optimizer/gpuqo.h:139, impl src/backend/optimizer/gpuqo/
+ *   gpuqo_main_internal.cu:177-185; caller gpuqo_main.c:584.
+ *
+ * gpuqo_algorithm: GPUQO_DPSUB runs the GPU DP - MPDP (biconnected-block
+ *   csg-cmp enumeration) when gpuqo_dpsub_bicc_enable is set, plain DPsub
+ *   (all-subsets enumeration with CCC) otherwise.  The CPU algorithm codes
+ *   (GPUQO_CPU_DPSUB, GPUQO_CPU_DPSUB_BICC and their parallel/DPE variants)
+ *   return the same plans as the reference's CPU engines; they are served by
+ *   the same GPU kernels (plain DPsub for *_DPSUB, MPDP for *_BICC*).
+ *   Other codes (DPsize, DPccp, heuristics) are outside this library's
+ *   scope and return NULL with a message, as the reference does for
+ *   unsupported combinations (gpuqo_main_internal.cu:75-78).
+ * IDP: when 1 < gpuqo_idp_n_iters < n_rels, gpuqo_idp_type selects IDP2
+ *   (gpuqo_idp.cu:260) or UnionDP (gpuqo_dpdp_union.cu:448) over the GPU DP.
+ *
+ * The input is borrowed.  The returned tree and every id Bitmapset are
+ * palloc'd (inside Postgres: the caller's memory context; standalone: the
+ * library's malloc-based palloc).  Returns NULL on error, after printing a
+ * message to stderr; gpuqo_b200_last_error() returns the code.
+ */
+QueryTreeC *gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC *info);
+
+/* ---------------------------------------------------------------------- */
+/* GUC variables (bound by address from guc.c; reference definition sites) */
+/* ---------------------------------------------------------------------- */
+extern int gpuqo_algorithm;                          /* gpuqo_main.c:43 */
+extern int gpuqo_scratchpad_size_mb;                 /* gpuqo_dpsize.cu:41 */
+extern int gpuqo_max_memo_size_mb;                   /* gpuqo_dpsize.cu:42 */
+extern int gpuqo_min_memo_size_mb;                   /* gpuqo_dpsize.cu:43 */
+extern int gpuqo_n_parallel;                         /* gpuqo_dpsub_common.cu:45 */
+extern bool gpuqo_dpsub_filter_enable;               /* gpuqo_dpsub_filtered.cu:44 */
+extern int gpuqo_dpsub_filter_threshold;             /* :45 */
+extern int gpuqo_dpsub_filter_cpu_enum_threshold;    /* :46 */
+extern int gpuqo_dpsub_filter_keys_overprovisioning; /* :47 */
+extern bool gpuqo_dpsub_ccc_enable;                  /* :50 */
+extern bool gpuqo_dpsub_csg_enable;                  /* :53 */
+extern int gpuqo_dpsub_csg_threshold;                /* :54 */
+extern bool gpuqo_dpsub_tree_enable;                 /* :57 */
+extern bool gpuqo_dpsub_bicc_enable;                 /* :60 */
+extern int gpuqo_dpe_n_threads;                      /* gpuqo_cpu_dpe.cu:33 */
+extern int gpuqo_dpe_pairs_per_depbuf;               /* gpuqo_cpu_dpe.cu:34 */
+extern int gpuqo_cpu_dpsub_parallel_chunk_size;      /* gpuqo_cpu_dpsub_parallel.cu:30 */
+extern bool gpuqo_spanning_tree_enable;              /* gpuqo_spanning_tree.cu:15 */
+extern int gpuqo_idp_n_iters;                        /* gpuqo_idp.cu:14 */
+extern int gpuqo_idp_type;                           /* gpuqo_idp.cu:15 */
+extern int gpuqo_dplin_csg_threshold_lindp;          /* gpuqo_cpu_dplin.cu:27 */
+extern int gpuqo_dplin_threshold_lindp;              /* gpuqo_cpu_dplin.cu:28 */
+extern int gpuqo_dplin_threshold_idp;                /* gpuqo_cpu_dplin.cu:29 */
+
+/* ---------------------------------------------------------------------- */
+/* Library extensions (no counterpart in the reference)                    */
+/* ---------------------------------------------------------------------- */
+
+/* Status codes of the extension entry points. */
+enum {
+    GPUQO_B200_OK = 0,
+    GPUQO_B200_ERR_ARGS = 1,        /* bad arguments / unsupported input */
+    GPUQO_B200_ERR_CUDA = 2,        /* CUDA runtime error */
+    GPUQO_B200_ERR_NOMEM = 3,       /* device memory budget exceeded */
+    GPUQO_B200_ERR_TOO_LARGE = 4,   /* exact DP beyond the dense-memo limit */
+    GPUQO_B200_ERR_UNSUPPORTED = 5, /* algorithm outside this library */
+    GPUQO_B200_ERR_CANCELLED = 6    /* InterruptPending was set */
+};
+
+/* Code of the last failed call on this thread (GPUQO_B200_OK if none). */
+int gpuqo_b200_last_error(void);
+
+/* Frees a tree returned by gpuqo_run / the batch API with pfree. */
+void gpuqo_b200_free_query_tree(QueryTreeC *qt);
+
+/* Counters of the last exact-DP run (summed over IDP sub-problems). */
+typedef struct GpuqoB200Stats {
+    uint64_t connected_sets;      /* csgs evaluated (levels >= 2) */
+    uint64_t evaluated_pairs;     /* valid csg-cmp pairs costed */
+    uint64_t filtered_subsets;    /* candidate subsets unranked and tested */
+    uint64_t memo_bytes;          /* device memo footprint */
+    double   device_ms;           /* device time of the DP (CUDA events) */
+    double   eval_kernel_ms;      /* summed time of the evaluate kernels */
+    uint32_t eval_kernel_launches;
+    uint32_t n_subproblems;       /* exact DP runs (1, or IDP iterations) */
+    uint32_t kernel_launches;     /* kernels launched by the DP runs */
+    uint32_t reserved;
+} GpuqoB200Stats;
+void gpuqo_b200_get_stats(GpuqoB200Stats *out);
+
+/* When non-zero, per-kernel CUDA events are recorded around every evaluate
+ * launch (for the kernel-time figures in the stats); off by default. */
+extern int gpuqo_b200_profile_kernels;
+
+/*
+ * Device-resident timing of the exact DP of one query (< 32 relations, no
+ * IDP): the planner info is converted and uploaded once, then the captured DP
+ * graph is replayed warmup + iters times; CUDA events on the library's stream
+ * time each replay, with a 256 MB L2 flush between replays when flush_l2 is
+ * set.  *ms_per_iter receives the mean device milliseconds per replay and
+ * *tree (if non-NULL) the plan of the last replay.  Returns a status code.
+ */
+int gpuqo_b200_time_resident(int gpuqo_algorithm, GpuqoPlannerInfoC *info, int warmup, int iters,
+                             int flush_l2, double *ms_per_iter, QueryTreeC **tree);
+
+/*
+ * Batched exact DP: optimises n_queries independent queries (each < 32
+ * relations, no IDP) with one persistent launch sequence per relation count
+ * level, all queries' memos packed in one device arena.  Trees are written to
+ * out[i] (palloc'd, NULL on error).  Same plans as gpuqo_run per query.
+ * Returns a status code.
+ */
+int gpuqo_b200_run_batch(int gpuqo_algorithm, GpuqoPlannerInfoC **infos,
+                         int n_queries, QueryTreeC **out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUQO_B200_H */

@@ -864,3 +864,27 @@ QueryTreeC *gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC *info_c) {
     free_info(&info);
     return res;
 }
+
+/*
+ * Single join evaluation on the caller's (unrelabelled) planner info, for
+ * arithmetic-consistency checks of plans too large for a full oracle run:
+ * given the children's (rows, startup, total, width), returns the join's, as
+ * make_join_relation computes it (gpuqo_cpu_common.cuh:169-186).
+ * vals_in: [l_rows, l_startup, l_total, l_width, r_rows, r_startup, r_total,
+ * r_width]; vals_out: [rows, startup, total, width].
+ */
+void oracle_eval_join(GpuqoPlannerInfoC *info_c, uint64_t left_id, uint64_t right_id,
+                      const float *vals_in, float *vals_out) {
+    Info info;
+    convert_info(info_c, &info);
+    Rel l, r;
+    l.rows = vals_in[0]; l.cost.startup = vals_in[1]; l.cost.total = vals_in[2]; l.width = (int)vals_in[3];
+    r.rows = vals_in[4]; r.cost.startup = vals_in[5]; r.cost.total = vals_in[6]; r.width = (int)vals_in[7];
+    float rows = estimate_join_rows(&info, left_id, &l, right_id, &r);
+    PathCost c = calc_join_cost(&info, left_id, &l, right_id, &r, rows);
+    vals_out[0] = rows;
+    vals_out[1] = c.startup;
+    vals_out[2] = c.total;
+    vals_out[3] = (float)(l.width + r.width);
+    free_info(&info);
+}

@@ -71,4 +71,9 @@ typedef struct QueryTreeC {
 QueryTreeC *gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC *info);
 void oracle_free_query_tree(QueryTreeC *qt);
 
+
+/* One make_join_relation evaluation on the caller's (unrelabelled) info. */
+void oracle_eval_join(GpuqoPlannerInfoC *info, uint64_t left_id, uint64_t right_id,
+                      const float *vals_in, float *vals_out);
+
 #endif

@@ -123,3 +123,17 @@ def run_port(q: Query, algorithm: int, idp_n_iters: int = 0,
     tree = capi.tree_to_py(res)
     lib.oracle_free_query_tree(C.cast(res, C.c_void_p))
     return tree, dt
+
+
+def eval_join(q: Query, left_id: int, right_id: int, lvals, rvals):
+    """Oracle join evaluation (rows, startup, total, width) of one join."""
+    lib = load_port()
+    f = lib.oracle_eval_join
+    f.argtypes = [C.POINTER(capi.GpuqoPlannerInfoC), C.c_uint64, C.c_uint64,
+                  C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    f.restype = None
+    b = capi.PlannerInfoBuilder(q)
+    vin = (C.c_float * 8)(*(list(lvals) + list(rvals)))
+    vout = (C.c_float * 4)()
+    f(b.pointer(), left_id, right_id, vin, vout)
+    return tuple(vout)

@@ -1,0 +1,469 @@
+// dp_device.cuh - device-side data layout and per-pair arithmetic of the
+// B200 join-order DP (DPsub / MPDP).
+//
+// Relation sets on the device use COMPACT masks: bit i = relation i after the
+// BFS relabelling (the reference's Postgres-style masks use bit i+1; the shift
+// preserves every order the algorithm depends on: lowest bit, pdep order,
+// integer order of subsets).
+//
+// Floating point follows the reference's cost model operation by operation
+// (src/backend/optimizer/gpuqo/gpuqo_cost.cuh, gpuqo_cost_postgres.cuh,
+// gpuqo_row_estimation.cuh).  This file must be compiled with -fmad=false:
+// the reference's CPU engines never fuse a multiply with an add.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dp_layout.h"
+
+namespace gqb {
+
+// ---------------------------------------------------------------------------
+// bit helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lowest(uint32_t x) { return x & (0u - x); }
+__device__ __forceinline__ int lowest_idx(uint32_t x) { return __ffs(x) - 1; }
+__device__ __forceinline__ int popc(uint32_t x) { return __popc(x); }
+
+// gpuqo_bitmapset.cuh:302-305: next subset of `set` after `sub` (pdep order)
+__device__ __forceinline__ uint32_t next_subset(uint32_t sub, uint32_t set) { return set & (sub - set); }
+
+// deposit the low bits of `val` into the set bits of `mask`
+__device__ __forceinline__ uint32_t pdep32(uint32_t val, uint32_t mask) {
+    uint32_t r = 0;
+    while (mask && val) {
+        uint32_t low = mask & (0u - mask);
+        if (val & 1u) r |= low;
+        val >>= 1;
+        mask ^= low;
+    }
+    return r;
+}
+
+// gpuqo_filter.cuh:119-147: closure of `from` inside `subset`
+__device__ __forceinline__ uint32_t grow(uint32_t from, uint32_t subset, const uint32_t *adj) {
+    uint32_t V = 0, N = from;
+    while (N) {
+        int i = __ffs(N) - 1;
+        V |= 1u << i;
+        N = (N | adj[i]) & subset & ~V;
+    }
+    return V;
+}
+
+// gpuqo_filter.cuh:149-160
+__device__ __forceinline__ bool is_connected(uint32_t s, const uint32_t *adj) {
+    if (!s) return false;
+    return grow(lowest(s), s, adj) == s;
+}
+
+// float -> int as the reference's x86-64 host build converts it
+// (cvttss2si: truncation, INT_MIN when out of range or NaN).  The device's
+// own conversion saturates instead, so it is emulated.
+__device__ __forceinline__ int f2i_x86(float f) {
+    if (!(f > -2147483649.0f && f < 2147483648.0f)) return (int)0x80000000;
+    return __float2int_rz(f);
+}
+
+__device__ __forceinline__ int ceil_log2_l(long long num) {
+    int res = 63 - __clzll(num);
+    if ((1LL << res) == num) return res;
+    return res + 1;
+}
+
+// order-preserving map of a float to uint32 (NaN handled by the caller);
+// -0.0 is folded to +0.0 because the reference compares with '<'
+__device__ __forceinline__ uint32_t ord_float(float f) {
+    if (f == 0.0f) f = 0.0f;
+    uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// ---------------------------------------------------------------------------
+// cost model pieces (gpuqo_cost_postgres.cuh)
+// ---------------------------------------------------------------------------
+struct RelVal {
+    float rows, startup, total;
+    int width;
+};
+
+__device__ __forceinline__ RelVal load_rel(const float4 *memo, uint32_t s) {
+    float4 v = __ldcg(memo + s);
+    RelVal r;
+    r.rows = v.x;
+    r.startup = v.y;
+    r.total = v.z;
+    r.width = __float_as_int(v.w);
+    return r;
+}
+
+// :850-862
+__device__ __forceinline__ float clamp_row_est(float nrows) {
+    return nrows <= 1.0f ? 1.0f : rintf(nrows);
+}
+
+// :820-841 (MAXALIGN with MAXIMUM_ALIGNOF 8, RELATION_OVERHEAD 24, BLCKSZ 8192)
+__device__ __forceinline__ float relation_byte_size(float tuples, int width) {
+    unsigned long long a = ((unsigned long long)(long long)width + 7ull) & ~7ull;
+    return tuples * (float)(a + 24ull);
+}
+__device__ __forceinline__ float page_size(float tuples, int width) {
+    return ceilf(relation_byte_size(tuples, width) / 8192.0f);
+}
+
+struct Htsz {
+    int numbuckets, numbatches;
+};
+
+// :480-621 ExecChooseHashTableSize
+__device__ __forceinline__ Htsz exec_choose_hash_table_size(float ntuples, int tupwidth, int work_mem) {
+    Htsz res;
+    res.numbatches = 1;
+    if (ntuples <= 0.0f) ntuples = 1000.0f;
+    int tupsize = 32 + (int)(((unsigned long long)(long long)tupwidth + 7ull) & ~7ull);
+    float inner_rel_bytes = ntuples * (float)tupsize;
+    long long hash_table_bytes = (long long)work_mem * 1024LL;
+    float space_allowed = (float)hash_table_bytes;
+    long long skew_table_bytes = hash_table_bytes * 2 / 100;
+    long long num_skew_mcvs = skew_table_bytes / (tupsize + 84);
+    if (num_skew_mcvs > 0) hash_table_bytes -= skew_table_bytes;
+    long long max_pointers = (long long)(space_allowed / 8.0f);
+    {
+        unsigned long long a = (unsigned long long)max_pointers, b = 0x3fffffffULL / 8ULL;
+        max_pointers = (long long)(a < b ? a : b);
+    }
+    long long mppow2 = 1LL << ceil_log2_l(max_pointers);
+    if (max_pointers != mppow2) max_pointers = mppow2 / 2;
+    if (max_pointers > (long long)(2147483647 / 2)) max_pointers = 2147483647 / 2;
+    float dbuckets = ceilf(ntuples / 1.0f);
+    dbuckets = fminf(dbuckets, (float)max_pointers);
+    res.numbuckets = (int)dbuckets;
+    if (res.numbuckets < 1024) res.numbuckets = 1024;
+    res.numbuckets = 1 << ceil_log2_l(res.numbuckets);
+    long long bucket_bytes = 8LL * res.numbuckets;
+    if (inner_rel_bytes + (float)bucket_bytes > (float)hash_table_bytes) {
+        long long bucket_size = (long long)tupsize + 8LL;
+        long long lbuckets = 1LL << ceil_log2_l(hash_table_bytes / bucket_size);
+        if (lbuckets > max_pointers) lbuckets = max_pointers;
+        res.numbuckets = (int)lbuckets;
+        res.numbuckets = 1 << ceil_log2_l(res.numbuckets);
+        bucket_bytes = 8LL * res.numbuckets;
+        float dbatch = ceilf(inner_rel_bytes / (float)(hash_table_bytes - bucket_bytes));
+        dbatch = fminf(dbatch, (float)max_pointers);
+        int minbatch = (int)dbatch;
+        int p2 = 1 << ceil_log2_l(minbatch);
+        res.numbatches = p2 > 2 ? p2 : 2;
+    }
+    return res;
+}
+
+// :705-787 __estimate_hash_bucketsize
+__device__ __forceinline__ float bucketsize_one(const DevVar &v, float rel_rows, float rel_tuples, int nbuckets) {
+    float estfract, ndistinct, mcvfreq, avgfreq;
+    ndistinct = v.stadistinct;
+    if (ndistinct < 0.0f) ndistinct = -ndistinct * rel_tuples;
+    if (ndistinct <= 0.0f) return 0.1f;
+    avgfreq = (1.0f - v.stanullfrac) / ndistinct;
+    if (rel_tuples > 0.0f) {
+        ndistinct *= rel_rows / rel_tuples;
+        ndistinct = clamp_row_est(ndistinct);
+    }
+    if (ndistinct > (float)nbuckets) estfract = 1.0f / (float)nbuckets;
+    else estfract = 1.0f / ndistinct;
+    mcvfreq = v.mcvfreq;
+    if (avgfreq > 0.0f && mcvfreq > avgfreq) estfract *= mcvfreq / avgfreq;
+    if (estfract < 1.0e-6f) estfract = 1.0e-6f;
+    else if (estfract > 1.0f) estfract = 1.0f;
+    return estfract;
+}
+
+struct Extra {
+    bool inner_unique;
+    bool indexed_join_quals;
+    float joinrows, outer_match_frac, match_count;
+};
+
+// :114-279 cost_nestloop; (n_quals, per_tuple) is cost_qual_eval(inner, outer)
+__device__ __forceinline__ void cost_nestloop(const DevHeader &h, const RelVal &outer, float inner_rows,
+                                              float inner_startup, float inner_total, const Extra &extra,
+                                              float qual_per_tuple, float &out_startup, float &out_total) {
+    float startup_cost = 0.0f, run_cost = 0.0f;
+    float outer_path_rows = outer.rows, inner_path_rows = inner_rows, ntuples;
+    if (!h.enable_nestloop) startup_cost += h.disable_cost;
+    startup_cost += inner_startup + outer.startup;
+    run_cost += outer.total - outer.startup;
+    if (outer_path_rows > 1.0f) run_cost += (outer_path_rows - 1.0f) * inner_startup;
+    float inner_run_cost = inner_total - inner_startup;
+    float inner_rescan_run_cost = inner_run_cost;
+    if (extra.inner_unique) {
+        float outer_matched_rows = rintf(outer_path_rows * extra.outer_match_frac);
+        float outer_unmatched_rows = outer_path_rows - outer_matched_rows;
+        float inner_scan_frac = 2.0f / (extra.match_count + 1.0f);
+        ntuples = outer_matched_rows * inner_path_rows * inner_scan_frac;
+        if (extra.indexed_join_quals) {
+            run_cost += inner_run_cost * inner_scan_frac;
+            if (outer_matched_rows > 1.0f)
+                run_cost += (outer_matched_rows - 1.0f) * inner_rescan_run_cost * inner_scan_frac;
+            run_cost += outer_unmatched_rows * inner_rescan_run_cost / inner_path_rows;
+        } else {
+            ntuples += outer_unmatched_rows * inner_path_rows;
+            run_cost += inner_run_cost;
+            if (outer_unmatched_rows >= 1.0f) outer_unmatched_rows -= 1.0f;
+            else outer_matched_rows -= 1.0f;
+            if (outer_matched_rows > 0.0f) run_cost += outer_matched_rows * inner_rescan_run_cost * inner_scan_frac;
+            if (outer_unmatched_rows > 0.0f) run_cost += outer_unmatched_rows * inner_rescan_run_cost;
+        }
+    } else {
+        run_cost += inner_run_cost;
+        if (outer_path_rows > 1.0f) run_cost += (outer_path_rows - 1.0f) * inner_rescan_run_cost;
+        ntuples = outer_path_rows * inner_path_rows;
+    }
+    startup_cost += 0.0f;  // cost_qual_eval startup is always 0
+    float cpu_per_tuple = h.cpu_tuple_cost + qual_per_tuple;
+    run_cost += cpu_per_tuple * ntuples;
+    out_startup = startup_cost;
+    out_total = startup_cost + run_cost;
+}
+
+// :291-468 cost_hashjoin
+__device__ __forceinline__ void cost_hashjoin(const DevHeader &h, const RelVal &outer, const RelVal &inner,
+                                              const Extra &extra, int n_quals, float qual_per_tuple,
+                                              const Htsz &hz, float bs_bucketsize, float bs_mcvfreq,
+                                              float &out_startup, float &out_total) {
+    float startup_cost = 0.0f, run_cost = 0.0f, hashjointuples;
+    float outer_path_rows = outer.rows, inner_path_rows = inner.rows;
+    if (!h.enable_hashjoin) startup_cost += h.disable_cost;
+    startup_cost += outer.startup;
+    run_cost += outer.total - outer.startup;
+    startup_cost += inner.total;
+    startup_cost += (h.cpu_operator_cost * (float)n_quals + h.cpu_tuple_cost) * inner_path_rows;
+    run_cost += h.cpu_operator_cost * (float)n_quals * outer_path_rows;
+    if (hz.numbatches > 1) {
+        float outerpages = page_size(outer_path_rows, outer.width);
+        float innerpages = page_size(inner_path_rows, inner.width);
+        startup_cost += h.seq_page_cost * innerpages;
+        run_cost += h.seq_page_cost * (innerpages + 2.0f * outerpages);
+    }
+    float virtualbuckets = (float)hz.numbuckets * (float)hz.numbatches;
+    (void)virtualbuckets;
+    if (relation_byte_size(clamp_row_est(inner_path_rows * bs_mcvfreq), inner.width) >
+        (float)((long long)h.work_mem * 1024LL))
+        startup_cost += h.disable_cost;
+    if (extra.inner_unique) {
+        float outer_matched_rows = rintf(outer_path_rows * extra.outer_match_frac);
+        float inner_scan_frac = 2.0f / (extra.match_count + 1.0f);
+        startup_cost += 0.0f;
+        run_cost += qual_per_tuple * outer_matched_rows *
+                    clamp_row_est(inner_path_rows * bs_bucketsize * inner_scan_frac) * 0.5f;
+        run_cost += qual_per_tuple * (outer_path_rows - outer_matched_rows) *
+                    clamp_row_est(inner_path_rows / virtualbuckets) * 0.05f;
+        hashjointuples = outer_matched_rows;
+    } else {
+        startup_cost += 0.0f;
+        run_cost += qual_per_tuple * outer_path_rows * clamp_row_est(inner_path_rows * bs_bucketsize) * 0.5f;
+        hashjointuples = extra.joinrows;
+    }
+    run_cost += h.cpu_tuple_cost * hashjointuples;
+    out_startup = startup_cost;
+    out_total = startup_cost + run_cost;
+}
+
+// gpuqo_row_estimation.cuh:26-45 fkselc_of_ec; returns NaN when no FK applies
+__device__ __forceinline__ float fkselc_of_ec(const DevInfoView &d, int off_fk, uint32_t ec, uint32_t outer_rels,
+                                              uint32_t inner_rels) {
+    uint32_t tmp = outer_rels;
+    while (tmp) {
+        uint32_t out_id = lowest(tmp);
+        int out_idx = popc((out_id - 1u) & ec);
+        uint32_t match = inner_rels & d.fks[off_fk + out_idx];
+        if (match) {
+            int in_idx = lowest_idx(match);
+            return (float)(1.0 / (double)fmaxf(1.0f, d.h->tuples[in_idx]));
+        }
+        tmp &= ~out_id;
+    }
+    return __int_as_float(0x7fffffff);
+}
+
+// gpuqo_row_estimation.cuh:49-88 (for a class that matches both sides)
+__device__ __forceinline__ float ec_selectivity(const DevInfoView &d, int i, uint32_t ec, uint32_t ml, uint32_t mr) {
+    uint32_t off = d.ec_off[i];
+    int off_sels = (int)(off >> 16), off_fks = (int)(off & 0xFFFFu);
+    float fk = fkselc_of_ec(d, off_fks, ec, ml, mr);
+    if (!isnan(fk)) return fk;
+    fk = fkselc_of_ec(d, off_fks, ec, mr, ml);
+    if (!isnan(fk)) return fk;
+    int size = popc(ec);
+    int il = popc((lowest(ml) - 1u) & ec);
+    int ir = popc((lowest(mr) - 1u) & ec);
+    if (il > ir) { int t = il; il = ir; ir = t; }
+    int idx = il * size - il * (il + 1) / 2 + (ir - il - 1);
+    return d.sels[off_sels + idx];
+}
+
+// ---------------------------------------------------------------------------
+// One join evaluation: estimate_join_rows + calc_join_cost + width
+// (gpuqo_cpu_common.cuh:169-186 make_join_relation; gpuqo_cost.cuh:81-157).
+// All per-equivalence-class passes of the reference (selectivity product,
+// cost_qual_eval, is_inner_unique, estimate_hash_bucket_stats) are fused into
+// one pass; each quantity is accumulated in the reference's class order, so
+// every float result is the reference's.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
+                                            const RelVal &r) {
+    const DevHeader &h = *d.h;
+    const bool inner_single = (R & (R - 1u)) == 0u;
+    // the hash table size depends on the inner side only; needed by the
+    // bucket-size estimate inside the class loop
+    Htsz hz = exec_choose_hash_table_size(r.rows, r.width, h.work_mem);
+    int nbuckets = f2i_x86((float)hz.numbuckets * (float)hz.numbatches);
+
+    float sel = 1.0f;
+    int n_quals = 0;
+    float per_tuple = 0.0f;
+    bool inner_unique = false, any_index = false;
+    float bucketsize = 1.0f, mcvfreq = 1.0f;
+    const int n_ec = h.n_ec;
+    for (int i = 0; i < n_ec; i++) {
+        uint32_t ec = d.ec_relids[i];
+        uint32_t ml = ec & L, mr = ec & R;
+        if (!ml || !mr) continue;
+        sel *= ec_selectivity(d, i, ec, ml, mr);
+        per_tuple += h.cpu_operator_cost;
+        n_quals++;
+        int off_fks = (int)(d.ec_off[i] & 0xFFFFu);
+        uint32_t m = mr;
+        bool first = true;
+        while (m) {
+            uint32_t in_id = lowest(m);
+            int in_idx = popc((in_id - 1u) & ec);
+            const DevVar v = d.vars[off_fks + in_idx];
+            if (first && inner_single) {
+                if ((v.flags & 1u) && (v.flags & 2u)) inner_unique = true;
+                if (v.flags & 1u) any_index = true;
+            }
+            first = false;
+            int rel = lowest_idx(in_id);
+            float this_bs = bucketsize_one(v, h.rows[rel], h.tuples[rel], nbuckets);
+            if (bucketsize > this_bs) bucketsize = this_bs;
+            if (mcvfreq > v.mcvfreq) mcvfreq = v.mcvfreq;
+            m &= ~in_id;
+        }
+    }
+
+    RelVal out;
+    float rows = sel * l.rows * r.rows;
+    out.rows = rows > 1.0f ? roundf(rows) : 1.0f;
+    out.width = l.width + r.width;
+
+    Extra extra;
+    extra.inner_unique = inner_unique;
+    extra.indexed_join_quals = false;
+    extra.joinrows = out.rows;
+    extra.outer_match_frac = out.rows / (l.rows * r.rows);
+    extra.match_count = r.rows;
+
+    float min_s, min_t, s, t;
+    cost_nestloop(h, l, r.rows, r.startup, r.total, extra, per_tuple, min_s, min_t);
+    if (h.enable_hashjoin) {
+        cost_hashjoin(h, l, r, extra, n_quals, per_tuple, hz, bucketsize, mcvfreq, s, t);
+        if (t < min_t) { min_s = s; min_t = t; }
+    }
+    if (any_index && !((h.composite_mask >> lowest_idx(R)) & 1u)) {
+        extra.indexed_join_quals = true;
+        for (int i = 0; i < n_ec; i++) {
+            uint32_t ec = d.ec_relids[i];
+            uint32_t ml = ec & L, mr = ec & R;
+            if (!ml || !mr) continue;
+            int off_fks = (int)(d.ec_off[i] & 0xFFFFu);
+            int in_idx = popc((lowest(mr) - 1u) & ec);
+            const DevVar v = d.vars[off_fks + in_idx];
+            if (!(v.flags & 1u)) continue;
+            cost_nestloop(h, l, v.idx_rows, v.idx_startup, v.idx_total, extra, per_tuple, s, t);
+            if (t < min_t) { min_s = s; min_t = t; }
+        }
+    }
+    out.startup = min_s;
+    out.total = min_t;
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// Biconnected blocks of a connected set, in the output order of the
+// reference's iterative Hopcroft-Tarjan (gpuqo_cpu_dpsub_bicc.cu:65-170):
+// DFS from the lowest relation, neighbours in increasing index order, a block
+// emitted when returning from child v to u with low[v] >= disc[u].  A vertex
+// stack replaces the reference's edge stack; both yield the same vertex sets
+// in the same order.  Returns the number of blocks; prefix[b] = number of
+// candidate pairs in blocks < b (each block b contributes 2^|b| - 2).
+// ---------------------------------------------------------------------------
+struct Blocks {
+    int nb;
+    uint32_t total;               // sum of 2^|b| - 2
+    uint32_t mask[kMaxRels];
+    uint32_t prefix[kMaxRels + 1];
+};
+
+__device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blocks &B) {
+    uint8_t disc[kMaxRels], low[kMaxRels], parent[kMaxRels];
+    uint8_t stk_u[kMaxRels];
+    uint32_t stk_e[kMaxRels];
+    uint8_t vstk[kMaxRels];
+    int sp = 0, vsp = 0, t = 0;
+    uint32_t visited = 0;
+    B.nb = 0;
+    B.total = 0;
+    int root = lowest_idx(S);
+    visited |= 1u << root;
+    disc[root] = (uint8_t)t++;
+    low[root] = 255;
+    parent[root] = 255;
+    vstk[vsp++] = (uint8_t)root;
+    stk_u[sp] = (uint8_t)root;
+    stk_e[sp] = adj[root] & S;
+    sp++;
+    while (sp > 0) {
+        int u = stk_u[sp - 1];
+        uint32_t e = stk_e[sp - 1];
+        if (e == 0) {
+            sp--;
+            if (sp > 0) {
+                int p = stk_u[sp - 1];
+                if (low[u] >= disc[p]) {
+                    uint32_t blk = 1u << p;
+                    int w;
+                    do {
+                        w = vstk[--vsp];
+                        blk |= 1u << w;
+                    } while (w != u);
+                    B.prefix[B.nb] = B.total;
+                    B.mask[B.nb++] = blk;
+                    B.total += (1u << popc(blk)) - 2u;
+                }
+                if (low[u] < low[p]) low[p] = low[u];
+                stk_e[sp - 1] &= ~(1u << u);
+            }
+            continue;
+        }
+        int v = lowest_idx(e);
+        if (!((visited >> v) & 1u)) {
+            visited |= 1u << v;
+            parent[v] = (uint8_t)u;
+            disc[v] = (uint8_t)t++;
+            low[v] = 255;
+            vstk[vsp++] = (uint8_t)v;
+            stk_u[sp] = (uint8_t)v;
+            stk_e[sp] = adj[v] & S;
+            sp++;
+        } else {
+            if (parent[u] != v && disc[v] < disc[u]) {
+                if (disc[v] < low[u]) low[u] = disc[v];
+            }
+            stk_e[sp - 1] = e & ~(1u << v);
+        }
+    }
+    B.prefix[B.nb] = B.total;
+}
+
+}  // namespace gqb

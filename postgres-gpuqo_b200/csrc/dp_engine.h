@@ -1,0 +1,53 @@
+// dp_engine.h - host interface of the device DP engine (dp_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "dp_layout.h"
+
+namespace gqb {
+
+enum DpMode : int {
+    kModeDpsub = 0,   // all-subsets enumeration (gpuqo_algorithm=dpsub, bicc off)
+    kModeMpdp = 1,    // biconnected-block enumeration (bicc on)
+};
+
+// One node of the extracted plan, compact masks (bit i = relation i).
+struct TreeNode {
+    uint32_t set;
+    int32_t left, right;          // node indices, -1 for leaves
+    float rows, startup, total;
+    int32_t width;
+};
+
+struct EngineStats {
+    uint64_t connected_sets = 0;
+    uint64_t evaluated_pairs = 0;
+    uint64_t filtered_subsets = 0;
+    uint64_t memo_bytes = 0;
+    double device_ms = 0.0;
+    double eval_kernel_ms = 0.0;
+    uint32_t eval_kernel_launches = 0;
+    uint32_t kernel_launches = 0;
+};
+
+// Runs one exact DP on the calling thread's current device.  `blob` is the
+// device planner info (DevHeader + class arrays, see dp_device.cuh).  On
+// success fills `nodes` (root first) and returns 0; otherwise a
+// GPUQO_B200_ERR_* code and a message in `err`.
+int engine_run(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, bool profile,
+               std::vector<TreeNode> &nodes, EngineStats &stats, std::string &err);
+
+// Device-resident timing of one DP (planner info uploaded once, the DP graph
+// replayed `iters` times, CUDA events on the engine stream, optional L2 flush
+// between replays).  Also returns the plan of the last replay.
+int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, int warmup, int iters,
+                         bool flush_l2, double &ms_per_iter, std::vector<TreeNode> &nodes, EngineStats &stats,
+                         std::string &err);
+
+// Device-memory estimate (bytes) of one exact DP over n relations.
+uint64_t engine_bytes_needed(int n);
+
+}  // namespace gqb

@@ -1,0 +1,75 @@
+// dp_layout.h - layout of the device planner-info blob, shared by the host
+// code that builds it and the kernels that read it.
+#pragma once
+
+#include <cstdint>
+
+#ifndef __CUDACC__
+#define GQB_HD
+#else
+#define GQB_HD __host__ __device__
+#endif
+
+namespace gqb {
+
+constexpr int kMaxRels = 32;      // compact masks are 32-bit
+constexpr int kWarp = 32;
+
+// ---------------------------------------------------------------------------
+// Device planner info blob (built on the host, copied into shared memory by
+// every CTA).  Layout: DevHeader, then
+//   uint32 ec_relids[n_ec]; uint32 ec_off[n_ec] (off_sels << 16 | off_fks);
+//   float sels[n_sels]; uint32 fks[n_fks]; DevVar vars[n_fks]
+// ---------------------------------------------------------------------------
+struct DevVar {
+    float stadistinct, stanullfrac, mcvfreq;
+    float idx_rows, idx_startup, idx_total;
+    uint32_t flags;                       // bit0 index.available, bit1 index.unique
+};
+static_assert(sizeof(DevVar) == 28, "DevVar layout");
+
+struct DevHeader {
+    int n, n_ec, n_sels, n_fks;
+    float cpu_operator_cost, cpu_tuple_cost, seq_page_cost, disable_cost;
+    int work_mem, enable_nestloop, enable_hashjoin;
+    uint32_t composite_mask;
+    uint32_t blob_words;                  // total blob size in 32-bit words
+    uint32_t pad[3];
+    uint32_t adj[kMaxRels];
+    float rows[kMaxRels];
+    float tuples[kMaxRels];
+    float startup[kMaxRels];
+    float total[kMaxRels];
+    int width[kMaxRels];
+};
+
+struct DevInfoView {
+    const DevHeader *h;
+    const uint32_t *ec_relids;
+    const uint32_t *ec_off;
+    const float *sels;
+    const uint32_t *fks;
+    const DevVar *vars;
+};
+
+GQB_HD inline DevInfoView make_view(const void *blob) {
+    DevInfoView v;
+    v.h = reinterpret_cast<const DevHeader *>(blob);
+    const uint32_t *p = reinterpret_cast<const uint32_t *>(v.h + 1);
+    v.ec_relids = p;
+    p += v.h->n_ec;
+    v.ec_off = p;
+    p += v.h->n_ec;
+    v.sels = reinterpret_cast<const float *>(p);
+    p += v.h->n_sels;
+    v.fks = p;
+    p += v.h->n_fks;
+    v.vars = reinterpret_cast<const DevVar *>(p);
+    return v;
+}
+
+GQB_HD inline uint32_t blob_words_for(int n_ec, int n_sels, int n_fks) {
+    return (uint32_t)(sizeof(DevHeader) / 4 + 2 * n_ec + n_sels + n_fks + n_fks * (sizeof(DevVar) / 4));
+}
+
+}  // namespace gqb

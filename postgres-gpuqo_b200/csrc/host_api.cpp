@@ -1,0 +1,499 @@
+// host_api.cpp - C ABI of libgpuqo_b200.so: gpuqo_run, the GUC variables,
+// conversion of the planner's C structures, BFS relabelling, plan output.
+//
+// The flow of one call mirrors __gpuqo_run (gpuqo_main_internal.cu:82-160):
+// convert -> BFS relabel -> exact DP (or IDP driver) -> map the plan back ->
+// palloc'd QueryTreeC.  The exact DP runs on the GPU (dp_kernels.cu).
+#include <csignal>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dp_engine.h"
+#include "gpuqo_b200.h"
+#include "host_idp.h"
+#include "host_info.h"
+
+// ---------------------------------------------------------------------------
+// Postgres backend symbols.  Weak: inside postgres the backend's own
+// definitions win; standalone (tests, bench) these stand in.
+// ---------------------------------------------------------------------------
+extern "C" {
+__attribute__((weak)) void *palloc(size_t size) { return malloc(size ? size : 1); }
+__attribute__((weak)) void *palloc0(size_t size) { return calloc(1, size ? size : 1); }
+__attribute__((weak)) void pfree(void *p) { free(p); }
+__attribute__((weak)) volatile sig_atomic_t InterruptPending = 0;
+__attribute__((weak)) void ProcessInterrupts(void) {}
+
+// Postgres cost GUCs read by setParams (gpuqo_planner_info.cu:84-131),
+// with Postgres defaults and the enable_* settings the reference's cost model
+// assumes (README "Limitations").
+__attribute__((weak)) double seq_page_cost = 1.0;
+__attribute__((weak)) double random_page_cost = 4.0;
+__attribute__((weak)) double cpu_tuple_cost = 0.01;
+__attribute__((weak)) double cpu_index_tuple_cost = 0.005;
+__attribute__((weak)) double cpu_operator_cost = 0.0025;
+__attribute__((weak)) int effective_cache_size = 524288;
+__attribute__((weak)) double disable_cost = 1.0e10;
+__attribute__((weak)) bool enable_seqscan = true;
+__attribute__((weak)) bool enable_indexscan = true;
+__attribute__((weak)) bool enable_tidscan = false;
+__attribute__((weak)) bool enable_sort = true;
+__attribute__((weak)) bool enable_hashagg = true;
+__attribute__((weak)) bool enable_nestloop = true;
+__attribute__((weak)) bool enable_mergejoin = false;
+__attribute__((weak)) bool enable_hashjoin = true;
+__attribute__((weak)) int work_mem = 4096;
+
+// gpuqo GUC variables, initialised to the boot values of guc.c
+// (src/backend/utils/misc/guc.c:1103-1170, 2140-2297, 4810-4826).
+__attribute__((weak)) int gpuqo_algorithm = GPUQO_DPSIZE;   // defined by gpuqo_main.c in postgres
+int gpuqo_scratchpad_size_mb = 10;
+int gpuqo_max_memo_size_mb = 1024;
+int gpuqo_min_memo_size_mb = 1;
+int gpuqo_n_parallel = 10240;
+bool gpuqo_dpsub_filter_enable = true;
+int gpuqo_dpsub_filter_threshold = 16;
+int gpuqo_dpsub_filter_cpu_enum_threshold = 1024;
+int gpuqo_dpsub_filter_keys_overprovisioning = 100;
+bool gpuqo_dpsub_ccc_enable = true;
+bool gpuqo_dpsub_csg_enable = true;
+int gpuqo_dpsub_csg_threshold = 128;
+bool gpuqo_dpsub_tree_enable = false;
+bool gpuqo_dpsub_bicc_enable = false;
+int gpuqo_dpe_n_threads = 4;
+int gpuqo_dpe_pairs_per_depbuf = 128;
+int gpuqo_cpu_dpsub_parallel_chunk_size = 64;
+bool gpuqo_spanning_tree_enable = false;
+int gpuqo_idp_n_iters = 0;
+int gpuqo_idp_type = GPUQO_IDP2;
+int gpuqo_dplin_csg_threshold_lindp = 10000;
+int gpuqo_dplin_threshold_lindp = 14;
+int gpuqo_dplin_threshold_idp = 100;
+
+int gpuqo_b200_profile_kernels = 0;
+}
+
+namespace gqb {
+
+static thread_local int t_last_error = GPUQO_B200_OK;
+static thread_local GpuqoB200Stats t_stats;
+
+void set_error(int code, const std::string &msg) {
+    t_last_error = code;
+    if (code != GPUQO_B200_OK) fprintf(stderr, "gpuqo_b200: %s\n", msg.c_str());
+}
+
+void stats_reset() { memset(&t_stats, 0, sizeof(t_stats)); }
+
+void stats_add(const EngineStats &s) {
+    t_stats.connected_sets += s.connected_sets;
+    t_stats.evaluated_pairs += s.evaluated_pairs;
+    t_stats.filtered_subsets += s.filtered_subsets;
+    if (s.memo_bytes > t_stats.memo_bytes) t_stats.memo_bytes = s.memo_bytes;
+    t_stats.device_ms += s.device_ms;
+    t_stats.eval_kernel_ms += s.eval_kernel_ms;
+    t_stats.eval_kernel_launches += s.eval_kernel_launches;
+    t_stats.kernel_launches += s.kernel_launches;
+    t_stats.n_subproblems += 1;
+}
+
+static inline int popc64(mask64 x) { return __builtin_popcountll(x); }
+static inline mask64 lowest64(mask64 x) { return x & (~x + 1); }
+static inline int lowest_pos64(mask64 x) { return __builtin_ffsll((long long)x) - 1; }
+static inline mask64 bit64(int n) { return (mask64)1 << n; }
+static inline mask64 pdep64(mask64 val, mask64 mask) {
+    mask64 r = 0;
+    for (mask64 bb = 1; mask; bb += bb) {
+        mask64 low = lowest64(mask);
+        if (val & bb) r |= low;
+        mask &= mask - 1;
+    }
+    return r;
+}
+static inline int ec_nsels(int s) { return s * (s - 1) / 2; }
+static inline int ec_index(int l, int r, int size) {
+    if (l > r) std::swap(l, r);
+    return l * size - l * (l + 1) / 2 + (r - l - 1);
+}
+
+HostParams read_params() {
+    HostParams p;
+    p.effective_cache_size = (float)effective_cache_size;
+    p.random_page_cost = (float)random_page_cost;
+    p.seq_page_cost = (float)seq_page_cost;
+    p.cpu_tuple_cost = (float)cpu_tuple_cost;
+    p.cpu_index_tuple_cost = (float)cpu_index_tuple_cost;
+    p.cpu_operator_cost = (float)cpu_operator_cost;
+    p.disable_cost = (float)disable_cost;
+    p.enable_seqscan = enable_seqscan;
+    p.enable_indexscan = enable_indexscan;
+    p.enable_tidscan = enable_tidscan;
+    p.enable_sort = enable_sort;
+    p.enable_hashagg = enable_hashagg;
+    p.enable_nestloop = enable_nestloop;
+    p.enable_mergejoin = enable_mergejoin;
+    p.enable_hashjoin = enable_hashjoin;
+    p.work_mem = work_mem;
+    return p;
+}
+
+static mask64 bms_word0(const Bitmapset *b, bool &wide) {
+    if (!b) return 0;
+    for (int i = 1; i < b->nwords; i++)
+        if (b->words[i]) wide = true;
+    return b->nwords > 0 ? b->words[0] : 0;
+}
+
+bool convert_info(const GpuqoPlannerInfoC *c, HostInfo &out, std::string &err) {
+    if (!c || c->n_rels < 1) {
+        err = "empty planner info";
+        return false;
+    }
+    if (c->n_rels >= 64) {
+        err = "64-bit conversion called with >= 64 relations";
+        return false;
+    }
+    bool wide = false;
+    out.n = c->n_rels;
+    out.p = read_params();
+    out.base.resize(out.n);
+    out.edge.resize(out.n);
+    for (int i = 0; i < out.n; i++) {
+        out.edge[i] = bms_word0(c->edge_table[i], wide);
+        HostBaseRel &b = out.base[i];
+        b.id = bms_word0(c->base_rels[i].id, wide);
+        b.rows = c->base_rels[i].rows;
+        b.tuples = c->base_rels[i].tuples;
+        b.width = c->base_rels[i].width;
+        b.cost = c->base_rels[i].cost;
+        b.composite = false;
+        if (b.id != bit64(i + 1)) {
+            err = "base relation " + std::to_string(i) + " does not carry relid bit " + std::to_string(i + 1);
+            return false;
+        }
+    }
+    out.ec_relids.clear();
+    out.ec_sels.clear();
+    out.ec_fks.clear();
+    out.ec_vars.clear();
+    for (const EqClassInfo *ec = c->eq_classes; ec != NULL; ec = ec->next) {
+        mask64 r = bms_word0(ec->relids, wide);
+        out.ec_relids.push_back(r);
+        int s = popc64(r);
+        for (int j = 0; j < ec_nsels(s); j++) out.ec_sels.push_back(ec->sels[j]);
+        for (int j = 0; j < s; j++) {
+            out.ec_fks.push_back(ec->fk ? bms_word0(ec->fk[j], wide) : 0);
+            out.ec_vars.push_back(ec->vars[j]);
+        }
+    }
+    if (wide) {
+        err = "relation ids beyond the 64-bit range";
+        return false;
+    }
+    return true;
+}
+
+std::vector<int> bfs_order(const HostInfo &info) {
+    std::vector<int> order;
+    std::vector<int> queue;
+    queue.reserve(info.n);
+    queue.push_back(0);
+    size_t front = 0;
+    mask64 seen = bit64(1);
+    while (front < queue.size() && (int)order.size() < info.n) {
+        int b = queue[front++];
+        mask64 edges = info.edge[b];
+        order.push_back(b);
+        while (edges) {
+            int next = lowest_pos64(edges);
+            if (!(seen & bit64(next))) queue.push_back(next - 1);
+            edges &= ~bit64(next);
+        }
+        seen |= info.edge[b];
+    }
+    return order;
+}
+
+HostInfo relabel(const HostInfo &from, const std::vector<int> &from_of_to) {
+    const int nt = (int)from_of_to.size();
+    std::vector<int> to_of_from(64, -1);
+    for (int t = 0; t < nt; t++) to_of_from[from_of_to[t]] = t;
+    auto remap = [&](mask64 m) {
+        mask64 o = 0;
+        for (int t = 0; t < nt; t++)
+            if (m & bit64(from_of_to[t] + 1)) o |= bit64(t + 1);
+        return o;
+    };
+    HostInfo to;
+    to.n = nt;
+    to.p = from.p;
+    to.base.resize(nt);
+    to.edge.resize(nt);
+    for (int t = 0; t < nt; t++) {
+        to.edge[t] = remap(from.edge[from_of_to[t]]) & ~bit64(t + 1);
+        to.base[t] = from.base[from_of_to[t]];
+        to.base[t].id = bit64(t + 1);
+    }
+    to.ec_relids.resize(from.ec_relids.size());
+    to.ec_sels.resize(from.ec_sels.size());
+    to.ec_fks.resize(from.ec_fks.size());
+    to.ec_vars.resize(from.ec_vars.size());
+    int off_sels = 0, off_fks = 0;
+    for (size_t i = 0; i < from.ec_relids.size(); i++) {
+        mask64 ecf = from.ec_relids[i];
+        mask64 ect = remap(ecf);
+        int s = popc64(ecf);
+        to.ec_relids[i] = ect;
+        for (int lt = 0; lt < s; lt++) {
+            mask64 id_lt = pdep64(bit64(lt), ect);
+            mask64 id_lf = bit64(from_of_to[lowest_pos64(id_lt) - 1] + 1);
+            int lf = popc64((lowest64(id_lf) - 1) & ecf);
+            for (int rt = lt + 1; rt < s; rt++) {
+                mask64 id_rt = pdep64(bit64(rt), ect);
+                mask64 id_rf = bit64(from_of_to[lowest_pos64(id_rt) - 1] + 1);
+                int rf = popc64((lowest64(id_rf) - 1) & ecf);
+                to.ec_sels[off_sels + ec_index(lt, rt, s)] = from.ec_sels[off_sels + ec_index(lf, rf, s)];
+            }
+            to.ec_fks[off_fks + lt] = remap(from.ec_fks[off_fks + lf]);
+            to.ec_vars[off_fks + lt] = from.ec_vars[off_fks + lf];
+        }
+        off_sels += ec_nsels(s);
+        off_fks += s;
+    }
+    return to;
+}
+
+std::vector<uint32_t> build_blob(const HostInfo &info) {
+    const int n_ec = (int)info.ec_relids.size();
+    const int n_sels = (int)info.ec_sels.size();
+    const int n_fks = (int)info.ec_fks.size();
+    std::vector<uint32_t> blob(blob_words_for(n_ec, n_sels, n_fks), 0u);
+    DevHeader *h = reinterpret_cast<DevHeader *>(blob.data());
+    h->n = info.n;
+    h->n_ec = n_ec;
+    h->n_sels = n_sels;
+    h->n_fks = n_fks;
+    h->cpu_operator_cost = info.p.cpu_operator_cost;
+    h->cpu_tuple_cost = info.p.cpu_tuple_cost;
+    h->seq_page_cost = info.p.seq_page_cost;
+    h->disable_cost = info.p.disable_cost;
+    h->work_mem = info.p.work_mem;
+    h->enable_nestloop = info.p.enable_nestloop ? 1 : 0;
+    h->enable_hashjoin = info.p.enable_hashjoin ? 1 : 0;
+    h->composite_mask = 0;
+    h->blob_words = (uint32_t)blob.size();
+    for (int i = 0; i < info.n; i++) {
+        h->adj[i] = (uint32_t)(info.edge[i] >> 1);
+        h->rows[i] = info.base[i].rows;
+        h->tuples[i] = info.base[i].tuples;
+        h->startup[i] = info.base[i].cost.startup;
+        h->total[i] = info.base[i].cost.total;
+        h->width[i] = info.base[i].width;
+        if (info.base[i].composite) h->composite_mask |= 1u << i;
+    }
+    DevInfoView v = make_view(blob.data());
+    uint32_t *relids = const_cast<uint32_t *>(v.ec_relids);
+    uint32_t *offs = const_cast<uint32_t *>(v.ec_off);
+    float *sels = const_cast<float *>(v.sels);
+    uint32_t *fks = const_cast<uint32_t *>(v.fks);
+    DevVar *vars = const_cast<DevVar *>(v.vars);
+    int off_sels = 0, off_fks = 0;
+    for (int i = 0; i < n_ec; i++) {
+        relids[i] = (uint32_t)(info.ec_relids[i] >> 1);
+        offs[i] = ((uint32_t)off_sels << 16) | (uint32_t)off_fks;
+        int s = popc64(info.ec_relids[i]);
+        off_sels += ec_nsels(s);
+        off_fks += s;
+    }
+    for (int i = 0; i < n_sels; i++) sels[i] = info.ec_sels[i];
+    for (int i = 0; i < n_fks; i++) {
+        fks[i] = (uint32_t)(info.ec_fks[i] >> 1);
+        const VarInfo &vi = info.ec_vars[i];
+        vars[i].stadistinct = vi.stats.stadistinct;
+        vars[i].stanullfrac = vi.stats.stanullfrac;
+        vars[i].mcvfreq = vi.stats.mcvfreq;
+        vars[i].idx_rows = vi.index.rows;
+        vars[i].idx_startup = vi.index.cost.startup;
+        vars[i].idx_total = vi.index.cost.total;
+        vars[i].flags = (vi.index.available ? 1u : 0u) | (vi.index.unique ? 2u : 0u);
+    }
+    return blob;
+}
+
+// Exact DP of a relabelled info with <= 31 relations on the GPU.
+int exact_dp(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, std::string &err) {
+    if (info.n > 31) {
+        err = "exact DP over " + std::to_string(info.n) + " relations exceeds the dense-memo limit (31)";
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    if (info.ec_sels.size() >= 65536 || info.ec_fks.size() >= 65536) {
+        err = "too many equivalence-class entries";
+        return GPUQO_B200_ERR_ARGS;
+    }
+    std::vector<uint32_t> blob = build_blob(info);
+    EngineStats st;
+    int rc = engine_run(blob, info.n, mode, gpuqo_dpsub_ccc_enable, gpuqo_b200_profile_kernels != 0, nodes, st, err);
+    if (rc == 0) stats_add(st);
+    return rc;
+}
+
+DpMode mode_for(int algorithm) {
+    switch (algorithm) {
+    case GPUQO_CPU_DPSUB_BICC:
+    case GPUQO_CPU_DPSUB_BICC_PARALLEL:
+        return kModeMpdp;
+    case GPUQO_CPU_DPSUB:
+    case GPUQO_CPU_DPSUB_PARALLEL:
+    case GPUQO_DPE_DPSUB:
+        return kModeDpsub;
+    default:
+        return gpuqo_dpsub_bicc_enable ? kModeMpdp : kModeDpsub;
+    }
+}
+
+bool algorithm_supported(int algorithm) {
+    switch (algorithm) {
+    case GPUQO_DPSUB:
+    case GPUQO_CPU_DPSUB:
+    case GPUQO_CPU_DPSUB_PARALLEL:
+    case GPUQO_CPU_DPSUB_BICC:
+    case GPUQO_CPU_DPSUB_BICC_PARALLEL:
+    case GPUQO_DPE_DPSUB:
+        return true;
+    default:
+        return false;
+    }
+}
+
+static Bitmapset *make_bms(mask64 m) {
+    Bitmapset *b = (Bitmapset *)palloc0(offsetof(Bitmapset, words) + sizeof(bitmapword));
+    b->nwords = 1;
+    b->words[0] = m;
+    return b;
+}
+
+// node array (compact masks over relabelled relations) -> QueryTreeC with the
+// caller's relids (remapQueryTree gpuqo_remapper.cu:279-300, convertQueryTree
+// gpuqo_planner_info.cu:256-270)
+static QueryTreeC *nodes_to_c(const std::vector<TreeNode> &nodes, int idx, const std::vector<int> &from_of_to) {
+    if (idx < 0) return NULL;
+    const TreeNode &t = nodes[idx];
+    QueryTreeC *q = (QueryTreeC *)palloc(sizeof(QueryTreeC));
+    mask64 orig = 0;
+    for (size_t k = 0; k < from_of_to.size(); k++)
+        if (t.set & (1u << k)) orig |= bit64(from_of_to[k] + 1);
+    q->id = make_bms(orig);
+    q->left = nodes_to_c(nodes, t.left, from_of_to);
+    q->right = nodes_to_c(nodes, t.right, from_of_to);
+    q->width = t.width;
+    q->cost.startup = t.startup;
+    q->cost.total = t.total;
+    q->rows = t.rows;
+    return q;
+}
+
+QueryTreeC *run_one(int algorithm, GpuqoPlannerInfoC *info_c) {
+    t_last_error = GPUQO_B200_OK;
+    std::string err;
+    if (!algorithm_supported(algorithm)) {
+        set_error(GPUQO_B200_ERR_UNSUPPORTED,
+                  "algorithm " + std::to_string(algorithm) + " is outside this library (DPsub/MPDP only)");
+        return NULL;
+    }
+    if (!info_c || info_c->n_rels < 1) {
+        set_error(GPUQO_B200_ERR_ARGS, "empty planner info");
+        return NULL;
+    }
+    if (InterruptPending) {
+        ProcessInterrupts();
+        set_error(GPUQO_B200_ERR_CANCELLED, "cancelled");
+        return NULL;
+    }
+    const int n = info_c->n_rels;
+    const bool idp = gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < n;
+    if (idp || n >= 64) return run_idp(algorithm, info_c);
+
+    HostInfo info;
+    if (!convert_info(info_c, info, err)) {
+        set_error(GPUQO_B200_ERR_ARGS, err);
+        return NULL;
+    }
+    std::vector<int> order = bfs_order(info);
+    HostInfo remapped = relabel(info, order);
+    std::vector<TreeNode> nodes;
+    int rc = exact_dp(remapped, mode_for(algorithm), nodes, err);
+    if (rc) {
+        set_error(rc, err);
+        return NULL;
+    }
+    return nodes_to_c(nodes, 0, order);
+}
+
+}  // namespace gqb
+
+using namespace gqb;
+
+extern "C" QueryTreeC *gpuqo_run(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *info) {
+    stats_reset();
+    return run_one(gpuqo_algorithm_arg, info);
+}
+
+extern "C" int gpuqo_b200_last_error(void) { return t_last_error; }
+
+extern "C" void gpuqo_b200_free_query_tree(QueryTreeC *qt) {
+    if (!qt) return;
+    gpuqo_b200_free_query_tree(qt->left);
+    gpuqo_b200_free_query_tree(qt->right);
+    if (qt->id) pfree(qt->id);
+    pfree(qt);
+}
+
+extern "C" void gpuqo_b200_get_stats(GpuqoB200Stats *out) {
+    if (out) *out = t_stats;
+}
+
+extern "C" int gpuqo_b200_time_resident(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *info_c, int warmup, int iters,
+                                        int flush_l2, double *ms_per_iter, QueryTreeC **tree) {
+    stats_reset();
+    t_last_error = GPUQO_B200_OK;
+    std::string err;
+    if (!algorithm_supported(gpuqo_algorithm_arg) || !info_c || info_c->n_rels < 1 || info_c->n_rels > 31 ||
+        warmup < 0 || iters < 1 || !ms_per_iter) {
+        set_error(GPUQO_B200_ERR_ARGS, "gpuqo_b200_time_resident: bad arguments");
+        return t_last_error;
+    }
+    HostInfo info;
+    if (!convert_info(info_c, info, err)) {
+        set_error(GPUQO_B200_ERR_ARGS, err);
+        return t_last_error;
+    }
+    std::vector<int> order = bfs_order(info);
+    HostInfo remapped = relabel(info, order);
+    std::vector<uint32_t> blob = build_blob(remapped);
+    std::vector<TreeNode> nodes;
+    EngineStats st;
+    int rc = engine_time_resident(blob, remapped.n, mode_for(gpuqo_algorithm_arg), gpuqo_dpsub_ccc_enable, warmup,
+                                  iters, flush_l2 != 0, *ms_per_iter, nodes, st, err);
+    if (rc) {
+        set_error(rc, err);
+        return rc;
+    }
+    stats_add(st);
+    if (tree) *tree = nodes_to_c(nodes, 0, order);
+    return GPUQO_B200_OK;
+}
+
+extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC **infos, int n_queries,
+                                    QueryTreeC **out) {
+    stats_reset();
+    if (!infos || !out || n_queries < 0) return GPUQO_B200_ERR_ARGS;
+    int status = GPUQO_B200_OK;
+    for (int i = 0; i < n_queries; i++) {
+        out[i] = run_one(gpuqo_algorithm_arg, infos[i]);
+        if (!out[i]) status = t_last_error;
+    }
+    return status;
+}

@@ -1,0 +1,42 @@
+"""CPU tests of the C ABI: the product library loads, exports every symbol
+include/gpuqo_b200.h declares, and the ctypes mirror of the reference structs
+has the reference's layout.  No compute call is made (no GPU here)."""
+import ctypes as C
+
+from gpuqo_b200 import capi, lib
+
+
+def test_library_exports_declared_symbols():
+    l = lib.load()
+    syms = lib.declared_symbols()
+    assert "gpuqo_run" in syms and "gpuqo_dpsub_bicc_enable" in syms
+    missing = [s for s in syms if not hasattr(l, s)]
+    assert not missing, missing
+
+
+def test_guc_boot_values():
+    l = lib.load()
+    # boot values of src/backend/utils/misc/guc.c
+    assert capi.get_int(l, "gpuqo_n_parallel") == 10240
+    assert capi.get_int(l, "gpuqo_dpsub_filter_threshold") == 16
+    assert capi.get_int(l, "gpuqo_idp_type") == capi.GPUQO_IDP2
+    assert C.c_bool.in_dll(l, "gpuqo_dpsub_ccc_enable").value is True
+    assert C.c_bool.in_dll(l, "gpuqo_dpsub_bicc_enable").value is False
+
+
+def test_struct_layouts_match_reference():
+    # LP64 layouts of src/include/optimizer/gpuqo_planner_info.h / gpuqo_common.h
+    assert C.sizeof(capi.PathCost) == 8
+    assert C.sizeof(capi.GpuqoIndexInfo) == 16
+    assert C.sizeof(capi.VarInfoC) == 28
+    assert C.sizeof(capi.BaseRelationC) == 32
+    assert C.sizeof(capi.EqClassInfo) == 48
+    assert C.sizeof(capi.GpuqoPlannerInfoC) == 48
+    assert C.sizeof(capi.QueryTreeC) == 40
+    assert capi.GpuqoPlannerInfoC.n_eq_classes.offset == 32
+
+
+def test_bitmapset_roundtrip():
+    for bits in (0b10, 1 << 63, (1 << 64) | 2, (1 << 200) | (1 << 65) | 4):
+        b = capi.make_bitmapset(bits)
+        assert capi.read_bitmapset(C.addressof(b)) == bits
