@@ -219,6 +219,39 @@ int gpuqo_b200_time_resident(int gpuqo_algorithm, GpuqoPlannerInfoC *info, int w
                              int flush_l2, double *ms_per_iter, QueryTreeC **tree);
 
 /*
+ * One node of a plan returned in caller-provided storage: relids in the
+ * caller's numbering (relation i is bit i+1), children as indices into the
+ * same array (-1 for leaves), node 0 is the root.
+ */
+typedef struct GpuqoB200PlanNode {
+    uint64_t relids;
+    int32_t left, right;
+    float rows;
+    float startup;
+    float total;
+    int32_t width;
+} GpuqoB200PlanNode;
+
+/*
+ * No counterpart in the reference.  Exact DP (same algorithm selection and
+ * same plans as gpuqo_run) that allocates nothing, for callers that cannot
+ * allocate device memory: a Postgres backend that must not leak GPU memory
+ * when elog(ERROR) longjmps out of a cancelled query, or a process whose
+ * device memory is owned by another pool.  All scratch lives in one static
+ * device array of about 6.7 MB that every GPU loading this library keeps
+ * until exit; queries are limited to 18 relations (larger ones return
+ * GPUQO_B200_ERR_TOO_LARGE with a message).  The caller passes the planner
+ * info (host, as for gpuqo_run), a CUDA stream (cudaStream_t, NULL for the
+ * default stream) and an output array of at least 2*n_rels-1 nodes; the call
+ * returns after the stream work completes.  The first call on each device
+ * looks up the scratch address (cudaGetSymbolAddress) - make it before any
+ * stream capture.  Calls share the scratch: calls that overlap on the GPU
+ * race.  Returns a status code.
+ */
+int gpuqo_b200_run_noalloc(int gpuqo_algorithm, const GpuqoPlannerInfoC *info, void *cuda_stream,
+                           GpuqoB200PlanNode *nodes, int max_nodes, int *n_nodes);
+
+/*
  * Batched exact DP: optimises n_queries independent queries (each < 32
  * relations, no IDP) with one persistent launch sequence per relation count
  * level, all queries' memos packed in one device arena.  Trees are written to

@@ -917,3 +917,343 @@ int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, 
 }
 
 }  // namespace gqb
+
+// ===========================================================================
+// Entry point that allocates nothing.
+//
+// Some callers cannot allocate device memory: code that must not leak when
+// Postgres aborts a query with elog(ERROR) (a longjmp past any cudaFree),
+// processes whose device memory is owned by another pool, and paths with a
+// fixed memory budget.  gpuqo_b200_run_noalloc serves them for queries of up
+// to kNoAllocMaxRels relations: every scratch buffer of the DP (dense memo,
+// level lists, overflow lists, counters, planner-info blob, plan nodes) is
+// carved out of the one file-scope array below, which every GPU that loads
+// this library holds until the process exits.  Host-side conversion uses
+// fixed-size stack buffers; kernels are launched directly on the caller's
+// stream (no graph, no events).
+//
+// In host code g_noalloc_scratch names a host-side stand-in, not the device
+// array; its device address comes from cudaGetSymbolAddress, done once per
+// device by the first call on that device (so make that first call before
+// any stream capture).  All calls share the array: calls that overlap on the
+// GPU race with each other.
+// ===========================================================================
+// Postgres cost GUCs (host_api.cpp / the backend), read the way setParams does
+extern "C" double seq_page_cost, cpu_tuple_cost, cpu_operator_cost, disable_cost;
+extern "C" int work_mem;
+extern "C" bool enable_nestloop, enable_hashjoin;
+
+namespace gqb {
+
+constexpr int kNoAllocMaxRels = 18;
+constexpr uint32_t kNoAllocMaxBlobWords = 6144;
+constexpr uint64_t kNoAllocMaxSets = 48620;   // C(18, 9), the largest level
+
+constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaMemo = 0;
+constexpr size_t kNaMemoLeft = kNaMemo + na_align((1ull << kNoAllocMaxRels) * sizeof(float4));
+constexpr size_t kNaSets = kNaMemoLeft + na_align((1ull << kNoAllocMaxRels) * sizeof(uint32_t));
+constexpr size_t kNaOvfSet = kNaSets + na_align(kNoAllocMaxSets * 4);
+constexpr size_t kNaOvfP = kNaOvfSet + na_align(kNoAllocMaxSets * 4);
+constexpr size_t kNaOvfOff = kNaOvfP + na_align(kNoAllocMaxSets * 4);
+constexpr size_t kNaOvfKey = kNaOvfOff + na_align(kNoAllocMaxSets * 4);
+constexpr size_t kNaOvfFirst = kNaOvfKey + na_align(kNoAllocMaxSets * 8);
+constexpr size_t kNaLvl = kNaOvfFirst + na_align(kNoAllocMaxSets * 8);
+constexpr size_t kNaGlob = kNaLvl + na_align(33 * sizeof(LevelCounters));
+constexpr size_t kNaBlob = kNaGlob + na_align(sizeof(GlobalCounters));
+constexpr size_t kNaBinom = kNaBlob + na_align(kNoAllocMaxBlobWords * 4);
+constexpr size_t kNaTree = kNaBinom + na_align(33 * 33 * 4);
+constexpr size_t kNaTreeN = kNaTree + na_align(64 * sizeof(TreeNode));
+constexpr size_t kNaTotal = kNaTreeN + na_align(sizeof(int));   // about 6.7 MB
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaTotal];
+
+static std::mutex g_na_mu;
+static unsigned char *g_na_ptr[64];   // device address of the scratch, per device
+static bool g_na_ready[64];
+
+// Once per device, with that device current: resolve the scratch address and
+// fill the binomial table.  No allocation.
+static int noalloc_setup(int dev) {
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (g_na_ready[dev]) return 0;
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || ptr == nullptr) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+        return GPUQO_B200_ERR_CUDA;
+    }
+    static uint32_t table[33 * 33];
+    for (int i = 0; i <= 32; i++)
+        for (int j = 0; j <= 32; j++) {
+            uint64_t v = binom64(i, j);
+            table[i * 33 + j] = v > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)v;
+        }
+    e = cudaMemcpy((unsigned char *)ptr + kNaBinom, table, sizeof(table), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: binomial table upload failed: %s\n", cudaGetErrorString(e));
+        return GPUQO_B200_ERR_CUDA;
+    }
+    g_na_ptr[dev] = (unsigned char *)ptr;
+    g_na_ready[dev] = true;
+    return 0;
+}
+
+static inline uint64_t na_bms(const Bitmapset *b) { return (b && b->nwords > 0) ? b->words[0] : 0ull; }
+static inline int na_popc(uint64_t x) { return __builtin_popcountll(x); }
+static inline uint64_t na_pdep(uint64_t val, uint64_t mask) {
+    uint64_t r = 0;
+    for (uint64_t bb = 1; mask; bb += bb) {
+        uint64_t low = mask & (~mask + 1);
+        if (val & bb) r |= low;
+        mask &= mask - 1;
+    }
+    return r;
+}
+static inline int na_ecidx(int l, int r, int size) {
+    if (l > r) { int t = l; l = r; r = t; }
+    return l * size - l * (l + 1) / 2 + (r - l - 1);
+}
+
+// GpuqoPlannerInfoC -> BFS-relabelled device blob in a caller buffer (the
+// same relabelling as bfs_order/relabel/build_blob, in fixed-size storage).
+static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &words, int *from_of_to) {
+    const int n = c->n_rels;
+    uint64_t edge[kNoAllocMaxRels];
+    for (int i = 0; i < n; i++) {
+        if (na_bms(c->base_rels[i].id) != (1ull << (i + 1))) return GPUQO_B200_ERR_ARGS;
+        edge[i] = na_bms(c->edge_table[i]);
+    }
+    // BFS order (gpuqo_bfs_indexing.cu:14-55)
+    int queue[kNoAllocMaxRels * kNoAllocMaxRels + 1];
+    int front = 0, back = 0, nt = 0;
+    queue[back++] = 0;
+    uint64_t seen = 2ull;
+    while (front != back && nt < n) {
+        int b = queue[front++];
+        from_of_to[nt++] = b;
+        uint64_t e = edge[b];
+        while (e) {
+            int next = __builtin_ffsll((long long)e) - 1;
+            if (!(seen & (1ull << next)) && back < kNoAllocMaxRels * kNoAllocMaxRels) queue[back++] = next - 1;
+            e &= ~(1ull << next);
+        }
+        seen |= edge[b];
+    }
+    if (nt != n) return GPUQO_B200_ERR_ARGS;   // disconnected graph
+    auto remap = [&](uint64_t m) {
+        uint64_t o = 0;
+        for (int t = 0; t < n; t++)
+            if (m & (1ull << (from_of_to[t] + 1))) o |= 1ull << t;   // compact bit t
+        return o;
+    };
+    int n_ec = 0, n_sels = 0, n_fks = 0;
+    for (const EqClassInfo *ec = c->eq_classes; ec; ec = ec->next) {
+        int s = na_popc(na_bms(ec->relids));
+        n_ec++;
+        n_sels += s * (s - 1) / 2;
+        n_fks += s;
+    }
+    if (n_sels >= 65536 || n_fks >= 65536) return GPUQO_B200_ERR_ARGS;
+    words = blob_words_for(n_ec, n_sels, n_fks);
+    if (words > kNoAllocMaxBlobWords) return GPUQO_B200_ERR_ARGS;
+    for (uint32_t i = 0; i < words; i++) blob[i] = 0u;
+    DevHeader *h = reinterpret_cast<DevHeader *>(blob);
+    h->n = n;
+    h->n_ec = n_ec;
+    h->n_sels = n_sels;
+    h->n_fks = n_fks;
+    h->cpu_operator_cost = (float)cpu_operator_cost;
+    h->cpu_tuple_cost = (float)cpu_tuple_cost;
+    h->seq_page_cost = (float)seq_page_cost;
+    h->disable_cost = (float)disable_cost;
+    h->work_mem = work_mem;
+    h->enable_nestloop = enable_nestloop ? 1 : 0;
+    h->enable_hashjoin = enable_hashjoin ? 1 : 0;
+    h->composite_mask = 0;
+    h->blob_words = words;
+    for (int t = 0; t < n; t++) {
+        const BaseRelationC &b = c->base_rels[from_of_to[t]];
+        h->adj[t] = (uint32_t)(remap(edge[from_of_to[t]]) & ~(1ull << t));
+        h->rows[t] = b.rows;
+        h->tuples[t] = b.tuples;
+        h->startup[t] = b.cost.startup;
+        h->total[t] = b.cost.total;
+        h->width[t] = b.width;
+    }
+    DevInfoView v = make_view(blob);
+    uint32_t *relids = const_cast<uint32_t *>(v.ec_relids);
+    uint32_t *offs = const_cast<uint32_t *>(v.ec_off);
+    float *sels = const_cast<float *>(v.sels);
+    uint32_t *fks = const_cast<uint32_t *>(v.fks);
+    DevVar *vars = const_cast<DevVar *>(v.vars);
+    int i = 0, off_sels = 0, off_fks = 0;
+    for (const EqClassInfo *ec = c->eq_classes; ec; ec = ec->next, i++) {
+        uint64_t ecf = na_bms(ec->relids);     // Postgres bits
+        uint64_t ect = remap(ecf);             // compact bits
+        int s = na_popc(ecf);
+        relids[i] = (uint32_t)ect;
+        offs[i] = ((uint32_t)off_sels << 16) | (uint32_t)off_fks;
+        for (int lt = 0; lt < s; lt++) {
+            uint64_t id_lt = na_pdep(1ull << lt, ect);
+            uint64_t id_lf = 1ull << (from_of_to[__builtin_ffsll((long long)id_lt) - 1] + 1);
+            int lf = na_popc((id_lf - 1) & ecf);
+            for (int rt = lt + 1; rt < s; rt++) {
+                uint64_t id_rt = na_pdep(1ull << rt, ect);
+                uint64_t id_rf = 1ull << (from_of_to[__builtin_ffsll((long long)id_rt) - 1] + 1);
+                int rf = na_popc((id_rf - 1) & ecf);
+                sels[off_sels + na_ecidx(lt, rt, s)] = ec->sels[na_ecidx(lf, rf, s)];
+            }
+            fks[off_fks + lt] = (uint32_t)remap(ec->fk ? na_bms(ec->fk[lf]) : 0ull);
+            const VarInfo &vi = ec->vars[lf];
+            DevVar &dv = vars[off_fks + lt];
+            dv.stadistinct = vi.stats.stadistinct;
+            dv.stanullfrac = vi.stats.stanullfrac;
+            dv.mcvfreq = vi.stats.mcvfreq;
+            dv.idx_rows = vi.index.rows;
+            dv.idx_startup = vi.index.cost.startup;
+            dv.idx_total = vi.index.cost.total;
+            dv.flags = (vi.index.available ? 1u : 0u) | (vi.index.unique ? 2u : 0u);
+        }
+        off_sels += s * (s - 1) / 2;
+        off_fks += s;
+    }
+    return 0;
+}
+
+}  // namespace gqb
+
+extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlannerInfoC *info, void *cuda_stream,
+                                      GpuqoB200PlanNode *out_nodes, int max_nodes, int *n_nodes) {
+    using namespace gqb;
+    if (!info || !out_nodes || !n_nodes) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: NULL argument\n");
+        return GPUQO_B200_ERR_ARGS;
+    }
+    const int n = info->n_rels;
+    if (n < 1 || n > kNoAllocMaxRels) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: %d relations; this entry point handles 1..%d\n", n,
+                kNoAllocMaxRels);
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    if (max_nodes < 2 * n - 1) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: output holds %d nodes, %d needed\n", max_nodes, 2 * n - 1);
+        return GPUQO_B200_ERR_ARGS;
+    }
+    DpMode mode;
+    switch (gpuqo_algorithm_arg) {
+    case GPUQO_CPU_DPSUB_BICC:
+    case GPUQO_CPU_DPSUB_BICC_PARALLEL:
+        mode = kModeMpdp;
+        break;
+    case GPUQO_CPU_DPSUB:
+    case GPUQO_CPU_DPSUB_PARALLEL:
+    case GPUQO_DPE_DPSUB:
+        mode = kModeDpsub;
+        break;
+    case GPUQO_DPSUB:
+        mode = gpuqo_dpsub_bicc_enable ? kModeMpdp : kModeDpsub;
+        break;
+    default:
+        fprintf(stderr, "gpuqo_b200_run_noalloc: algorithm %d is outside this library\n", gpuqo_algorithm_arg);
+        return GPUQO_B200_ERR_UNSUPPORTED;
+    }
+    uint32_t blob[kNoAllocMaxBlobWords];
+    uint32_t words = 0;
+    int from_of_to[kNoAllocMaxRels];
+    if (int rc = noalloc_blob(info, blob, words, from_of_to)) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: planner info not supported (disconnected graph, relid layout "
+                        "or more than %u blob words)\n", kNoAllocMaxBlobWords);
+        return rc;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GPUQO_B200_ERR_CUDA;
+    if (int rc = noalloc_setup(dev)) return rc;
+    unsigned char *base = g_na_ptr[dev];
+    cudaStream_t stream = (cudaStream_t)cuda_stream;
+    float4 *memo = (float4 *)(base + kNaMemo);
+    uint32_t *memo_left = (uint32_t *)(base + kNaMemoLeft);
+    uint32_t *sets = (uint32_t *)(base + kNaSets);
+    uint32_t *ovf_set = (uint32_t *)(base + kNaOvfSet);
+    uint32_t *ovf_P = (uint32_t *)(base + kNaOvfP);
+    uint32_t *ovf_off = (uint32_t *)(base + kNaOvfOff);
+    unsigned long long *ovf_key = (unsigned long long *)(base + kNaOvfKey);
+    unsigned long long *ovf_first = (unsigned long long *)(base + kNaOvfFirst);
+    LevelCounters *lvl = (LevelCounters *)(base + kNaLvl);
+    GlobalCounters *glob = (GlobalCounters *)(base + kNaGlob);
+    uint32_t *d_blob = (uint32_t *)(base + kNaBlob);
+    uint32_t *binom = (uint32_t *)(base + kNaBinom);
+    TreeNode *tree = (TreeNode *)(base + kNaTree);
+    int *tree_n = (int *)(base + kNaTreeN);
+    int sm_count = 148;
+    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+    const int ccc = gpuqo_dpsub_ccc_enable ? 1 : 0;
+    const size_t smem = (size_t)(((words + 3u) & ~3u) + kWarpsPerBlock * kQueueWords) * 4u;
+
+    // counters start at zero on every call; the memo needs no clearing (only
+    // entries written earlier in the same call are read)
+    cudaMemcpyAsync(d_blob, blob, words * 4, cudaMemcpyHostToDevice, stream);
+    cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
+    cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
+    cudaMemsetAsync(tree_n, 0, sizeof(int), stream);
+    k_init_base<<<1, 32, 0, stream>>>(d_blob, memo, memo_left);
+    for (int k = 2; k <= n; k++) {
+        uint64_t total = binom64(n, k);
+        uint64_t threads = std::min<uint64_t>((uint64_t)sm_count * 8 * kBlock, (total + 3) / 4);
+        threads = std::max<uint64_t>(threads, 32);
+        uint32_t per_thread = (uint32_t)((total + threads - 1) / threads);
+        uint32_t fblocks = (uint32_t)((total + (uint64_t)per_thread * kBlock - 1) / ((uint64_t)per_thread * kBlock));
+        LevelCounters *lc = lvl + k;
+        k_filter<<<fblocks, kBlock, 0, stream>>>(d_blob, binom, n, k, total, per_thread, sets, lc);
+        int eblocks = (int)std::min<uint64_t>((uint64_t)sm_count * 4, (total + kWarpsPerBlock - 1) / kWarpsPerBlock);
+        bool may_overflow = ((1ull << k) - 2ull) > kOvfLimit;
+        if (mode == kModeDpsub) {
+            k_eval<kModeDpsub><<<eblocks, kBlock, smem, stream>>>(d_blob, words, k, sets, lc, memo, memo_left, ovf_set,
+                                                                  ovf_P, ovf_off, ovf_key, ovf_first, glob, ccc);
+            if (may_overflow) {
+                k_ovf_chunks<kModeDpsub><<<sm_count * 4, kBlock, smem, stream>>>(
+                    d_blob, words, k, lc, memo, ovf_set, ovf_P, ovf_off, ovf_key, ovf_first, glob, ccc);
+                k_ovf_finalize<kModeDpsub><<<sm_count, kBlock, smem, stream>>>(d_blob, words, lc, memo, memo_left,
+                                                                               ovf_set, ovf_key, ovf_first);
+            }
+        } else {
+            k_eval<kModeMpdp><<<eblocks, kBlock, smem, stream>>>(d_blob, words, k, sets, lc, memo, memo_left, ovf_set,
+                                                                 ovf_P, ovf_off, ovf_key, ovf_first, glob, ccc);
+            if (may_overflow) {
+                k_ovf_chunks<kModeMpdp><<<sm_count * 4, kBlock, smem, stream>>>(
+                    d_blob, words, k, lc, memo, ovf_set, ovf_P, ovf_off, ovf_key, ovf_first, glob, ccc);
+                k_ovf_finalize<kModeMpdp><<<sm_count, kBlock, smem, stream>>>(d_blob, words, lc, memo, memo_left,
+                                                                              ovf_set, ovf_key, ovf_first);
+            }
+        }
+    }
+    k_extract<<<1, 32, 0, stream>>>(memo, memo_left, (1u << n) - 1u, tree, tree_n);
+    TreeNode host_nodes[64];
+    int host_n = 0;
+    cudaMemcpyAsync(host_nodes, tree, 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&host_n, tree_n, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: %s\n", cudaGetErrorString(e));
+        return GPUQO_B200_ERR_CUDA;
+    }
+    if (host_n != 2 * n - 1) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: plan extraction produced %d nodes\n", host_n);
+        return GPUQO_B200_ERR_CUDA;
+    }
+    for (int j = 0; j < host_n; j++) {
+        uint64_t orig = 0;
+        for (int t = 0; t < n; t++)
+            if (host_nodes[j].set & (1u << t)) orig |= 1ull << (from_of_to[t] + 1);
+        out_nodes[j].relids = orig;
+        out_nodes[j].left = host_nodes[j].left;
+        out_nodes[j].right = host_nodes[j].right;
+        out_nodes[j].rows = host_nodes[j].rows;
+        out_nodes[j].startup = host_nodes[j].startup;
+        out_nodes[j].total = host_nodes[j].total;
+        out_nodes[j].width = host_nodes[j].width;
+    }
+    *n_nodes = host_n;
+    return GPUQO_B200_OK;
+}
