@@ -199,7 +199,7 @@ typedef struct GpuqoB200Stats {
     uint32_t eval_kernel_launches;
     uint32_t n_subproblems;       /* exact DP runs (1, or IDP iterations) */
     uint32_t kernel_launches;     /* kernels launched by the DP runs */
-    uint32_t reserved;
+    uint32_t fallback_sets;       /* tree-mode sets re-evaluated in exact order (ties, NaN) */
 } GpuqoB200Stats;
 void gpuqo_b200_get_stats(GpuqoB200Stats *out);
 

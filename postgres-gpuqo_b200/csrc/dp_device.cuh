@@ -126,8 +126,8 @@ __device__ __forceinline__ Htsz exec_choose_hash_table_size(float ntuples, int t
     long long hash_table_bytes = (long long)work_mem * 1024LL;
     float space_allowed = (float)hash_table_bytes;
     long long skew_table_bytes = hash_table_bytes * 2 / 100;
-    long long num_skew_mcvs = skew_table_bytes / (tupsize + 84);
-    if (num_skew_mcvs > 0) hash_table_bytes -= skew_table_bytes;
+    // num_skew_mcvs = skew_table_bytes / (tupsize + 84) > 0  <=>  skew >= tupsize + 84
+    if (skew_table_bytes >= (long long)(tupsize + 84)) hash_table_bytes -= skew_table_bytes;
     long long max_pointers = (long long)(space_allowed / 8.0f);
     {
         unsigned long long a = (unsigned long long)max_pointers, b = 0x3fffffffULL / 8ULL;
@@ -144,7 +144,10 @@ __device__ __forceinline__ Htsz exec_choose_hash_table_size(float ntuples, int t
     long long bucket_bytes = 8LL * res.numbuckets;
     if (inner_rel_bytes + (float)bucket_bytes > (float)hash_table_bytes) {
         long long bucket_size = (long long)tupsize + 8LL;
-        long long lbuckets = 1LL << ceil_log2_l(hash_table_bytes / bucket_size);
+        long long q = (hash_table_bytes < 0x100000000LL && bucket_size < 0x100000000LL)
+                          ? (long long)((uint32_t)hash_table_bytes / (uint32_t)bucket_size)
+                          : hash_table_bytes / bucket_size;
+        long long lbuckets = 1LL << ceil_log2_l(q);
         if (lbuckets > max_pointers) lbuckets = max_pointers;
         res.numbuckets = (int)lbuckets;
         res.numbuckets = 1 << ceil_log2_l(res.numbuckets);
@@ -278,8 +281,7 @@ __device__ __forceinline__ float fkselc_of_ec(const DevInfoView &d, int off_fk, 
         int out_idx = popc((out_id - 1u) & ec);
         uint32_t match = inner_rels & d.fks[off_fk + out_idx];
         if (match) {
-            int in_idx = lowest_idx(match);
-            return (float)(1.0 / (double)fmaxf(1.0f, d.h->tuples[in_idx]));
+            return d.h->fksel[lowest_idx(match)];
         }
         tmp &= ~out_id;
     }
@@ -310,8 +312,9 @@ __device__ __forceinline__ float ec_selectivity(const DevInfoView &d, int i, uin
 // one pass; each quantity is accumulated in the reference's class order, so
 // every float result is the reference's.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
-                                            const RelVal &r) {
+template <bool MASKED>
+__device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
+                                              const RelVal &r, uint32_t ec_mask) {
     const DevHeader &h = *d.h;
     const bool inner_single = (R & (R - 1u)) == 0u;
     // the hash table size depends on the inner side only; needed by the
@@ -325,7 +328,14 @@ __device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, co
     bool inner_unique = false, any_index = false;
     float bucketsize = 1.0f, mcvfreq = 1.0f;
     const int n_ec = h.n_ec;
-    for (int i = 0; i < n_ec; i++) {
+    // MASKED: only the classes in ec_mask can match (classes on the split
+    // edge of a tree-shaped query); visited in increasing class order
+    uint32_t mrem = ec_mask;
+    for (int i = 0; MASKED ? (mrem != 0u) : (i < n_ec); i++) {
+        if (MASKED) {
+            i = __ffs(mrem) - 1;
+            mrem &= mrem - 1u;
+        }
         uint32_t ec = d.ec_relids[i];
         uint32_t ml = ec & L, mr = ec & R;
         if (!ml || !mr) continue;
@@ -372,7 +382,12 @@ __device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, co
     }
     if (any_index && !((h.composite_mask >> lowest_idx(R)) & 1u)) {
         extra.indexed_join_quals = true;
-        for (int i = 0; i < n_ec; i++) {
+        uint32_t mrem2 = ec_mask;
+        for (int i = 0; MASKED ? (mrem2 != 0u) : (i < n_ec); i++) {
+            if (MASKED) {
+                i = __ffs(mrem2) - 1;
+                mrem2 &= mrem2 - 1u;
+            }
             uint32_t ec = d.ec_relids[i];
             uint32_t ml = ec & L, mr = ec & R;
             if (!ml || !mr) continue;
@@ -389,19 +404,28 @@ __device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, co
     return out;
 }
 
+__device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
+                                            const RelVal &r) {
+    return join_eval_t<false>(d, L, l, R, r, 0u);
+}
+
 // ---------------------------------------------------------------------------
 // Biconnected blocks of a connected set, in the output order of the
 // reference's iterative Hopcroft-Tarjan (gpuqo_cpu_dpsub_bicc.cu:65-170):
 // DFS from the lowest relation, neighbours in increasing index order, a block
 // emitted when returning from child v to u with low[v] >= disc[u].  A vertex
 // stack replaces the reference's edge stack; both yield the same vertex sets
-// in the same order.  Returns the number of blocks; prefix[b] = number of
-// candidate pairs in blocks < b (each block b contributes 2^|b| - 2).
+// in the same order.  prefix[b] = number of candidate pairs in blocks < b
+// (each block b contributes 2^|b| - 2); sub[b] = vertices of the DFS subtree
+// of the block's child end v.  For a 2-vertex block {u, v} (a bridge) the two
+// sides of the split are exactly sub[b] and S - sub[b], which is what the
+// reference's grow() calls return for it (gpuqo_cpu_dpsub_bicc.cu:188-195).
 // ---------------------------------------------------------------------------
 struct Blocks {
     int nb;
     uint32_t total;               // sum of 2^|b| - 2
     uint32_t mask[kMaxRels];
+    uint32_t sub[kMaxRels];
     uint32_t prefix[kMaxRels + 1];
 };
 
@@ -409,6 +433,7 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
     uint8_t disc[kMaxRels], low[kMaxRels], parent[kMaxRels];
     uint8_t stk_u[kMaxRels];
     uint32_t stk_e[kMaxRels];
+    uint32_t desc[kMaxRels];
     uint8_t vstk[kMaxRels];
     int sp = 0, vsp = 0, t = 0;
     uint32_t visited = 0;
@@ -419,6 +444,7 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
     disc[root] = (uint8_t)t++;
     low[root] = 255;
     parent[root] = 255;
+    desc[root] = 1u << root;
     vstk[vsp++] = (uint8_t)root;
     stk_u[sp] = (uint8_t)root;
     stk_e[sp] = adj[root] & S;
@@ -438,10 +464,12 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
                         blk |= 1u << w;
                     } while (w != u);
                     B.prefix[B.nb] = B.total;
+                    B.sub[B.nb] = desc[u];
                     B.mask[B.nb++] = blk;
                     B.total += (1u << popc(blk)) - 2u;
                 }
                 if (low[u] < low[p]) low[p] = low[u];
+                desc[p] |= desc[u];
                 stk_e[sp - 1] &= ~(1u << u);
             }
             continue;
@@ -452,6 +480,7 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
             parent[v] = (uint8_t)u;
             disc[v] = (uint8_t)t++;
             low[v] = 255;
+            desc[v] = 1u << v;
             vstk[vsp++] = (uint8_t)v;
             stk_u[sp] = (uint8_t)v;
             stk_e[sp] = adj[v] & S;
@@ -464,6 +493,35 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
         }
     }
     B.prefix[B.nb] = B.total;
+}
+
+// Candidate p (0-based, reference enumeration order) of set S with blocks B:
+// the block subset lb is the (p - prefix[b] + 1)-th subset of block b in
+// nextSubset order; left/right are the reference's grow() results.
+// `b` is the caller's cursor (p must not decrease between calls).
+__device__ __forceinline__ bool mpdp_candidate(uint32_t S, const Blocks &B, const uint32_t *adj, uint32_t p, int &b,
+                                               uint32_t &L, uint32_t &R) {
+    while (b + 1 < B.nb && B.prefix[b + 1] <= p) b++;
+    const uint32_t blk = B.mask[b];
+    const uint32_t kk = p - B.prefix[b] + 1u;
+    if (popc(blk) == 2) {
+        // bridge {u, v}: kk = 1 -> lb = lowest vertex, kk = 2 -> the other
+        const uint32_t lo = lowest(blk);
+        const uint32_t lb = (kk == 1u) ? lo : (blk ^ lo);
+        const uint32_t sub = B.sub[b];
+        if (lb & sub) {
+            L = sub;
+            R = S ^ sub;
+        } else {
+            L = S ^ sub;
+            R = sub;
+        }
+        return true;
+    }
+    const uint32_t lb = pdep32(kk, blk), rb = blk ^ lb;
+    L = grow(lowest(lb), S & ~rb, adj);
+    R = grow(lowest(rb), S & ~lb, adj);
+    return (L | R) == S;
 }
 
 }  // namespace gqb

@@ -31,6 +31,7 @@ struct EngineStats {
     double eval_kernel_ms = 0.0;
     uint32_t eval_kernel_launches = 0;
     uint32_t kernel_launches = 0;
+    uint32_t fallback_sets = 0;
 };
 
 // Runs one exact DP on the calling thread's current device.  `blob` is the

@@ -61,6 +61,8 @@ struct LevelCounters {
     uint32_t n_sets;                   // connected sets found by k_filter
     uint32_t chunk_next;               // overflow work counter
     unsigned long long ovf_packed;     // (n_ovf << 40) | n_chunks
+    uint32_t n_fb;                     // sets sent to the exact-order fallback
+    uint32_t pad;
 };
 
 struct GlobalCounters {
@@ -71,6 +73,8 @@ struct DevArena {
     float4 *memo = nullptr;            // [2^n] rows, startup, total, width bits
     uint32_t *memo_left = nullptr;     // [2^n] left (outer) set of the best join
     uint32_t *sets = nullptr;          // [maxC] connected sets of the current level
+    uint32_t *sets2 = nullptr;         // [maxC] second level list (levels alternate)
+    uint32_t *seen = nullptr;          // [2^n bits] extension dedup bitmap
     uint32_t *ovf_set = nullptr;       // [maxC]
     uint32_t *ovf_P = nullptr;         // [maxC]
     uint32_t *ovf_off = nullptr;       // [maxC] first chunk id
@@ -143,6 +147,109 @@ __global__ void __launch_bounds__(kBlock) k_filter(const uint32_t *__restrict__ 
             __syncwarp();
         }
         if (has && r + 1 < r1) s = gosper_next(s);
+    }
+    if (cnt > 0) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&lc->n_sets, cnt);
+        base = __shfl_sync(kFull, base, 0);
+        if (lane < cnt) out_sets[base + lane] = st[lane];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_level_sets: the connected k-sets, by whichever enumeration is cheaper for
+// this level (decided on the device from the previous level's count):
+//   * extension: every connected (k-1)-set plus each of its neighbours; a
+//     test-and-set bitmap over all 2^n sets keeps the first producer of each
+//     k-set (work ~ count(k-1) * |neighbours|, for sparse graphs far below
+//     C(n,k));
+//   * filter: combinadic unrank + Gosper stepping over all C(n,k) subsets with
+//     the connectivity test (as k_filter; dense graphs).
+// Both produce the same set of connected k-sets; their order in the level list
+// does not affect the result (each set's best join is computed independently).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_level_sets(const uint32_t *__restrict__ blob,
+                                                       const uint32_t *__restrict__ binom_g, int n, int k,
+                                                       unsigned long long total, uint32_t per_thread,
+                                                       const uint32_t *__restrict__ prev_sets,
+                                                       const LevelCounters *__restrict__ prev_lc,
+                                                       uint32_t *__restrict__ bitmap, uint32_t *__restrict__ out_sets,
+                                                       LevelCounters *__restrict__ lc) {
+    __shared__ uint32_t adj[kMaxRels];
+    __shared__ uint32_t binom[33 * 33];
+    __shared__ uint32_t stage[kWarpsPerBlock][64];
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob);
+    for (int i = threadIdx.x; i < kMaxRels; i += blockDim.x) adj[i] = (i < n) ? h->adj[i] : 0u;
+    for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) binom[i] = binom_g[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *st = stage[warp];
+    uint32_t cnt = 0;
+    const uint32_t c_prev = (k == 2) ? (uint32_t)n : prev_lc->n_sets;
+    // per candidate the extension costs a neighbourhood scan share plus one
+    // L2 atomic; the filter a Gosper step plus a short connectivity test
+    const bool use_ext = (uint64_t)c_prev * (uint64_t)(k + 4 * (n - k + 1)) < total * 3ull;
+    auto emit = [&](bool ok, uint32_t s) {
+        uint32_t m = __ballot_sync(kFull, ok);
+        if (ok) st[cnt + __popc(m & ((1u << lane) - 1u))] = s;
+        cnt += __popc(m);
+        __syncwarp();
+        if (cnt >= 32) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&lc->n_sets, 32u);
+            base = __shfl_sync(kFull, base, 0);
+            out_sets[base + lane] = st[lane];
+            __syncwarp();
+            if (lane < cnt - 32) st[lane] = st[32 + lane];
+            cnt -= 32;
+            __syncwarp();
+        }
+    };
+    if (use_ext) {
+        const uint32_t nthreads = gridDim.x * blockDim.x;
+        const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+        // warp-uniform trip count over the previous level
+        const uint32_t rounds = (c_prev + nthreads - 1u) / nthreads;
+        for (uint32_t r = 0; r < rounds; r++) {
+            const uint32_t idx = tid + r * nthreads;
+            uint32_t S = 0u, N = 0u;
+            if (idx < c_prev) {
+                S = (k == 2) ? (1u << idx) : prev_sets[idx];
+                uint32_t x = S;
+                while (x) {
+                    int v = __ffs(x) - 1;
+                    x &= x - 1u;
+                    N |= adj[v];
+                }
+                N &= ~S;
+            }
+            const int deg = __popc(N);
+            const int maxdeg = (int)__reduce_max_sync(kFull, (uint32_t)deg);
+            for (int j = 0; j < maxdeg; j++) {
+                bool ok = false;
+                uint32_t T = 0u;
+                if (j < deg) {
+                    const uint32_t bitv = N & (0u - N);
+                    N ^= bitv;
+                    T = S | bitv;
+                    const uint32_t bm = 1u << (T & 31u);
+                    ok = !(atomicOr(&bitmap[T >> 5], bm) & bm);
+                }
+                emit(ok, T);
+            }
+        }
+    } else {
+        uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        uint64_t r0 = tid * per_thread;
+        uint64_t r1 = r0 + per_thread < total ? r0 + per_thread : total;
+        uint32_t s = r0 < total ? unrank_ksubset(r0, n, k, binom) : 0u;
+        for (uint32_t j = 0; j < per_thread; j++) {
+            uint64_t r = r0 + j;
+            bool has = r < r1;
+            bool ok = has && is_connected(s, adj);
+            emit(ok, s);
+            if (has && r + 1 < r1) s = gosper_next(s);
+        }
     }
     if (cnt > 0) {
         uint32_t base = 0;
@@ -329,14 +436,16 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
                                                  uint32_t *__restrict__ ovf_off,
                                                  unsigned long long *__restrict__ ovf_key,
                                                  unsigned long long *__restrict__ ovf_first,
-                                                 GlobalCounters *__restrict__ glob, int ccc) {
+                                                 GlobalCounters *__restrict__ glob, int ccc,
+                                                 const uint32_t *__restrict__ count_ptr = nullptr) {
+    const uint32_t count = count_ptr ? *count_ptr : lc->n_sets;
+    if (count == 0u) return;
     extern __shared__ uint32_t sm[];
     load_blob_to_smem(blob, blob_words, sm);
     const DevInfoView d = make_view(sm);
     const uint32_t *adj = d.h->adj;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t *q = sm + ((blob_words + 3u) & ~3u) + warp * kQueueWords;
-    const uint32_t count = lc->n_sets;
     const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
     unsigned long long pairs = 0;
     Blocks B;
@@ -373,6 +482,285 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
             else memo_write(memo, memo_left, S, best.val, best.left);
         }
         pairs += best.n_valid;
+    }
+    pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
+    if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
+}
+
+// ---------------------------------------------------------------------------
+// k_eval_mpdp: MPDP with G lanes per connected set (32/G sets per warp).
+// G is picked on the device from the level's set count so that small levels
+// still fill the GPU and large levels do not pay the per-set block search 32
+// times per warp.  Lanes of a group take candidates p = g, g+G, ...; the loop
+// runs the warp's maximum trip count so the group reductions can use
+// full-warp shuffles.
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t *adj, uint32_t first_set,
+                                            uint32_t stride_sets, const uint32_t *sets, uint32_t count,
+                                            LevelCounters *lc, float4 *memo, uint32_t *memo_left,
+                                            uint32_t *ovf_set, uint32_t *ovf_P, uint32_t *ovf_off,
+                                            unsigned long long *ovf_key, unsigned long long *ovf_first,
+                                            unsigned long long &pairs) {
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G, gl = lane % G;
+    const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
+    Blocks B;
+    for (uint32_t base = first_set; base < count; base += stride_sets) {
+        const uint32_t i = base + (uint32_t)grp;
+        const bool has = i < count;
+        const uint32_t S = has ? sets[i] : 0u;
+        uint32_t P = 0;
+        B.nb = 0;
+        if (has) {
+            find_blocks(S, adj, B);
+            P = B.total;
+        }
+        __syncwarp();
+        const bool ovf = has && P > kOvfLimit;
+        if (ovf && gl == 0) {
+            uint32_t nch = (P + kChunk - 1u) / kChunk;
+            unsigned long long old = atomicAdd(&lc->ovf_packed, (1ull << 40) | (unsigned long long)nch);
+            uint32_t idx = (uint32_t)(old >> 40);
+            ovf_set[idx] = S;
+            ovf_P[idx] = P;
+            ovf_off[idx] = (uint32_t)(old & 0xFFFFFFFFFFull);
+            ovf_key[idx] = ~0ull;
+            ovf_first[idx] = ~0ull;
+        }
+        const uint32_t myP = (has && !ovf) ? P : 0u;
+        const uint32_t iters = __reduce_max_sync(kFull, (myP + G - 1u) / G);
+        LaneBest best;
+        best.init();
+        int b = 0;
+        for (uint32_t it = 0; it < iters; it++) {
+            const uint32_t p = (uint32_t)gl + it * G;
+            if (p < myP) {
+                uint32_t L, R;
+                if (mpdp_candidate(S, B, adj, p, b, L, R)) evaluate_pair(d, memo, p, L, R, best);
+            }
+        }
+        // group reduction: min key, min first candidate (NaN rule)
+        uint32_t kh = (uint32_t)(best.key >> 32), kl = (uint32_t)best.key, fp = best.first_p;
+#pragma unroll
+        for (int off = G / 2; off >= 1; off >>= 1) {
+            uint32_t oh = __shfl_xor_sync(kFull, kh, off);
+            uint32_t ol = __shfl_xor_sync(kFull, kl, off);
+            uint32_t of = __shfl_xor_sync(kFull, fp, off);
+            if (oh < kh || (oh == kh && ol < kl)) {
+                kh = oh;
+                kl = ol;
+            }
+            if (of < fp) fp = of;
+        }
+        const bool nan_first = has && !ovf && best.first_p == fp && best.first_nan;
+        const unsigned nm = __ballot_sync(kFull, nan_first) & group_mask;
+        const unsigned long long gkey = ((unsigned long long)kh << 32) | kl;
+        if (has && !ovf) {
+            if (nm) {
+                if (nan_first) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
+            } else if (best.key == gkey && best.key != ~0ull) {
+                memo_write(memo, memo_left, S, best.val, best.left);
+            }
+        }
+        pairs += best.n_valid;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_eval_mpdp(const uint32_t *__restrict__ blob, uint32_t blob_words,
+                                                      const uint32_t *__restrict__ sets,
+                                                      LevelCounters *__restrict__ lc, float4 *__restrict__ memo,
+                                                      uint32_t *__restrict__ memo_left, uint32_t *__restrict__ ovf_set,
+                                                      uint32_t *__restrict__ ovf_P, uint32_t *__restrict__ ovf_off,
+                                                      unsigned long long *__restrict__ ovf_key,
+                                                      unsigned long long *__restrict__ ovf_first,
+                                                      GlobalCounters *__restrict__ glob, uint32_t target_lanes,
+                                                      int max_group) {
+    extern __shared__ uint32_t sm[];
+    load_blob_to_smem(blob, blob_words, sm);
+    const DevInfoView d = make_view(sm);
+    const uint32_t *adj = d.h->adj;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t count = lc->n_sets;
+    // lanes per set: enough lanes in flight to fill the GPU, no more than the
+    // largest useful group for this level
+    int G = 1;
+    while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
+    const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
+    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
+    unsigned long long pairs = 0;
+    switch (G) {
+#define GQB_G(g)                                                                                                  \
+    case g:                                                                                                       \
+        mpdp_groups<g>(d, adj, gwarp * (32 / g), nwarps * (32 / g), sets, count, lc, memo, memo_left, ovf_set,   \
+                       ovf_P, ovf_off, ovf_key, ovf_first, pairs);                                                \
+        break;
+        GQB_G(1)
+        GQB_G(2)
+        GQB_G(4)
+        GQB_G(8)
+        GQB_G(16)
+        GQB_G(32)
+#undef GQB_G
+    default:
+        break;
+    }
+    pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
+    if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
+}
+
+// ---------------------------------------------------------------------------
+// k_eval_tree: MPDP on a tree-shaped query graph (star, snowflake, chain).
+// Every connected set S is a subtree rooted at its lowest relation, every
+// block a bridge (parent a, child b), and the 2(k-1) candidates are the two
+// orientations of each edge: removing it leaves S & tsub[b] and the rest, so
+// no DFS is needed.  The reference's enumeration index of a candidate is
+// 2 * post(b) + side, where post(b) is b's post-order rank in S's DFS (the
+// order in which the reference emits blocks) and side 0 is lb = {a}:
+//     post(b) = |S & tbefore[b]| - |S & tanc[b]| + |S & tsub[b]| - 1
+// (preorder rank minus depth plus subtree size minus one; S's DFS visits S in
+// the query tree's preorder).  With ec_masked only the classes on edge (a, b)
+// can match.
+// ---------------------------------------------------------------------------
+struct EdgeIter {
+    uint32_t vs;      // vertices of S not yet started
+    uint32_t nb;      // remaining higher neighbours of v
+    int v;
+    uint32_t e;       // index of the next edge to be returned
+};
+
+__device__ __forceinline__ void edge_next(const uint32_t *adj, uint32_t S, EdgeIter &it, int &a, int &b) {
+    while (it.nb == 0u) {
+        it.v = __ffs(it.vs) - 1;
+        it.vs &= it.vs - 1u;
+        it.nb = adj[it.v] & S & ~((2u << it.v) - 1u);
+    }
+    a = it.v;
+    b = __ffs(it.nb) - 1;
+    it.nb &= it.nb - 1u;
+    it.e++;
+}
+
+template <int G, bool MASKED>
+__device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first_set, uint32_t stride_sets,
+                                            const uint32_t *sets, uint32_t count, int k, float4 *memo,
+                                            uint32_t *memo_left, unsigned long long &pairs) {
+    const DevHeader &h = *d.h;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G, gl = lane % G;
+    const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
+    const uint32_t P = 2u * (uint32_t)(k - 1);
+    const uint32_t per_lane = (P + G - 1u) / G;
+    for (uint32_t base = first_set; base < count; base += stride_sets) {
+        const uint32_t i = base + (uint32_t)grp;
+        const bool has = i < count;
+        const uint32_t S = has ? sets[i] : 0u;
+        EdgeIter it;
+        it.vs = S;
+        it.nb = 0u;
+        it.v = 0;
+        it.e = 0u;
+        int a = 0, b = 0;
+        LaneBest best;
+        best.init();
+        for (uint32_t j = 0; j < per_lane; j++) {
+            const uint32_t c = (uint32_t)gl + j * G;
+            const bool active = has && c < P;
+            if (active) {
+                const uint32_t target = c >> 1;
+                while (it.e <= target) edge_next(h.adj, S, it, a, b);
+            }
+            if (active) {
+                // a < b: a is b's parent in the query tree
+                const uint32_t comp_b = S & h.tsub[b];
+                const uint32_t side = c & 1u;
+                const uint32_t L = side ? comp_b : (S ^ comp_b);
+                const uint32_t R = S ^ L;
+                const uint32_t post = (uint32_t)(__popc(S & h.tbefore[b]) - __popc(S & h.tanc[b]) +
+                                                 __popc(comp_b) - 1);
+                const uint32_t p = 2u * post + side;
+                RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+                RelVal out = join_eval_t<MASKED>(d, L, l, R, r, MASKED ? h.edge_ec[b] : 0u);
+                const bool nan = isnan(out.total);
+                best.n_valid++;
+                if (p < best.first_p) {
+                    best.first_p = p;
+                    best.first_nan = nan;
+                    if (nan) {
+                        best.nan_val = out;
+                        best.nan_left = L;
+                    }
+                }
+                if (!nan) {
+                    const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
+                    if (key < best.key) {
+                        best.key = key;
+                        best.val = out;
+                        best.left = L;
+                    }
+                }
+            }
+        }
+        uint32_t kh = (uint32_t)(best.key >> 32), kl = (uint32_t)best.key, fp = best.first_p;
+#pragma unroll
+        for (int off = G / 2; off >= 1; off >>= 1) {
+            uint32_t oh = __shfl_xor_sync(kFull, kh, off);
+            uint32_t ol = __shfl_xor_sync(kFull, kl, off);
+            uint32_t of = __shfl_xor_sync(kFull, fp, off);
+            if (oh < kh || (oh == kh && ol < kl)) {
+                kh = oh;
+                kl = ol;
+            }
+            if (of < fp) fp = of;
+        }
+        const bool nan_first = has && best.first_p == fp && best.first_nan;
+        const unsigned nm = __ballot_sync(kFull, nan_first) & group_mask;
+        const unsigned long long gkey = ((unsigned long long)kh << 32) | kl;
+        if (has) {
+            if (nm) {
+                if (nan_first) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
+            } else if (best.key == gkey && best.key != ~0ull) {
+                memo_write(memo, memo_left, S, best.val, best.left);
+            }
+        }
+        pairs += best.n_valid;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_eval_tree(const uint32_t *__restrict__ blob, uint32_t blob_words, int k,
+                                                      const uint32_t *__restrict__ sets,
+                                                      LevelCounters *__restrict__ lc, float4 *__restrict__ memo,
+                                                      uint32_t *__restrict__ memo_left,
+                                                      GlobalCounters *__restrict__ glob, uint32_t target_lanes,
+                                                      int max_group) {
+    extern __shared__ uint32_t sm[];
+    load_blob_to_smem(blob, blob_words, sm);
+    const DevInfoView d = make_view(sm);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t count = lc->n_sets;
+    int G = 1;
+    while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
+    const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
+    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
+    const bool masked = d.h->ec_masked != 0u;
+    unsigned long long pairs = 0;
+    switch (G * 2 + (masked ? 1 : 0)) {
+#define GQB_T(g)                                                                                                 \
+    case 2 * g:                                                                                                  \
+        tree_groups<g, false>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo, memo_left, pairs);   \
+        break;                                                                                                   \
+    case 2 * g + 1:                                                                                              \
+        tree_groups<g, true>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo, memo_left, pairs);    \
+        break;
+        GQB_T(1)
+        GQB_T(2)
+        GQB_T(4)
+        GQB_T(8)
+        GQB_T(16)
+        GQB_T(32)
+#undef GQB_T
+    default:
+        break;
     }
     pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
     if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
@@ -648,6 +1036,8 @@ public:
         cudaFree(a.memo);
         cudaFree(a.memo_left);
         cudaFree(a.sets);
+        cudaFree(a.sets2);
+        cudaFree(a.seen);
         cudaFree(a.ovf_set);
         cudaFree(a.ovf_P);
         cudaFree(a.ovf_off);
@@ -660,6 +1050,8 @@ public:
         CK(cudaMalloc(&a.memo, slots * sizeof(float4)));
         CK(cudaMalloc(&a.memo_left, slots * sizeof(uint32_t)));
         CK(cudaMalloc(&a.sets, ms * sizeof(uint32_t)));
+        CK(cudaMalloc(&a.sets2, ms * sizeof(uint32_t)));
+        CK(cudaMalloc(&a.seen, std::max<uint64_t>(slots / 8, 4)));
         CK(cudaMalloc(&a.ovf_set, ms * sizeof(uint32_t)));
         CK(cudaMalloc(&a.ovf_P, ms * sizeof(uint32_t)));
         CK(cudaMalloc(&a.ovf_off, ms * sizeof(uint32_t)));
@@ -677,9 +1069,12 @@ public:
     // Enqueues the whole DP for n relations on `stream`.
     int enqueue(int n, DpMode mode, bool ccc, bool profile, uint32_t blob_words, std::string &err) {
         const size_t smem = eval_smem(blob_words);
+        const uint32_t max_block = reinterpret_cast<const DevHeader *>(h_blob)->max_block;
+        const bool tree_mode = reinterpret_cast<const DevHeader *>(h_blob)->tree_mode != 0u;
         const int eval_max_blocks = sm_count * 4;
         CK(cudaMemsetAsync(a.lvl, 0, 33 * sizeof(LevelCounters), stream));
         CK(cudaMemsetAsync(a.glob, 0, sizeof(GlobalCounters), stream));
+        CK(cudaMemsetAsync(a.seen, 0, std::max<uint64_t>((1ull << n) / 8, 4), stream));
         n_kernels = 0;
         k_init_base<<<1, 32, 0, stream>>>(a.blob, a.memo, a.memo_left);
         n_kernels++;
@@ -691,22 +1086,44 @@ public:
             uint32_t per_thread = (uint32_t)((total + threads - 1) / threads);
             uint32_t fblocks = (uint32_t)((total + (uint64_t)per_thread * kBlock - 1) / ((uint64_t)per_thread * kBlock));
             LevelCounters *lc = a.lvl + k;
-            k_filter<<<fblocks, kBlock, 0, stream>>>(a.blob, a.binom, n, k, total, per_thread, a.sets, lc);
+            uint32_t *cur_sets = (k & 1) ? a.sets2 : a.sets;
+            const uint32_t *prev_sets = (k & 1) ? a.sets : a.sets2;
+            k_level_sets<<<fblocks, kBlock, 0, stream>>>(a.blob, a.binom, n, k, total, per_thread, prev_sets,
+                                                         a.lvl + (k - 1), a.seen, cur_sets, lc);
             n_kernels += 2;
             int eblocks = (int)std::min<uint64_t>((uint64_t)eval_max_blocks, (total + kWarpsPerBlock - 1) / kWarpsPerBlock);
             CK(cudaEventRecordWithFlags(kev[2 * k], stream, cudaEventRecordExternal));
             if (mode == kModeDpsub) {
-                k_eval<kModeDpsub><<<eblocks, kBlock, smem, stream>>>(a.blob, blob_words, k, a.sets, lc, a.memo,
+                k_eval<kModeDpsub><<<eblocks, kBlock, smem, stream>>>(a.blob, blob_words, k, cur_sets, lc, a.memo,
                                                                       a.memo_left, a.ovf_set, a.ovf_P, a.ovf_off,
                                                                       a.ovf_key, a.ovf_first, a.glob, ccc);
             } else {
-                k_eval<kModeMpdp><<<eblocks, kBlock, smem, stream>>>(a.blob, blob_words, k, a.sets, lc, a.memo,
-                                                                     a.memo_left, a.ovf_set, a.ovf_P, a.ovf_off,
-                                                                     a.ovf_key, a.ovf_first, a.glob, ccc);
+                // max useful group: pairs of a k-set are at least 2(k-1)
+                int max_group = 1;
+                while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
+                const uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
+                int mblocks = (int)std::min<uint64_t>((uint64_t)sm_count * 4, (total * 32 + kBlock - 1) / kBlock);
+                if (tree_mode) {
+                    k_eval_tree<<<mblocks, kBlock, smem, stream>>>(a.blob, blob_words, k, cur_sets, lc, a.memo,
+                                                                   a.memo_left, a.glob, target_lanes, max_group);
+                } else {
+                    k_eval_mpdp<<<mblocks, kBlock, smem, stream>>>(a.blob, blob_words, cur_sets, lc, a.memo,
+                                                                   a.memo_left, a.ovf_set, a.ovf_P, a.ovf_off,
+                                                                   a.ovf_key, a.ovf_first, a.glob, target_lanes,
+                                                                   max_group);
+                }
             }
             CK(cudaEventRecordWithFlags(kev[2 * k + 1], stream, cudaEventRecordExternal));
-            bool may_overflow = (mode == kModeDpsub) ? (((1ull << k) - 2ull) > kOvfLimit)
-                                                     : (((1ull << k) - 2ull) > kOvfLimit);
+            bool may_overflow;
+            if (mode == kModeDpsub) {
+                may_overflow = ((1ull << k) - 2ull) > kOvfLimit;
+            } else {
+                // sum over blocks of 2^|b| - 2 with sum(|b| - 1) = k - 1 and
+                // |b| <= the query graph's largest block
+                int bmax = std::min<int>(std::max<int>((int)max_block, 2), k);
+                uint64_t nblk = (uint64_t)(k - 1 + bmax - 2) / (uint64_t)(bmax - 1);
+                may_overflow = nblk * ((1ull << bmax) - 2ull) > kOvfLimit;
+            }
             if (may_overflow) {
                 n_kernels += 2;
                 int oblocks = sm_count * 4;
@@ -760,7 +1177,10 @@ public:
         }
         CK(cudaMemcpyAsync(a.blob, h_blob, words * 4, cudaMemcpyHostToDevice, stream));
         exec = nullptr;
-        GraphKey key{n, (int)mode, ccc ? 1 : 0, (int)words};
+        const uint32_t mb = reinterpret_cast<const DevHeader *>(h_blob)->max_block;
+        const uint32_t tm = reinterpret_cast<const DevHeader *>(h_blob)->tree_mode;
+        GraphKey key{n, ((int)mode * 64 + (int)std::min<uint32_t>(mb, 63u)) * 2 + (int)(tm != 0u), ccc ? 1 : 0,
+                     (int)words};
         (void)profile;
         auto it = graphs.find(key);
         if (it != graphs.end()) {
@@ -821,6 +1241,7 @@ public:
         for (int k = 2; k <= n; k++) {
             csgs += h_lvl[k].n_sets;
             filt += binom64(n, k);
+            st.fallback_sets += h_lvl[k].n_fb;
         }
         st.connected_sets += csgs;
         st.filtered_subsets += filt;
@@ -1080,6 +1501,8 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         h->startup[t] = b.cost.startup;
         h->total[t] = b.cost.total;
         h->width[t] = b.width;
+        h->fksel[t] = (float)(1.0 / (double)fmaxf(1.0f, b.tuples));
+        h->tparent[t] = -1;
     }
     DevInfoView v = make_view(blob);
     uint32_t *relids = const_cast<uint32_t *>(v.ec_relids);

@@ -34,13 +34,27 @@ struct DevHeader {
     int work_mem, enable_nestloop, enable_hashjoin;
     uint32_t composite_mask;
     uint32_t blob_words;                  // total blob size in 32-bit words
-    uint32_t pad[3];
+    uint32_t max_block;                   // largest biconnected block of the query graph
+    uint32_t tree_mode;                   // query graph is a tree (tparent/tsub valid)
+    uint32_t ec_masked;                   // tree_mode and every class is a 2-member class on an edge
     uint32_t adj[kMaxRels];
     float rows[kMaxRels];
     float tuples[kMaxRels];
     float startup[kMaxRels];
     float total[kMaxRels];
     int width[kMaxRels];
+    // fkselc_of_ec's value for a foreign key into relation i:
+    // (float)(1.0 / (double)fmaxf(1.0f, tuples[i])) (gpuqo_row_estimation.cuh:36-38)
+    float fksel[kMaxRels];
+    // tree_mode: parent of relation i in the query tree rooted at relation 0,
+    // relations of the subtree under i, and the classes on edge (parent, i)
+    int tparent[kMaxRels];
+    uint32_t tsub[kMaxRels];
+    uint32_t edge_ec[kMaxRels];
+    // tree_mode: relations before i in the query tree's preorder (children
+    // visited in increasing index order) and the proper ancestors of i
+    uint32_t tbefore[kMaxRels];
+    uint32_t tanc[kMaxRels];
 };
 
 struct DevInfoView {

@@ -4,6 +4,8 @@
 // The flow of one call mirrors __gpuqo_run (gpuqo_main_internal.cu:82-160):
 // convert -> BFS relabel -> exact DP (or IDP driver) -> map the plan back ->
 // palloc'd QueryTreeC.  The exact DP runs on the GPU (dp_kernels.cu).
+#include <algorithm>
+#include <cmath>
 #include <csignal>
 #include <cstdio>
 #include <cstdlib>
@@ -97,6 +99,7 @@ void stats_add(const EngineStats &s) {
     t_stats.eval_kernel_ms += s.eval_kernel_ms;
     t_stats.eval_kernel_launches += s.eval_kernel_launches;
     t_stats.kernel_launches += s.kernel_launches;
+    t_stats.fallback_sets += s.fallback_sets;
     t_stats.n_subproblems += 1;
 }
 
@@ -266,6 +269,62 @@ HostInfo relabel(const HostInfo &from, const std::vector<int> &from_of_to) {
     return to;
 }
 
+// Size of the largest biconnected block of the query graph (Hopcroft-Tarjan
+// over compact adjacency masks).  Every block of a connected subset lies
+// inside a block of the whole graph, so this bounds the MPDP candidate count
+// of every set: sum over blocks of 2^|b| - 2 with sum(|b| - 1) = |S| - 1.
+static int max_block_size(const HostInfo &info) {
+    const int n = info.n;
+    if (n <= 1) return n;
+    std::vector<uint32_t> adj(n);
+    for (int i = 0; i < n; i++) adj[i] = (uint32_t)(info.edge[i] >> 1);
+    std::vector<int> disc(n, -1), low(n, 0), parent(n, -1), vstk, stk_u;
+    std::vector<uint32_t> stk_e;
+    int t = 0, best = 1;
+    for (int root = 0; root < n; root++) {
+        if (disc[root] >= 0) continue;
+        disc[root] = low[root] = t++;
+        vstk.push_back(root);
+        stk_u.push_back(root);
+        stk_e.push_back(adj[root]);
+        while (!stk_u.empty()) {
+            int u = stk_u.back();
+            uint32_t e = stk_e.back();
+            if (!e) {
+                stk_u.pop_back();
+                stk_e.pop_back();
+                if (!stk_u.empty()) {
+                    int p = stk_u.back();
+                    if (low[u] >= disc[p]) {
+                        int size = 1, w;
+                        do {
+                            w = vstk.back();
+                            vstk.pop_back();
+                            size++;
+                        } while (w != u);
+                        best = std::max(best, size);
+                    }
+                    low[p] = std::min(low[p], low[u]);
+                }
+                continue;
+            }
+            int v = __builtin_ffs((int)e) - 1;
+            stk_e.back() = e & ~(1u << v);
+            if (disc[v] < 0) {
+                parent[v] = u;
+                disc[v] = low[v] = t++;
+                vstk.push_back(v);
+                stk_u.push_back(v);
+                stk_e.push_back(adj[v]);
+            } else if (v != parent[u]) {
+                low[u] = std::min(low[u], disc[v]);
+            }
+        }
+        vstk.clear();
+    }
+    return best;
+}
+
 std::vector<uint32_t> build_blob(const HostInfo &info) {
     const int n_ec = (int)info.ec_relids.size();
     const int n_sels = (int)info.ec_sels.size();
@@ -285,6 +344,7 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     h->enable_hashjoin = info.p.enable_hashjoin ? 1 : 0;
     h->composite_mask = 0;
     h->blob_words = (uint32_t)blob.size();
+    h->max_block = (uint32_t)max_block_size(info);
     for (int i = 0; i < info.n; i++) {
         h->adj[i] = (uint32_t)(info.edge[i] >> 1);
         h->rows[i] = info.base[i].rows;
@@ -292,7 +352,66 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         h->startup[i] = info.base[i].cost.startup;
         h->total[i] = info.base[i].cost.total;
         h->width[i] = info.base[i].width;
+        h->fksel[i] = (float)(1.0 / (double)std::fmax(1.0f, info.base[i].tuples));
         if (info.base[i].composite) h->composite_mask |= 1u << i;
+    }
+    // Tree-shaped query graph (after BFS relabelling, every relation's parent
+    // is its only neighbour with a smaller index): parents, subtree masks and
+    // the classes sitting on each edge.
+    int n_edges = 0;
+    for (int i = 0; i < info.n; i++) n_edges += popc64(info.edge[i]);
+    n_edges /= 2;
+    bool tree = (n_edges == info.n - 1);
+    for (int i = 1; tree && i < info.n; i++) {
+        uint32_t lower = h->adj[i] & ((1u << i) - 1u);
+        if (popc64(lower) != 1) tree = false;
+        else h->tparent[i] = __builtin_ctz(lower);
+    }
+    h->tparent[0] = -1;
+    h->tree_mode = tree ? 1u : 0u;
+    h->ec_masked = 0u;
+    if (tree) {
+        for (int i = info.n - 1; i >= 0; i--) {
+            h->tsub[i] |= 1u << i;
+            if (i > 0) h->tsub[h->tparent[i]] |= h->tsub[i];
+        }
+        // preorder from relation 0, children in increasing index order (the
+        // order in which the reference's block search walks any subtree)
+        {
+            std::vector<int> stack(1, 0);
+            uint32_t seen_before = 0u;
+            while (!stack.empty()) {
+                int u = stack.back();
+                stack.pop_back();
+                h->tbefore[u] = seen_before;
+                seen_before |= 1u << u;
+                h->tanc[u] = (u == 0) ? 0u : (h->tanc[h->tparent[u]] | (1u << h->tparent[u]));
+                uint32_t kids = h->adj[u] & ~((2u << u) - 1u);   // children have larger indices
+                std::vector<int> ch;
+                while (kids) {
+                    ch.push_back(__builtin_ctz(kids));
+                    kids &= kids - 1u;
+                }
+                for (auto it = ch.rbegin(); it != ch.rend(); ++it) stack.push_back(*it);
+            }
+        }
+        bool masked = n_ec <= 32;
+        for (int e = 0; masked && e < n_ec; e++) {
+            uint32_t r = (uint32_t)(info.ec_relids[e] >> 1);
+            if (popc64(r) != 2) {
+                masked = false;
+                break;
+            }
+            int a = __builtin_ctz(r), b = 31 - __builtin_clz(r);   // a < b
+            if (h->tparent[b] != a) {
+                masked = false;   // a class between relations that are not adjacent
+                break;
+            }
+            h->edge_ec[b] |= 1u << e;
+        }
+        if (masked) h->ec_masked = 1u;
+        else
+            for (int i = 0; i < info.n; i++) h->edge_ec[i] = 0u;
     }
     DevInfoView v = make_view(blob.data());
     uint32_t *relids = const_cast<uint32_t *>(v.ec_relids);

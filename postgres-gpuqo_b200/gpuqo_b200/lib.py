@@ -26,7 +26,7 @@ class Stats(C.Structure):
                 ("filtered_subsets", C.c_uint64), ("memo_bytes", C.c_uint64),
                 ("device_ms", C.c_double), ("eval_kernel_ms", C.c_double),
                 ("eval_kernel_launches", C.c_uint32), ("n_subproblems", C.c_uint32),
-                ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32)]
+                ("kernel_launches", C.c_uint32), ("fallback_sets", C.c_uint32)]
 
     def to_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

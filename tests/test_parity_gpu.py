@@ -67,6 +67,21 @@ def test_random_vs_oracle(seed):
                 assert same_tree(got.tree, want), (q.name, alg, ccc)
 
 
+@pytest.mark.parametrize("seed", range(6))
+def test_tree_queries_with_ties(seed):
+    """Tree-shaped queries take the tree kernel; all-equal relations make
+    most costs tie, so most sets go through the exact-order fallback."""
+    qs = [query.random_graph(10 + seed, 7000 + seed, extra_edge_p=0.0, equal=True),
+          query.random_graph(12 + seed, 7100 + seed, extra_edge_p=0.0),
+          query.random_graph(13, 7200 + seed, extra_edge_p=0.0, rich=True),
+          query.star(8 + seed, 7300 + seed, rich=True),
+          query.chain(10 + seed, 7400 + seed)]
+    for q in qs:
+        want, _ = harness.run_port(q, 5)
+        got = gpu_run(q, 5)
+        assert same_tree(got.tree, want), q.name
+
+
 def test_overflow_path_large_sets():
     """Sets with more candidates than one warp's share take the chunked
     atomicMin path (clique levels >= 12 in DPsub); compare with the oracle."""
