@@ -57,7 +57,7 @@ def measured_peaks():
 
 def profiled_traffic():
     """DRAM bytes per k_eval launch from the committed ncu summary, if any."""
-    p = os.path.join(REPO, "profiles", "k_eval_mpdp_snowflake25.md")
+    p = os.path.join(REPO, "profiles", "k_eval_tree_snowflake25.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -282,7 +282,7 @@ def main():
             "pairs_per_s": pairs / (tot_ms / 1000.0) if tot_ms > 0 else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_eval<MPDP>", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None},
+                         "kernel": "k_eval_tree (MPDP)", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None},
             "e2e": {"value": e2e_value, "unit": "ms/query", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": kernels,

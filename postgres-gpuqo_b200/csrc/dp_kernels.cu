@@ -178,17 +178,21 @@ __global__ void __launch_bounds__(kBlock) k_level_sets(const uint32_t *__restric
     __shared__ uint32_t adj[kMaxRels];
     __shared__ uint32_t binom[33 * 33];
     __shared__ uint32_t stage[kWarpsPerBlock][64];
+    const uint32_t c_prev = (k == 2) ? (uint32_t)n : __ldcg(&prev_lc->n_sets);
+    // per candidate the extension costs a neighbourhood scan share plus one
+    // L2 atomic; the filter a Gosper step plus a short connectivity test
+    const bool use_ext = (uint64_t)c_prev * (uint64_t)(k + 4 * (n - k + 1)) < total * 3ull;
+    // the grid is sized for the filter; the extension needs one thread per
+    // set of the previous level, so surplus blocks leave at once
+    if (use_ext && (uint64_t)blockIdx.x * blockDim.x >= (uint64_t)c_prev) return;
     const DevHeader *h = reinterpret_cast<const DevHeader *>(blob);
     for (int i = threadIdx.x; i < kMaxRels; i += blockDim.x) adj[i] = (i < n) ? h->adj[i] : 0u;
-    for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) binom[i] = binom_g[i];
+    if (!use_ext)
+        for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) binom[i] = binom_g[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t *st = stage[warp];
     uint32_t cnt = 0;
-    const uint32_t c_prev = (k == 2) ? (uint32_t)n : prev_lc->n_sets;
-    // per candidate the extension costs a neighbourhood scan share plus one
-    // L2 atomic; the filter a Gosper step plus a short connectivity test
-    const bool use_ext = (uint64_t)c_prev * (uint64_t)(k + 4 * (n - k + 1)) < total * 3ull;
     auto emit = [&](bool ok, uint32_t s) {
         uint32_t m = __ballot_sync(kFull, ok);
         if (ok) st[cnt + __popc(m & ((1u << lane) - 1u))] = s;
@@ -206,7 +210,8 @@ __global__ void __launch_bounds__(kBlock) k_level_sets(const uint32_t *__restric
         }
     };
     if (use_ext) {
-        const uint32_t nthreads = gridDim.x * blockDim.x;
+        const uint32_t used_blocks = (uint32_t)min((uint64_t)gridDim.x, ((uint64_t)c_prev + blockDim.x - 1) / blockDim.x);
+        const uint32_t nthreads = used_blocks * blockDim.x;
         const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
         // warp-uniform trip count over the previous level
         const uint32_t rounds = (c_prev + nthreads - 1u) / nthreads;
@@ -727,7 +732,7 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_eval_tree(const uint32_t *__restrict__ blob, uint32_t blob_words, int k,
+__global__ void __launch_bounds__(kBlock, 4) k_eval_tree(const uint32_t *__restrict__ blob, uint32_t blob_words, int k,
                                                       const uint32_t *__restrict__ sets,
                                                       LevelCounters *__restrict__ lc, float4 *__restrict__ memo,
                                                       uint32_t *__restrict__ memo_left,
@@ -738,8 +743,11 @@ __global__ void __launch_bounds__(kBlock) k_eval_tree(const uint32_t *__restrict
     const DevInfoView d = make_view(sm);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t count = lc->n_sets;
-    int G = 1;
+    // group sizes 2, 8 or 32 (fewer instantiations keep the code in the
+    // instruction cache)
+    int G = 2;
     while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
+    G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
     const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
     const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
     const bool masked = d.h->ec_masked != 0u;
@@ -752,11 +760,8 @@ __global__ void __launch_bounds__(kBlock) k_eval_tree(const uint32_t *__restrict
     case 2 * g + 1:                                                                                              \
         tree_groups<g, true>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo, memo_left, pairs);    \
         break;
-        GQB_T(1)
         GQB_T(2)
-        GQB_T(4)
         GQB_T(8)
-        GQB_T(16)
         GQB_T(32)
 #undef GQB_T
     default:

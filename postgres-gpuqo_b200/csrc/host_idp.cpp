@@ -1,13 +1,872 @@
-// host_idp.cpp - IDP2 / UnionDP drivers (placeholder until the drivers land).
+// host_idp.cpp - IDP2 and UnionDP drivers over the GPU exact DP.
+//
+// Restates, on the host, the reference's iterative drivers and the machinery
+// they use, for queries of any size (relations up to kBigBits - 1):
+//   gpuqo_run_idp2 / _rec / find_most_expensive_subtree  gpuqo_idp.cu:96-297
+//   gpuqo_run_dpdp_union / _rec, DisjointSet, edge queues gpuqo_dpdp_union.cu:29-472
+//   gpuqo_cpu_goo (IDP2's seed plan)                      gpuqo_cpu_goo.cu:27-150
+//   Remapper (composite relations, re-estimated classes)  gpuqo_remapper.cu:34-300
+//   makeBFSIndexRemapper                                   gpuqo_bfs_indexing.cu:14-55
+//   estimate_join_rows/selectivity on plan nodes           gpuqo_row_estimation.cuh:26-148
+// Every sub-problem (at most 31 relations after remapping) is solved by the
+// GPU engine through exact_dp(), without a BFS relabelling, as the reference
+// calls gpuqo_run_switch on the remapped info.
+//
+// The remapper's lookups, which the reference performs by scanning its list
+// of entries, use an owner table instead (entries partition the relations,
+// so "entry e intersects id" is "some relation of id is owned by e"); results
+// are identical.  The heaps and priority queues are the same libstdc++
+// algorithms fed in the same order, so their tie behaviour is the reference's.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <queue>
+#include <string>
+#include <vector>
+
+#include "dp_engine.h"
+#include "gpuqo_b200.h"
 #include "host_idp.h"
+#include "host_info.h"
+
+extern "C" int gpuqo_idp_n_iters;
+extern "C" int gpuqo_idp_type;
+extern "C" void *palloc(size_t size);
+extern "C" void *palloc0(size_t size);
 
 namespace gqb {
 
-QueryTreeC *run_idp(int algorithm, GpuqoPlannerInfoC *info) {
-    (void)algorithm;
-    (void)info;
-    set_error(GPUQO_B200_ERR_UNSUPPORTED, "IDP drivers are not built yet");
-    return nullptr;
+int exact_dp(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, std::string &err);
+DpMode mode_for(int algorithm);
+
+// ---------------------------------------------------------------------------
+// fixed-capacity bitset with the reference's numbering (relation i = bit i+1)
+// ---------------------------------------------------------------------------
+constexpr int kBigWords = 16;
+constexpr int kBigBits = kBigWords * 64;
+
+struct BB {
+    std::array<uint64_t, kBigWords> w{};
+    static BB bit(int i) {
+        BB b;
+        b.w[i >> 6] = 1ull << (i & 63);
+        return b;
+    }
+    bool test(int i) const { return (w[i >> 6] >> (i & 63)) & 1ull; }
+    void set(int i) { w[i >> 6] |= 1ull << (i & 63); }
+    void unset(int i) { w[i >> 6] &= ~(1ull << (i & 63)); }
+    bool empty() const {
+        for (auto x : w)
+            if (x) return false;
+        return true;
+    }
+    int size() const {
+        int c = 0;
+        for (auto x : w) c += __builtin_popcountll(x);
+        return c;
+    }
+    int lowest_pos() const {
+        for (int i = 0; i < kBigWords; i++)
+            if (w[i]) return i * 64 + __builtin_ctzll(w[i]);
+        return -1;
+    }
+    BB lowest() const {
+        BB b;
+        int p = lowest_pos();
+        if (p >= 0) b.set(p);
+        return b;
+    }
+    // all bits below the lowest set bit (GpuqoBitmapset::allLower)
+    BB all_lower() const {
+        BB b;
+        int p = lowest_pos();
+        for (int i = 0; i < p; i++) b.set(i);
+        return b;
+    }
+    BB operator|(const BB &o) const {
+        BB r;
+        for (int i = 0; i < kBigWords; i++) r.w[i] = w[i] | o.w[i];
+        return r;
+    }
+    BB operator&(const BB &o) const {
+        BB r;
+        for (int i = 0; i < kBigWords; i++) r.w[i] = w[i] & o.w[i];
+        return r;
+    }
+    BB operator-(const BB &o) const {
+        BB r;
+        for (int i = 0; i < kBigWords; i++) r.w[i] = w[i] & ~o.w[i];
+        return r;
+    }
+    BB &operator|=(const BB &o) {
+        for (int i = 0; i < kBigWords; i++) w[i] |= o.w[i];
+        return *this;
+    }
+    BB &operator-=(const BB &o) {
+        for (int i = 0; i < kBigWords; i++) w[i] &= ~o.w[i];
+        return *this;
+    }
+    bool intersects(const BB &o) const {
+        for (int i = 0; i < kBigWords; i++)
+            if (w[i] & o.w[i]) return true;
+        return false;
+    }
+    bool is_subset_of(const BB &o) const {
+        for (int i = 0; i < kBigWords; i++)
+            if (w[i] & ~o.w[i]) return false;
+        return true;
+    }
+    bool operator==(const BB &o) const { return w == o.w; }
+    bool operator!=(const BB &o) const { return w != o.w; }
+    // integer order (Bitmapset32/64 compare bits; bms_compare compares from
+    // the highest word down)
+    bool operator<(const BB &o) const {
+        for (int i = kBigWords - 1; i >= 0; i--)
+            if (w[i] != o.w[i]) return w[i] < o.w[i];
+        return false;
+    }
+    template <class F> void for_each(F f) const {
+        for (int i = 0; i < kBigWords; i++) {
+            uint64_t x = w[i];
+            while (x) {
+                f(i * 64 + __builtin_ctzll(x));
+                x &= x - 1;
+            }
+        }
+    }
+};
+
+struct GBase {
+    BB id;
+    float rows, tuples;
+    int width;
+    PathCost cost;
+    bool composite;
+};
+
+struct GInfo {
+    int n = 0;
+    HostParams p;
+    std::vector<GBase> base;
+    std::vector<BB> edge;
+    std::vector<BB> ec;                // relids
+    std::vector<std::vector<int>> ec_members;  // relation indices (bit - 1), increasing
+    std::vector<float> sels;
+    std::vector<BB> fks;
+    std::vector<VarInfo> vars;
+    std::vector<int> ec_off_sels, ec_off_fks;
+    void index() {
+        ec_members.assign(ec.size(), {});
+        ec_off_sels.assign(ec.size(), 0);
+        ec_off_fks.assign(ec.size(), 0);
+        int os = 0, of = 0;
+        for (size_t i = 0; i < ec.size(); i++) {
+            ec.at(i).for_each([&](int b) { ec_members[i].push_back(b - 1); });
+            ec_off_sels[i] = os;
+            ec_off_fks[i] = of;
+            int s = (int)ec_members[i].size();
+            os += s * (s - 1) / 2;
+            of += s;
+        }
+    }
+};
+
+struct QT {
+    BB id;
+    float rows;
+    PathCost cost;
+    int width;
+    QT *left = nullptr, *right = nullptr;
+};
+
+// node arena of one gpuqo_run call (the reference's trees are freed piecemeal;
+// here they live until the call returns)
+struct Arena {
+    std::vector<std::unique_ptr<QT>> nodes;
+    QT *make() {
+        nodes.emplace_back(new QT());
+        return nodes.back().get();
+    }
+};
+
+static inline int ec_index(int l, int r, int size) {
+    if (l > r) std::swap(l, r);
+    return l * size - l * (l + 1) / 2 + (r - l - 1);
+}
+
+// ---------------------------------------------------------------------------
+// row estimation on arbitrary relation sets (gpuqo_row_estimation.cuh)
+// ---------------------------------------------------------------------------
+static bool ec_hits(const GInfo &g, int e, const BB &s) {
+    for (int m : g.ec_members[e])
+        if (s.test(m + 1)) return true;
+    return false;
+}
+
+// :26-45
+static float fkselc_of_ec(const GInfo &g, int e, const BB &outer, const BB &inner) {
+    BB tmp = outer;
+    const BB &ecr = g.ec[e];
+    while (!tmp.empty()) {
+        BB out_id = tmp.lowest();
+        int out_idx = (out_id.all_lower() & ecr).size();
+        BB match = inner & g.fks[g.ec_off_fks[e] + out_idx];
+        if (!match.empty()) {
+            int in_idx = match.lowest_pos() - 1;
+            return (float)(1.0 / (double)std::fmax(1.0f, g.base[in_idx].tuples));
+        }
+        tmp -= out_id;
+    }
+    return NAN;
+}
+
+// :49-88
+static float estimate_ec_selectivity(const GInfo &g, int e, const BB &l, const BB &r) {
+    const BB &ecr = g.ec[e];
+    int size = (int)g.ec_members[e].size();
+    BB ml = ecr & l, mr = ecr & r;
+    if (ml.empty() || mr.empty()) return 1.0f;
+    float fk = fkselc_of_ec(g, e, ml, mr);
+    if (!std::isnan(fk)) return fk;
+    fk = fkselc_of_ec(g, e, mr, ml);
+    if (!std::isnan(fk)) return fk;
+    int il = (ml.all_lower() & ecr).size();
+    int ir = (mr.all_lower() & ecr).size();
+    return g.sels[g.ec_off_sels[e] + ec_index(il, ir, size)];
+}
+
+// :93-118
+static float estimate_join_selectivity(const GInfo &g, const BB &l, const BB &r) {
+    float sel = 1.0f;
+    for (size_t e = 0; e < g.ec.size(); e++) {
+        if (!ec_hits(g, (int)e, l) || !ec_hits(g, (int)e, r)) continue;   // factor 1.0f
+        sel *= estimate_ec_selectivity(g, (int)e, l, r);
+    }
+    return sel;
+}
+
+// :135-148 (QueryTree overload)
+static float estimate_join_rows(const GInfo &g, const QT &l, const QT &r) {
+    float sel = estimate_join_selectivity(g, l.id, r.id);
+    float rows = sel * l.rows * r.rows;
+    return rows > 1 ? std::round(rows) : 1;
+}
+
+// ---------------------------------------------------------------------------
+// conversion and relabelling
+// ---------------------------------------------------------------------------
+static BB bms_to_bb(const Bitmapset *b, bool &too_wide) {
+    BB r;
+    if (!b) return r;
+    for (int i = 0; i < b->nwords; i++) {
+        if (i >= kBigWords) {
+            if (b->words[i]) too_wide = true;
+            continue;
+        }
+        r.w[i] = b->words[i];
+    }
+    return r;
+}
+
+static bool convert_big(const GpuqoPlannerInfoC *c, GInfo &g, std::string &err) {
+    if (c->n_rels >= kBigBits - 1) {
+        err = "more than " + std::to_string(kBigBits - 2) + " relations";
+        return false;
+    }
+    bool wide = false;
+    g.n = c->n_rels;
+    g.p = read_params();
+    g.base.resize(g.n);
+    g.edge.resize(g.n);
+    for (int i = 0; i < g.n; i++) {
+        g.edge[i] = bms_to_bb(c->edge_table[i], wide);
+        GBase &b = g.base[i];
+        b.id = bms_to_bb(c->base_rels[i].id, wide);
+        b.rows = c->base_rels[i].rows;
+        b.tuples = c->base_rels[i].tuples;
+        b.width = c->base_rels[i].width;
+        b.cost = c->base_rels[i].cost;
+        b.composite = false;
+        if (b.id != BB::bit(i + 1)) {
+            err = "base relation " + std::to_string(i) + " does not carry relid bit " + std::to_string(i + 1);
+            return false;
+        }
+    }
+    for (const EqClassInfo *ec = c->eq_classes; ec; ec = ec->next) {
+        BB r = bms_to_bb(ec->relids, wide);
+        g.ec.push_back(r);
+        int s = r.size();
+        for (int j = 0; j < s * (s - 1) / 2; j++) g.sels.push_back(ec->sels[j]);
+        for (int j = 0; j < s; j++) {
+            g.fks.push_back(ec->fk ? bms_to_bb(ec->fk[j], wide) : BB());
+            g.vars.push_back(ec->vars[j]);
+        }
+    }
+    if (wide) {
+        err = "relation ids beyond the supported range";
+        return false;
+    }
+    g.index();
+    return true;
+}
+
+struct Entry {
+    BB from;
+    int to;
+    QT *qt;
+};
+
+// Remapper (gpuqo_remapper.cu) over a list of disjoint entries.
+class Remap {
+public:
+    std::vector<Entry> list;
+    std::vector<int> owner;     // relation index (bit - 1) -> entry position, -1 if none
+    Remap(const std::vector<Entry> &l, int n_from) : list(l), owner(n_from, -1) {
+        for (size_t k = 0; k < list.size(); k++)
+            list[k].from.for_each([&](int b) {
+                if (b - 1 < n_from) owner[b - 1] = (int)k;
+            });
+    }
+    // remapRelid (:49-59)
+    BB rel(const BB &id) const {
+        BB out;
+        id.for_each([&](int b) {
+            int k = (b - 1 < (int)owner.size()) ? owner[b - 1] : -1;
+            if (k >= 0) out.set(list[k].to + 1);
+        });
+        return out;
+    }
+    // remapRelidNoComposite (:61-75)
+    BB rel_nocomp(const BB &id, const GInfo &from) const {
+        BB out;
+        id.for_each([&](int b) {
+            int k = (b - 1 < (int)owner.size()) ? owner[b - 1] : -1;
+            if (k < 0) return;
+            const Entry &e = list[k];
+            if (e.from.size() > 1 || from.base[e.from.lowest_pos() - 1].composite) return;
+            out.set(e.to + 1);
+        });
+        return out;
+    }
+    // remapRelidInv (:77-87)
+    BB inv(const BB &id) const {
+        BB out;
+        for (const Entry &e : list)
+            if (id.test(e.to + 1)) out |= e.from;
+        return out;
+    }
+    bool ec_inside_one_entry(const GInfo &g, int e) const {
+        int k0 = -2;
+        for (int m : g.ec_members[e]) {
+            int k = owner[m];
+            if (k < 0) return false;
+            if (k0 == -2) k0 = k;
+            else if (k != k0) return false;
+        }
+        return k0 >= 0;
+    }
+
+    // remapPlannerInfo (:201-277) with remapEdgeTable / remapBaseRels /
+    // remapEqClass (:89-199)
+    GInfo info(const GInfo &from) const {
+        GInfo to;
+        to.n = (int)list.size();
+        to.p = from.p;
+        to.base.resize(to.n);
+        to.edge.assign(to.n, BB());
+        for (const Entry &e : list) {
+            BB et;
+            e.from.for_each([&](int b) { et |= rel(from.edge[b - 1]); });
+            et.unset(e.to + 1);
+            to.edge[e.to] = et;
+            GBase &tb = to.base[e.to];
+            tb.id = rel(e.from);
+            if (e.qt) {
+                tb.rows = e.qt->rows;
+                tb.cost = e.qt->cost;
+                tb.width = e.qt->width;
+                tb.tuples = e.qt->rows;
+            } else {
+                const GBase &fb = from.base[e.from.lowest_pos() - 1];
+                tb.rows = fb.rows;
+                tb.cost = fb.cost;
+                tb.width = fb.width;
+                tb.tuples = fb.tuples;
+            }
+            tb.composite = (e.from.size() == 1) ? from.base[e.from.lowest_pos() - 1].composite : true;
+        }
+        for (size_t i = 0; i < from.ec.size(); i++) {
+            if (ec_inside_one_entry(from, (int)i)) continue;
+            const BB &ecf = from.ec[i];
+            BB ect = rel(ecf);
+            int s_from = (int)from.ec_members[i].size();
+            int s_to = ect.size();
+            size_t sel_base = to.sels.size(), fk_base = to.fks.size();
+            to.sels.resize(sel_base + s_to * (s_to - 1) / 2, 0.0f);
+            to.fks.resize(fk_base + s_to, BB());
+            to.vars.resize(fk_base + s_to);
+            std::vector<int> to_bits;
+            ect.for_each([&](int b) { to_bits.push_back(b); });
+            for (int lt = 0; lt < s_to; lt++) {
+                BB id_lt = BB::bit(to_bits[lt]);
+                BB id_lf = inv(id_lt);
+                int lf = (id_lf.all_lower() & ecf).size();
+                for (int rt = lt + 1; rt < s_to; rt++) {
+                    BB id_rt = BB::bit(to_bits[rt]);
+                    BB id_rf = inv(id_rt);
+                    int rf = (id_rf.all_lower() & ecf).size();
+                    float v;
+                    if (id_lf.size() == 1 && id_rf.size() == 1)
+                        v = from.sels[from.ec_off_sels[i] + ec_index(lf, rf, s_from)];
+                    else
+                        v = estimate_ec_selectivity(from, (int)i, id_lf, id_rf);
+                    to.sels[sel_base + ec_index(lt, rt, s_to)] = v;
+                }
+                if (id_lf.size() == 1 && !from.base[id_lf.lowest_pos() - 1].composite)
+                    to.fks[fk_base + lt] = rel_nocomp(from.fks[from.ec_off_fks[i] + lf], from);
+                to.vars[fk_base + lt] = from.vars[from.ec_off_fks[i] + lf];
+                if (id_lf.size() > 1) to.vars[fk_base + lt].index.available = false;
+            }
+            to.ec.push_back(ect);
+        }
+        to.index();
+        return to;
+    }
+
+    // remapQueryTree (:279-300)
+    QT *tree_back(const QT *qt, Arena &A) const {
+        if (!qt) return nullptr;
+        if (qt->id.size() == 1) {
+            int idx = qt->id.lowest_pos() - 1;
+            for (const Entry &e : list)
+                if (e.qt && e.to == idx) return e.qt;
+        }
+        QT *o = A.make();
+        o->id = inv(qt->id);
+        o->left = tree_back(qt->left, A);
+        o->right = tree_back(qt->right, A);
+        o->rows = qt->rows;
+        o->cost = qt->cost;
+        o->width = qt->width;
+        return o;
+    }
+
+    // remapQueryTreeFwd (:302-321)
+    QT *tree_fwd(const QT *qt, Arena &A) const {
+        if (!qt) return nullptr;
+        QT *o = A.make();
+        o->id = rel(qt->id);
+        if (o->id.size() == 1) {
+            o->left = o->right = nullptr;
+        } else {
+            o->left = tree_fwd(qt->left, A);
+            o->right = tree_fwd(qt->right, A);
+        }
+        o->rows = qt->rows;
+        o->cost = qt->cost;
+        o->width = qt->width;
+        return o;
+    }
+};
+
+static std::vector<Entry> identity_list(const GInfo &g) {
+    std::vector<Entry> l;
+    for (int i = 0; i < g.n; i++) l.push_back(Entry{g.base[i].id, i, nullptr});
+    return l;
+}
+
+// makeBFSIndexRemapper (gpuqo_bfs_indexing.cu:14-55)
+static std::vector<Entry> bfs_list(const GInfo &g) {
+    std::vector<int> queue(1, 0);
+    size_t front = 0;
+    std::vector<Entry> l;
+    BB seen = BB::bit(1);
+    int bfs_idx = 0;
+    while (front < queue.size() && bfs_idx < g.n) {
+        int b = queue[front++];
+        l.push_back(Entry{BB::bit(b + 1), bfs_idx++, nullptr});
+        g.edge[b].for_each([&](int next) {
+            if (!seen.test(next)) queue.push_back(next - 1);
+        });
+        seen |= g.edge[b];
+    }
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// exact DP of a remapped sub-problem on the GPU
+// ---------------------------------------------------------------------------
+static int to_host_info(const GInfo &g, HostInfo &h, std::string &err) {
+    if (g.n > 63) {
+        err = "sub-problem of " + std::to_string(g.n) + " relations";
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    auto m64 = [](const BB &b) { return b.w[0]; };
+    h.n = g.n;
+    h.p = g.p;
+    h.base.resize(g.n);
+    h.edge.resize(g.n);
+    for (int i = 0; i < g.n; i++) {
+        h.edge[i] = m64(g.edge[i]);
+        h.base[i].id = m64(g.base[i].id);
+        h.base[i].rows = g.base[i].rows;
+        h.base[i].tuples = g.base[i].tuples;
+        h.base[i].width = g.base[i].width;
+        h.base[i].cost = g.base[i].cost;
+        h.base[i].composite = g.base[i].composite;
+    }
+    h.ec_relids.clear();
+    for (const BB &e : g.ec) h.ec_relids.push_back(m64(e));
+    h.ec_sels = g.sels;
+    h.ec_fks.clear();
+    for (const BB &f : g.fks) h.ec_fks.push_back(m64(f));
+    h.ec_vars = g.vars;
+    return 0;
+}
+
+struct Ctx {
+    DpMode mode;
+    Arena A;
+    int err = 0;
+    std::string msg;
+};
+
+static QT *nodes_to_qt(const std::vector<TreeNode> &nodes, int idx, Arena &A) {
+    if (idx < 0) return nullptr;
+    const TreeNode &t = nodes[idx];
+    QT *q = A.make();
+    for (int k = 0; k < 32; k++)
+        if (t.set & (1u << k)) q->id.set(k + 1);
+    q->rows = t.rows;
+    q->cost.startup = t.startup;
+    q->cost.total = t.total;
+    q->width = t.width;
+    q->left = nodes_to_qt(nodes, t.left, A);
+    q->right = nodes_to_qt(nodes, t.right, A);
+    return q;
+}
+
+// gpuqo_run_idp2_dp (gpuqo_idp.cu:123-141) / gpuqo_run_dpdp_union_dp
+// (gpuqo_dpdp_union.cu:254-272): remap, solve, map the plan back
+static QT *solve_sub(const GInfo &info, const std::vector<Entry> &list, Ctx &C) {
+    Remap R(list, info.n);
+    GInfo sub = R.info(info);
+    HostInfo h;
+    if (int rc = to_host_info(sub, h, C.msg)) {
+        C.err = rc;
+        return nullptr;
+    }
+    std::vector<TreeNode> nodes;
+    int rc = exact_dp(h, C.mode, nodes, C.msg);
+    if (rc) {
+        C.err = rc;
+        return nullptr;
+    }
+    QT *qt = nodes_to_qt(nodes, 0, C.A);
+    return R.tree_back(qt, C.A);
+}
+
+// ---------------------------------------------------------------------------
+// GOO (gpuqo_cpu_goo.cu:61-150): greedy on the smallest intermediate result
+// ---------------------------------------------------------------------------
+struct GooNode {
+    QT *qt;
+    BB edges;      // union of the relations' edges (are_connected_ids operand)
+};
+
+static QT *goo(const GInfo &g, Arena &A) {
+    auto compare = [](QT *l, QT *r) {
+        if (l != nullptr && r != nullptr) return l->rows > r->rows;
+        return r != nullptr;
+    };
+    std::vector<QT *> heap;
+    std::map<BB, GooNode> rels;
+    auto edges_of = [&](const BB &id) {
+        BB e;
+        id.for_each([&](int b) { e |= g.edge[b - 1]; });
+        return e;
+    };
+    auto join = [&](QT &l, QT &r) {
+        QT *q = A.make();
+        q->id = l.id | r.id;
+        q->rows = estimate_join_rows(g, l, r);
+        q->cost.startup = 0;
+        q->cost.total = q->rows + l.cost.total + r.cost.total;
+        q->left = &l;
+        q->right = &r;
+        q->width = l.width + r.width;
+        return q;
+    };
+    for (int i = 0; i < g.n; i++) {
+        QT *q = A.make();
+        q->id = g.base[i].id;
+        q->rows = g.base[i].rows;
+        q->cost.startup = 0;
+        q->cost.total = g.base[i].rows;
+        q->width = g.base[i].width;
+        rels.emplace(q->id, GooNode{q, edges_of(q->id)});
+    }
+    // are_valid_pair (gpuqo_filter.cuh:84-90): connected and disjoint
+    auto valid = [](const GooNode &a, const BB &bid) { return a.edges.intersects(bid) && !a.qt->id.intersects(bid); };
+    for (auto i = rels.begin(); i != rels.end(); ++i)
+        for (auto j = i; j != rels.end(); ++j)
+            if (valid(i->second, j->first)) {
+                heap.push_back(join(*i->second.qt, *j->second.qt));
+                std::push_heap(heap.begin(), heap.end(), compare);
+            }
+    QT *smallest = nullptr;
+    do {
+        if (heap.empty()) return nullptr;   // disconnected query graph
+        std::pop_heap(heap.begin(), heap.end(), compare);
+        smallest = heap.back();
+        heap.pop_back();
+        auto lp = rels.find(smallest->left->id);
+        auto rp = rels.find(smallest->right->id);
+        if (lp == rels.end() || rp == rels.end()) {
+            smallest = nullptr;
+            continue;
+        }
+        rels.erase(lp);
+        rels.erase(rp);
+        GooNode sn{smallest, edges_of(smallest->id)};
+        for (auto j = rels.begin(); j != rels.end(); ++j)
+            if (valid(sn, j->first)) {
+                heap.push_back(join(*smallest, *j->second.qt));
+                std::push_heap(heap.begin(), heap.end(), compare);
+            }
+        rels.emplace(smallest->id, sn);
+    } while (smallest == nullptr || smallest->id.size() < g.n);
+    return smallest;
+}
+
+// ---------------------------------------------------------------------------
+// IDP2 (gpuqo_idp.cu:96-297)
+// ---------------------------------------------------------------------------
+static QT *most_expensive_subtree(QT *qt, int max_size) {
+    if (qt->id.size() <= max_size) return qt;
+    QT *l = most_expensive_subtree(qt->left, max_size);
+    QT *r = most_expensive_subtree(qt->right, max_size);
+    if (l->id.size() == 1) return r;
+    if (r->id.size() == 1) return l;
+    if (l->cost.total > r->cost.total) return l;
+    if (l->cost.total < r->cost.total) return r;
+    if (l->id.size() < r->id.size()) return l;
+    return r;
+}
+
+static QT *idp2_rec(QT *goo_qt, const GInfo &info, const std::vector<Entry> &list, int n_iters, Ctx &C) {
+    Remap R(list, info.n);
+    GInfo ni = R.info(info);
+    QT *ngoo = R.tree_fwd(goo_qt, C.A);
+    const int iters = std::min(ni.n, n_iters);
+    QT *maximal = most_expensive_subtree(ngoo, iters);
+    std::vector<Entry> reopt;
+    {
+        int i = 0;
+        maximal->id.for_each([&](int b) { reopt.push_back(Entry{BB::bit(b), i++, nullptr}); });
+    }
+    QT *reopt_qt = solve_sub(ni, reopt, C);
+    if (!reopt_qt) return nullptr;
+    QT *res;
+    if (iters == ni.n) {
+        res = reopt_qt;
+    } else {
+        std::vector<Entry> next;
+        next.push_back(Entry{reopt_qt->id, 0, reopt_qt});
+        int j = 1;
+        for (int i = 0; i < ni.n; i++)
+            if (!ni.base[i].id.is_subset_of(reopt_qt->id)) next.push_back(Entry{ni.base[i].id, j++, nullptr});
+        res = idp2_rec(ngoo, ni, next, n_iters, C);
+        if (!res) return nullptr;
+    }
+    return R.tree_back(res, C.A);
+}
+
+static QT *run_idp2(const GInfo &info, int n_iters, Ctx &C) {
+    QT *goo_qt = goo(info, C.A);
+    if (!goo_qt) {
+        C.err = GPUQO_B200_ERR_ARGS;
+        C.msg = "query graph is not connected";
+        return nullptr;
+    }
+    return idp2_rec(goo_qt, info, identity_list(info), n_iters, C);
+}
+
+// ---------------------------------------------------------------------------
+// UnionDP (gpuqo_dpdp_union.cu:29-472)
+// ---------------------------------------------------------------------------
+struct GraphEdge {
+    BB left, right;
+    int left_size, right_size, total_size;
+    float rows, selectivity, weight;
+};
+
+struct CompareEdges {
+    bool operator()(const GraphEdge *l, const GraphEdge *r) const {
+        if (l->total_size == r->total_size) return l->weight > r->weight;
+        return l->total_size > r->total_size;
+    }
+};
+
+static QT *union_rec(const GInfo &info, const std::vector<Entry> &list, int n_iters, Ctx &C) {
+    Remap R(list, info.n);
+    GInfo ni = R.info(info);
+    const int iters = std::min(ni.n, n_iters);
+    if (ni.n == iters) return solve_sub(info, list, C);
+
+    // fillPriorityQueues (:212-251): edges in the reference's BFS order,
+    // weight = selectivity * rows * rows (createGraphEdge :164-209)
+    std::vector<std::unique_ptr<GraphEdge>> edges;
+    std::priority_queue<GraphEdge *, std::vector<GraphEdge *>, CompareEdges> pq;
+    {
+        std::queue<int> bq;
+        int bfs_idx = 0;
+        bq.push(0);
+        BB seen2 = BB::bit(1);
+        while (!bq.empty() && bfs_idx < ni.n) {
+            int b = bq.front();
+            bq.pop();
+            bfs_idx++;
+            ni.edge[b].for_each([&](int next) {
+                if (seen2.test(next)) return;
+                bq.push(next - 1);
+                GraphEdge *e = new GraphEdge();
+                e->left = ni.base[b].id;
+                e->right = ni.base[next - 1].id;
+                e->selectivity = estimate_join_selectivity(ni, e->left, e->right);
+                e->rows = e->selectivity * ni.base[b].rows * ni.base[next - 1].rows;
+                e->left_size = e->right_size = 1;
+                e->total_size = 2;
+                e->weight = e->rows;
+                edges.emplace_back(e);
+                pq.push(e);
+            });
+            seen2 |= BB::bit(b + 1);
+        }
+    }
+    // DisjointSet over relation indices (:36-101)
+    std::vector<int> parent(ni.n), size(ni.n, 1);
+    std::vector<BB> csg(ni.n);
+    for (int i = 0; i < ni.n; i++) {
+        parent[i] = i;
+        csg[i] = ni.base[i].id;
+    }
+    std::function<int(int)> find = [&](int x) {
+        if (parent[x] != x) parent[x] = find(parent[x]);
+        return parent[x];
+    };
+    const int upper_threshold = 16;
+    while (!pq.empty()) {
+        GraphEdge *e = pq.top();
+        pq.pop();
+        int l = e->left.lowest_pos() - 1, r = e->right.lowest_pos() - 1;
+        int x = find(l), y = find(r);
+        if (x == y) continue;
+        if (e->total_size != size[x] + size[y]) {
+            e->left_size = size[x];
+            e->right_size = size[y];
+            e->total_size = e->left_size + e->right_size;
+            pq.push(e);
+        } else if (e->total_size < upper_threshold) {
+            if (size[x] > size[y]) {
+                parent[y] = x;
+                size[x] += size[y];
+                csg[x] |= csg[y];
+            } else if (size[x] < size[y]) {
+                parent[x] = y;
+                size[y] += size[x];
+                csg[y] |= csg[x];
+            } else {
+                parent[x] = y;
+                size[y] *= 2;
+                csg[y] |= csg[x];
+            }
+        }
+    }
+    std::vector<BB> subgraphs;
+    BB seen;
+    for (int i = 0; i < ni.n; i++) {
+        const BB &cs = csg[find(i)];
+        if (!cs.is_subset_of(seen)) subgraphs.push_back(cs);
+        seen |= cs;
+    }
+    std::vector<Entry> next;
+    for (size_t i = 0; i < subgraphs.size(); i++) {
+        std::vector<Entry> reopt;
+        int j = 0;
+        subgraphs[i].for_each([&](int b) { reopt.push_back(Entry{BB::bit(b), j++, nullptr}); });
+        QT *q = solve_sub(ni, reopt, C);
+        if (!q) return nullptr;
+        next.push_back(Entry{q->id, (int)i, q});
+    }
+    QT *res = union_rec(ni, next, n_iters, C);
+    if (!res) return nullptr;
+    return R.tree_back(res, C.A);
+}
+
+// ---------------------------------------------------------------------------
+// entry
+// ---------------------------------------------------------------------------
+static QueryTreeC *qt_to_c(const QT *q) {
+    if (!q) return nullptr;
+    QueryTreeC *o = (QueryTreeC *)palloc(sizeof(QueryTreeC));
+    int top = 0;
+    for (int i = 0; i < kBigWords; i++)
+        if (q->id.w[i]) top = i;
+    int nwords = top + 1;
+    Bitmapset *b = (Bitmapset *)palloc0(offsetof(Bitmapset, words) + nwords * sizeof(bitmapword));
+    b->nwords = nwords;
+    for (int i = 0; i < nwords; i++) b->words[i] = q->id.w[i];
+    o->id = b;
+    o->rows = q->rows;
+    o->cost = q->cost;
+    o->width = q->width;
+    o->left = qt_to_c(q->left);
+    o->right = qt_to_c(q->right);
+    return o;
+}
+
+QueryTreeC *run_idp(int algorithm, GpuqoPlannerInfoC *info_c) {
+    std::string err;
+    const int n = info_c->n_rels;
+    const bool idp = gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < n;
+    if (!idp) {
+        set_error(GPUQO_B200_ERR_UNSUPPORTED,
+                  std::to_string(n) + " relations need IDP (set gpuqo_idp_n_iters between 2 and n-1)");
+        return nullptr;
+    }
+    if (gpuqo_idp_type != GPUQO_IDP2 && gpuqo_idp_type != GPUQO_UNION) {
+        set_error(GPUQO_B200_ERR_UNSUPPORTED, "gpuqo_idp_type: only IDP2 and UNION are provided");
+        return nullptr;
+    }
+    GInfo g;
+    if (!convert_big(info_c, g, err)) {
+        set_error(GPUQO_B200_ERR_ARGS, err);
+        return nullptr;
+    }
+    Ctx C;
+    C.mode = mode_for(algorithm);
+    // __gpuqo_run (gpuqo_main_internal.cu:102-137): BFS relabel, IDP, map back
+    std::vector<Entry> bl = bfs_list(g);
+    if ((int)bl.size() != g.n) {
+        set_error(GPUQO_B200_ERR_ARGS, "query graph is not connected");
+        return nullptr;
+    }
+    Remap R(bl, g.n);
+    GInfo rg = R.info(g);
+    QT *qt = (gpuqo_idp_type == GPUQO_IDP2) ? run_idp2(rg, gpuqo_idp_n_iters, C)
+                                             : union_rec(rg, identity_list(rg), gpuqo_idp_n_iters, C);
+    if (!qt) {
+        set_error(C.err ? C.err : GPUQO_B200_ERR_ARGS, C.msg.empty() ? "IDP failed" : C.msg);
+        return nullptr;
+    }
+    QT *back = R.tree_back(qt, C.A);
+    return qt_to_c(back);
 }
 
 }  // namespace gqb
