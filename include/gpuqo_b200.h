@@ -252,12 +252,16 @@ int gpuqo_b200_run_noalloc(int gpuqo_algorithm, const GpuqoPlannerInfoC *info, v
                            GpuqoB200PlanNode *nodes, int max_nodes, int *n_nodes);
 
 /*
- * Batched exact DP: optimises n_queries independent queries (each < 32
- * relations, no IDP) with one persistent launch sequence per relation count
- * level, all queries' memos packed in one device arena.  Trees are written to
- * out[i] (palloc'd, NULL on error).  Same plans as gpuqo_run per query.
- * Returns a status code.
+ * Batched exact DP: optimises n_queries independent queries in one call.
+ * MPDP queries of up to 30 relations (no IDP) are packed into waves whose
+ * dense memos share one device arena of at most gpuqo_b200_batch_memory_mb;
+ * each wave runs level by level with one enumeration and one evaluation
+ * launch per level for all of its queries.  Other queries (plain DPsub, IDP,
+ * very large biconnected blocks) run one by one through gpuqo_run's path.
+ * Trees are written to out[i] (palloc'd, NULL on error); every plan is the
+ * one gpuqo_run returns for that query.  Returns a status code.
  */
+extern int gpuqo_b200_batch_memory_mb;
 int gpuqo_b200_run_batch(int gpuqo_algorithm, GpuqoPlannerInfoC **infos,
                          int n_queries, QueryTreeC **out);
 

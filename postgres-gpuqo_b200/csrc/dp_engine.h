@@ -48,6 +48,15 @@ int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, 
                          bool flush_l2, double &ms_per_iter, std::vector<TreeNode> &nodes, EngineStats &stats,
                          std::string &err);
 
+// Batched MPDP of many sub-problems (each <= 30 relations and eligible, see
+// batch_eligible), level-synchronous per wave; waves are consecutive queries
+// whose memory stays within wave_bytes.  out[i] gets query i's plan nodes.
+int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, uint64_t wave_bytes,
+                     std::vector<std::vector<TreeNode>> &out, EngineStats &stats, std::vector<double> &wave_ms,
+                     std::string &err);
+bool batch_eligible(const std::vector<uint32_t> &blob);
+uint64_t batch_query_bytes(int n);
+
 // Device-memory estimate (bytes) of one exact DP over n relations.
 uint64_t engine_bytes_needed(int n);
 

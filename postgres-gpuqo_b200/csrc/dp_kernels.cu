@@ -615,17 +615,17 @@ __global__ void __launch_bounds__(kBlock) k_eval_mpdp(const uint32_t *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// k_eval_tree: MPDP on a tree-shaped query graph (star, snowflake, chain).
-// Every connected set S is a subtree rooted at its lowest relation, every
-// block a bridge (parent a, child b), and the 2(k-1) candidates are the two
-// orientations of each edge: removing it leaves S & tsub[b] and the rest, so
-// no DFS is needed.  The reference's enumeration index of a candidate is
-// 2 * post(b) + side, where post(b) is b's post-order rank in S's DFS (the
-// order in which the reference emits blocks) and side 0 is lb = {a}:
-//     post(b) = |S & tbefore[b]| - |S & tanc[b]| + |S & tsub[b]| - 1
-// (preorder rank minus depth plus subtree size minus one; S's DFS visits S in
-// the query tree's preorder).  With ec_masked only the classes on edge (a, b)
-// can match.
+// k_eval_tree: MPDP on a tree-shaped query graph (star, snowflake, chain, and
+// the contracted trees of IDP sub-problems), any relation numbering.
+// A connected set S is a subtree; the reference's block search walks it from
+// its lowest relation r, and every block is a bridge {a, b}, a < b.  With the
+// query tree rooted at r, let c be the child end of the edge: removing the
+// edge leaves S & sub_r[c] and the rest, so no DFS is needed.  Candidate
+// order: blocks are emitted in post-order of their child end, and the
+// reference's enumeration index is 2 * post_r(c) + (lb == {a} ? 0 : 1) with
+//     post_r(c) = |S & before_r[c]| - |S & anc_r[c]| + |S & sub_r[c]| - 1
+// (preorder rank minus depth plus subtree size minus one).  With ec_masked
+// only the classes on edge {a, b} can match.
 // ---------------------------------------------------------------------------
 struct EdgeIter {
     uint32_t vs;      // vertices of S not yet started
@@ -676,16 +676,26 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
                 while (it.e <= target) edge_next(h.adj, S, it, a, b);
             }
             if (active) {
-                // a < b: a is b's parent in the query tree
-                const uint32_t comp_b = S & h.tsub[b];
+                const uint32_t *tab = reinterpret_cast<const uint32_t *>(d.h) + h.tree_tab;
+                const int n = h.n, nn = n * n;
+                const int rt = __ffs(S) - 1;
+                const uint32_t *anc_r = tab + 2 * nn + rt * n;
+                const int ch = ((anc_r[b] >> a) & 1u) ? b : a;        // child end w.r.t. root rt
+                const uint32_t comp_c = S & tab[rt * n + ch];
+                const uint32_t comp_a = (ch == a) ? comp_c : (S ^ comp_c);
                 const uint32_t side = c & 1u;
-                const uint32_t L = side ? comp_b : (S ^ comp_b);
+                const uint32_t L = side ? (S ^ comp_a) : comp_a;       // side 0: lb = {a}
                 const uint32_t R = S ^ L;
-                const uint32_t post = (uint32_t)(__popc(S & h.tbefore[b]) - __popc(S & h.tanc[b]) +
-                                                 __popc(comp_b) - 1);
+                const uint32_t post = (uint32_t)(__popc(S & tab[nn + rt * n + ch]) - __popc(S & anc_r[ch]) +
+                                                 __popc(comp_c) - 1);
                 const uint32_t p = 2u * post + side;
+                uint32_t ecm = 0u;
+                if (MASKED) {
+                    const int ch0 = ((tab[2 * nn + b] >> a) & 1u) ? b : a;   // child end w.r.t. relation 0
+                    ecm = h.edge_ec[ch0];
+                }
                 RelVal l = load_rel(memo, L), r = load_rel(memo, R);
-                RelVal out = join_eval_t<MASKED>(d, L, l, R, r, MASKED ? h.edge_ec[b] : 0u);
+                RelVal out = join_eval_t<MASKED>(d, L, l, R, r, ecm);
                 const bool nan = isnan(out.total);
                 best.n_valid++;
                 if (p < best.first_p) {
@@ -1507,7 +1517,6 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         h->total[t] = b.cost.total;
         h->width[t] = b.width;
         h->fksel[t] = (float)(1.0 / (double)fmaxf(1.0f, b.tuples));
-        h->tparent[t] = -1;
     }
     DevInfoView v = make_view(blob);
     uint32_t *relids = const_cast<uint32_t *>(v.ec_relids);
@@ -1685,3 +1694,518 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
     *n_nodes = host_n;
     return GPUQO_B200_OK;
 }
+
+// ===========================================================================
+// Batched MPDP: many independent queries level by level.  One wave packs the
+// memos of its queries into one arena; per level one enumeration launch and
+// one evaluation launch serve every query of the wave, so small queries no
+// longer pay per-query launch latency.  Items of a level list are
+// (query << 32 | set).  The planner info of each query stays in global
+// memory (read through the read-only cache) because groups of one warp may
+// belong to different queries.
+// ===========================================================================
+namespace gqb {
+
+struct BatchQ {
+    uint32_t blob_off;                 // word offset into the wave's blob buffer
+    uint32_t n;
+    uint32_t first_base;               // index of its first singleton in the level-1 list
+    uint32_t pad;
+    unsigned long long memo_off;       // entry offset into the memo arena
+    unsigned long long seen_off;       // word offset into the dedup bitmap arena
+};
+
+__global__ void kb_init(const BatchQ *__restrict__ qs, int nq, const uint32_t *__restrict__ blobs,
+                        float4 *__restrict__ memo, uint32_t *__restrict__ memo_left,
+                        unsigned long long *__restrict__ list1, LevelCounters *__restrict__ lvl1) {
+    const int q = blockIdx.x;
+    if (q >= nq) return;
+    const BatchQ Q = qs[q];
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off);
+    for (int i = threadIdx.x; i < (int)Q.n; i += blockDim.x) {
+        memo[Q.memo_off + (1ull << i)] =
+            make_float4(h->rows[i], h->startup[i], h->total[i], __int_as_float(h->width[i]));
+        memo_left[Q.memo_off + (1ull << i)] = 0u;
+        list1[Q.first_base + i] = ((unsigned long long)q << 32) | (1u << i);
+    }
+    if (threadIdx.x == 0) atomicAdd(&lvl1->n_sets, Q.n);
+}
+
+// connected k-sets of every query, by extension of its (k-1)-sets
+__global__ void __launch_bounds__(kBlock) kb_level_sets(const BatchQ *__restrict__ qs,
+                                                        const uint32_t *__restrict__ blobs,
+                                                        const unsigned long long *__restrict__ prev,
+                                                        const LevelCounters *__restrict__ prev_lc,
+                                                        uint32_t *__restrict__ seen,
+                                                        unsigned long long *__restrict__ out,
+                                                        LevelCounters *__restrict__ lc) {
+    __shared__ unsigned long long stage[kWarpsPerBlock][64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long *st = stage[warp];
+    uint32_t cnt = 0;
+    const uint32_t c_prev = __ldcg(&prev_lc->n_sets);
+    const uint32_t nthreads = gridDim.x * blockDim.x;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t rounds = (c_prev + nthreads - 1u) / nthreads;
+    for (uint32_t r = 0; r < rounds; r++) {
+        const uint32_t idx = tid + r * nthreads;
+        uint32_t S = 0u, N = 0u, q = 0u;
+        const uint32_t *adj = nullptr;
+        unsigned long long seen_off = 0;
+        if (idx < c_prev) {
+            const unsigned long long it = __ldcg(prev + idx);
+            q = (uint32_t)(it >> 32);
+            S = (uint32_t)it;
+            const BatchQ Q = qs[q];
+            adj = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->adj;
+            seen_off = Q.seen_off;
+            uint32_t x = S;
+            while (x) {
+                int v = __ffs(x) - 1;
+                x &= x - 1u;
+                N |= __ldg(adj + v);
+            }
+            N &= ~S;
+        }
+        const int deg = __popc(N);
+        const int maxdeg = (int)__reduce_max_sync(kFull, (uint32_t)deg);
+        for (int j = 0; j < maxdeg; j++) {
+            bool ok = false;
+            unsigned long long item = 0;
+            if (j < deg) {
+                const uint32_t bitv = N & (0u - N);
+                N ^= bitv;
+                const uint32_t T = S | bitv;
+                const uint32_t bm = 1u << (T & 31u);
+                ok = !(atomicOr(&seen[seen_off + (T >> 5)], bm) & bm);
+                item = ((unsigned long long)q << 32) | T;
+            }
+            uint32_t m = __ballot_sync(kFull, ok);
+            if (ok) st[cnt + __popc(m & ((1u << lane) - 1u))] = item;
+            cnt += __popc(m);
+            __syncwarp();
+            if (cnt >= 32) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&lc->n_sets, 32u);
+                base = __shfl_sync(kFull, base, 0);
+                out[base + lane] = st[lane];
+                __syncwarp();
+                if (lane < cnt - 32) st[lane] = st[32 + lane];
+                cnt -= 32;
+                __syncwarp();
+            }
+        }
+    }
+    if (cnt > 0) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&lc->n_sets, cnt);
+        base = __shfl_sync(kFull, base, 0);
+        if (lane < cnt) out[base + lane] = st[lane];
+    }
+}
+
+// candidate c of a tree-shaped query (see k_eval_tree): edge {a, b}, a < b
+__device__ __forceinline__ void tree_cand(const DevHeader &h, uint32_t S, int a, int b, uint32_t c, uint32_t &L,
+                                          uint32_t &R, uint32_t &p, uint32_t &ecm, bool masked) {
+    const uint32_t *tab = reinterpret_cast<const uint32_t *>(&h) + h.tree_tab;
+    const int n = h.n, nn = n * n;
+    const int rt = __ffs(S) - 1;
+    const uint32_t *anc_r = tab + 2 * nn + rt * n;
+    const int ch = ((__ldg(anc_r + b) >> a) & 1u) ? b : a;
+    const uint32_t comp_c = S & __ldg(tab + rt * n + ch);
+    const uint32_t comp_a = (ch == a) ? comp_c : (S ^ comp_c);
+    const uint32_t side = c & 1u;
+    L = side ? (S ^ comp_a) : comp_a;
+    R = S ^ L;
+    const uint32_t post =
+        (uint32_t)(__popc(S & __ldg(tab + nn + rt * n + ch)) - __popc(S & __ldg(anc_r + ch)) + __popc(comp_c) - 1);
+    p = 2u * post + side;
+    ecm = 0u;
+    if (masked) {
+        const int ch0 = ((__ldg(tab + 2 * nn + b) >> a) & 1u) ? b : a;
+        ecm = h.edge_ec[ch0];
+    }
+}
+
+__device__ __forceinline__ void best_update(LaneBest &best, uint32_t p, uint32_t L, const RelVal &out) {
+    const bool nan = isnan(out.total);
+    best.n_valid++;
+    if (p < best.first_p) {
+        best.first_p = p;
+        best.first_nan = nan;
+        if (nan) {
+            best.nan_val = out;
+            best.nan_left = L;
+        }
+    }
+    if (!nan) {
+        const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
+        if (key < best.key) {
+            best.key = key;
+            best.val = out;
+            best.left = L;
+        }
+    }
+}
+
+template <int G>
+__device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *blobs, uint32_t first, uint32_t stride,
+                                             const unsigned long long *items, uint32_t count, int k, float4 *memo_all,
+                                             uint32_t *memo_left_all, unsigned long long &pairs) {
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G, gl = lane % G;
+    const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
+    Blocks B;
+    for (uint32_t base = first; base < count; base += stride) {
+        const uint32_t i = base + (uint32_t)grp;
+        const bool has = i < count;
+        unsigned long long it = has ? __ldcg(items + i) : 0ull;
+        const uint32_t q = (uint32_t)(it >> 32), S = (uint32_t)it;
+        BatchQ Q;
+        Q.blob_off = 0;
+        Q.memo_off = 0;
+        if (has) Q = qs[q];
+        const DevInfoView d = make_view(blobs + Q.blob_off);
+        const DevHeader &h = *d.h;
+        float4 *memo = memo_all + Q.memo_off;
+        uint32_t *memo_left = memo_left_all + Q.memo_off;
+        const bool tree = has && h.tree_mode != 0u;
+        const bool masked = tree && h.ec_masked != 0u;
+        uint32_t P = 0;
+        B.nb = 0;
+        if (has) {
+            if (tree) {
+                P = 2u * (uint32_t)(k - 1);
+            } else {
+                find_blocks(S, h.adj, B);
+                P = B.total;
+            }
+        }
+        __syncwarp();
+        const uint32_t iters = __reduce_max_sync(kFull, (P + G - 1u) / G);
+        LaneBest best;
+        best.init();
+        EdgeIter ei;
+        ei.vs = S;
+        ei.nb = 0u;
+        ei.v = 0;
+        ei.e = 0u;
+        int ea = 0, eb = 0, bcur = 0;
+        for (uint32_t j = 0; j < iters; j++) {
+            const uint32_t c = (uint32_t)gl + j * G;
+            const bool active = has && c < P;
+            uint32_t L = 0, R = 0, p = 0, ecm = 0;
+            bool valid = false;
+            if (active) {
+                if (tree) {
+                    while (ei.e <= (c >> 1)) edge_next(h.adj, S, ei, ea, eb);
+                    tree_cand(h, S, ea, eb, c, L, R, p, ecm, masked);
+                    valid = true;
+                } else {
+                    p = c;
+                    valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R);
+                }
+            }
+            if (valid) {
+                RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+                RelVal out = masked ? join_eval_t<true>(d, L, l, R, r, ecm) : join_eval_t<false>(d, L, l, R, r, 0u);
+                best_update(best, p, L, out);
+            }
+        }
+        uint32_t kh = (uint32_t)(best.key >> 32), kl = (uint32_t)best.key, fp = best.first_p;
+#pragma unroll
+        for (int off = G / 2; off >= 1; off >>= 1) {
+            uint32_t oh = __shfl_xor_sync(kFull, kh, off);
+            uint32_t ol = __shfl_xor_sync(kFull, kl, off);
+            uint32_t of = __shfl_xor_sync(kFull, fp, off);
+            if (oh < kh || (oh == kh && ol < kl)) {
+                kh = oh;
+                kl = ol;
+            }
+            if (of < fp) fp = of;
+        }
+        const bool nan_first = has && best.first_p == fp && best.first_nan;
+        const unsigned nm = __ballot_sync(kFull, nan_first) & group_mask;
+        const unsigned long long gkey = ((unsigned long long)kh << 32) | kl;
+        if (has) {
+            if (nm) {
+                if (nan_first) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
+            } else if (best.key == gkey && best.key != ~0ull) {
+                memo_write(memo, memo_left, S, best.val, best.left);
+            }
+        }
+        pairs += best.n_valid;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kb_eval(const BatchQ *__restrict__ qs, const uint32_t *__restrict__ blobs,
+                                                  const unsigned long long *__restrict__ items,
+                                                  const LevelCounters *__restrict__ lc, int k,
+                                                  float4 *__restrict__ memo, uint32_t *__restrict__ memo_left,
+                                                  GlobalCounters *__restrict__ glob, uint32_t target_lanes,
+                                                  int max_group) {
+    const uint32_t count = __ldcg(&lc->n_sets);
+    if (count == 0u) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int G = 2;
+    while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
+    G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
+    const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
+    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
+    unsigned long long pairs = 0;
+    if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, items, count, k, memo, memo_left, pairs);
+    else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, items, count, k, memo, memo_left, pairs);
+    else batch_groups<32>(qs, blobs, gwarp, nwarps, items, count, k, memo, memo_left, pairs);
+    pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
+    if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
+}
+
+__global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const float4 *__restrict__ memo,
+                           const uint32_t *__restrict__ memo_left, TreeNode *__restrict__ out,
+                           int *__restrict__ n_out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const BatchQ Q = qs[q];
+    const uint32_t full = (Q.n == 32) ? 0xFFFFFFFFu : ((1u << Q.n) - 1u);
+    TreeNode *o = out + (size_t)q * 64;
+    const float4 *m = memo + Q.memo_off;
+    const uint32_t *ml = memo_left + Q.memo_off;
+    int n = 0;
+    uint32_t stack_set[64];
+    int stack_parent[64], stack_side[64];
+    int sp = 0;
+    stack_set[sp] = full;
+    stack_parent[sp] = -1;
+    stack_side[sp] = 0;
+    sp++;
+    while (sp > 0 && n < 64) {
+        sp--;
+        uint32_t s = stack_set[sp];
+        int parent = stack_parent[sp], side = stack_side[sp];
+        float4 v = __ldcg(m + s);
+        TreeNode t;
+        t.set = s;
+        t.left = -1;
+        t.right = -1;
+        t.rows = v.x;
+        t.startup = v.y;
+        t.total = v.z;
+        t.width = __float_as_int(v.w);
+        int me = n++;
+        o[me] = t;
+        if (parent >= 0) {
+            if (side == 0) o[parent].left = me;
+            else o[parent].right = me;
+        }
+        uint32_t l = __ldcg(ml + s) & s;
+        if (__popc(s) > 1 && l != 0u && l != s && sp + 2 <= 64) {
+            stack_set[sp] = s ^ l;
+            stack_parent[sp] = me;
+            stack_side[sp] = 1;
+            sp++;
+            stack_set[sp] = l;
+            stack_parent[sp] = me;
+            stack_side[sp] = 0;
+            sp++;
+        }
+    }
+    n_out[q] = n;
+}
+
+// Candidate bound of a query for the batch (the batch has no overflow path):
+// sum over blocks of 2^|b| - 2 with |b| <= the graph's largest block.
+static uint64_t mpdp_candidate_bound(int n, int max_block) {
+    int bmax = std::min(std::max(max_block, 2), std::max(n, 2));
+    uint64_t nblk = (uint64_t)(n - 1 + bmax - 2) / (uint64_t)(bmax - 1);
+    return nblk * ((1ull << bmax) - 2ull);
+}
+
+bool batch_eligible(const std::vector<uint32_t> &blob) {
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+    return h->n >= 1 && h->n <= 30 && mpdp_candidate_bound(h->n, (int)h->max_block) <= kOvfLimit;
+}
+
+uint64_t batch_query_bytes(int n) {
+    const uint64_t slots = 1ull << n;
+    return slots * (sizeof(float4) + 4) + slots / 8 + 2 * max_level_sets(n) * 8 + 64 * sizeof(TreeNode) + 4096;
+}
+
+struct BatchEngine {
+    int device = -1, sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // arena (grown on demand)
+    uint64_t cap_slots = 0, cap_items = 0, cap_words = 0, cap_seen = 0;
+    int cap_q = 0;
+    float4 *memo = nullptr;
+    uint32_t *memo_left = nullptr, *blobs = nullptr, *seen = nullptr;
+    unsigned long long *listA = nullptr, *listB = nullptr;
+    BatchQ *qs = nullptr;
+    TreeNode *tree = nullptr;
+    int *tree_n = nullptr;
+    LevelCounters *lvl = nullptr;
+    GlobalCounters *glob = nullptr;
+
+    int init(std::string &err) {
+        if (stream) return 0;
+        CK(cudaGetDevice(&device));
+        CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+        CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        CK(cudaMalloc(&lvl, 33 * sizeof(LevelCounters)));
+        CK(cudaMalloc(&glob, sizeof(GlobalCounters)));
+        return 0;
+    }
+
+    template <class T> int grow(T *&p, uint64_t &cap, uint64_t need, std::string &err) {
+        if (need <= cap) return 0;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        CK(cudaMalloc(&p, need * sizeof(T)));
+        cap = need;
+        return 0;
+    }
+
+    // One wave: all queries' memos fit.  blobs: per query planner-info blob.
+    int run_wave(const std::vector<const std::vector<uint32_t> *> &wb, std::vector<std::vector<TreeNode>> &out,
+                 EngineStats &st, double &ms, std::string &err) {
+        const int nq = (int)wb.size();
+        std::vector<BatchQ> hq(nq);
+        uint64_t slots = 0, words = 0, seen_words = 0, items = 0, base = 0;
+        int maxn = 0;
+        for (int q = 0; q < nq; q++) {
+            const DevHeader *h = reinterpret_cast<const DevHeader *>(wb[q]->data());
+            const int n = h->n;
+            hq[q].blob_off = (uint32_t)words;
+            hq[q].n = (uint32_t)n;
+            hq[q].first_base = (uint32_t)base;
+            hq[q].memo_off = slots;
+            hq[q].seen_off = seen_words;
+            words += (wb[q]->size() + 3) & ~(size_t)3;
+            slots += 1ull << n;
+            seen_words += std::max<uint64_t>((1ull << n) / 32, 1);
+            items += max_level_sets(n);
+            base += (uint64_t)n;
+            maxn = std::max(maxn, n);
+        }
+        items = std::max(items, base);
+        uint64_t c1 = cap_slots, c2 = cap_slots, c3 = cap_words, c4 = cap_seen, c5 = cap_items, c6 = cap_items;
+        if (int rc = grow(memo, c1, slots, err)) return rc;
+        if (int rc = grow(memo_left, c2, slots, err)) return rc;
+        cap_slots = std::min(c1, c2);
+        if (int rc = grow(blobs, c3, words, err)) return rc;
+        cap_words = c3;
+        if (int rc = grow(seen, c4, seen_words, err)) return rc;
+        cap_seen = c4;
+        if (int rc = grow(listA, c5, items, err)) return rc;
+        if (int rc = grow(listB, c6, items, err)) return rc;
+        cap_items = std::min(c5, c6);
+        if (nq > cap_q) {
+            cudaFree(qs);
+            cudaFree(tree);
+            cudaFree(tree_n);
+            qs = nullptr;
+            tree = nullptr;
+            tree_n = nullptr;
+            cap_q = 0;
+            CK(cudaMalloc(&qs, nq * sizeof(BatchQ)));
+            CK(cudaMalloc(&tree, (size_t)nq * 64 * sizeof(TreeNode)));
+            CK(cudaMalloc(&tree_n, nq * sizeof(int)));
+            cap_q = nq;
+        }
+        std::vector<uint32_t> hblob(words, 0u);
+        for (int q = 0; q < nq; q++) std::copy(wb[q]->begin(), wb[q]->end(), hblob.begin() + hq[q].blob_off);
+        CK(cudaMemcpyAsync(blobs, hblob.data(), words * 4, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(qs, hq.data(), nq * sizeof(BatchQ), cudaMemcpyHostToDevice, stream));
+        CK(cudaEventRecord(ev0, stream));
+        CK(cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream));
+        CK(cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream));
+        CK(cudaMemsetAsync(seen, 0, seen_words * 4, stream));
+        kb_init<<<nq, 32, 0, stream>>>(qs, nq, blobs, memo, memo_left, listA, lvl + 1);
+        uint32_t kernels = 1;
+        const uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
+        for (int k = 2; k <= maxn; k++) {
+            unsigned long long *prev = (k & 1) ? listB : listA;
+            unsigned long long *cur = (k & 1) ? listA : listB;
+            kb_level_sets<<<sm_count * 8, kBlock, 0, stream>>>(qs, blobs, prev, lvl + (k - 1), seen, cur, lvl + k);
+            int max_group = 1;
+            while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
+            kb_eval<<<sm_count * 4, kBlock, 0, stream>>>(qs, blobs, cur, lvl + k, k, memo, memo_left, glob,
+                                                         target_lanes, max_group);
+            kernels += 2;
+        }
+        kb_extract<<<(nq + 127) / 128, 128, 0, stream>>>(qs, nq, memo, memo_left, tree, tree_n);
+        kernels++;
+        CK(cudaEventRecord(ev1, stream));
+        std::vector<TreeNode> htree((size_t)nq * 64);
+        std::vector<int> hn(nq);
+        std::vector<LevelCounters> hl(33);
+        GlobalCounters hg;
+        CK(cudaMemcpyAsync(htree.data(), tree, (size_t)nq * 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hn.data(), tree_n, nq * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hl.data(), lvl, 33 * sizeof(LevelCounters), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(&hg, glob, sizeof(GlobalCounters), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        CK(cudaGetLastError());
+        float fms = 0.f;
+        CK(cudaEventElapsedTime(&fms, ev0, ev1));
+        ms = fms;
+        out.resize(nq);
+        for (int q = 0; q < nq; q++) {
+            if (hn[q] != 2 * (int)hq[q].n - 1) {
+                err = "batched plan extraction produced " + std::to_string(hn[q]) + " nodes";
+                return GPUQO_B200_ERR_CUDA;
+            }
+            out[q].assign(htree.begin() + (size_t)q * 64, htree.begin() + (size_t)q * 64 + hn[q]);
+        }
+        for (int k = 2; k <= maxn; k++) st.connected_sets += hl[k].n_sets;
+        st.evaluated_pairs += hg.evaluated_pairs;
+        st.memo_bytes = std::max<uint64_t>(st.memo_bytes, slots * (sizeof(float4) + 4));
+        st.device_ms += fms;
+        st.kernel_launches += kernels;
+        return 0;
+    }
+};
+
+static std::map<int, std::unique_ptr<BatchEngine>> g_batch;
+
+int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, uint64_t wave_bytes,
+                     std::vector<std::vector<TreeNode>> &out, EngineStats &st, std::vector<double> &wave_ms,
+                     std::string &err) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        err = "cudaGetDevice failed";
+        return GPUQO_B200_ERR_CUDA;
+    }
+    auto &be = g_batch[dev];
+    if (!be) be.reset(new BatchEngine());
+    if (int rc = be->init(err)) return rc;
+    out.assign(blobs.size(), {});
+    // waves: consecutive queries while the wave's memory stays within budget
+    size_t i = 0;
+    while (i < blobs.size()) {
+        std::vector<const std::vector<uint32_t> *> wave;
+        std::vector<size_t> idx;
+        uint64_t bytes = 0;
+        while (i < blobs.size()) {
+            const int n = reinterpret_cast<const DevHeader *>(blobs[i]->data())->n;
+            const uint64_t b = batch_query_bytes(n);
+            if (!wave.empty() && bytes + b > wave_bytes) break;
+            wave.push_back(blobs[i]);
+            idx.push_back(i);
+            bytes += b;
+            i++;
+        }
+        std::vector<std::vector<TreeNode>> wout;
+        double ms = 0;
+        if (int rc = be->run_wave(wave, wout, st, ms, err)) return rc;
+        wave_ms.push_back(ms);
+        for (size_t j = 0; j < idx.size(); j++) out[idx[j]] = std::move(wout[j]);
+    }
+    return 0;
+}
+
+}  // namespace gqb

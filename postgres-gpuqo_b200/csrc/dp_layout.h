@@ -35,8 +35,10 @@ struct DevHeader {
     uint32_t composite_mask;
     uint32_t blob_words;                  // total blob size in 32-bit words
     uint32_t max_block;                   // largest biconnected block of the query graph
-    uint32_t tree_mode;                   // query graph is a tree (tparent/tsub valid)
+    uint32_t tree_mode;                   // query graph is a tree (tree tables present)
     uint32_t ec_masked;                   // tree_mode and every class is a 2-member class on an edge
+    uint32_t tree_tab;                    // word offset of the tree tables (see below), 0 if none
+    uint32_t pad;
     uint32_t adj[kMaxRels];
     float rows[kMaxRels];
     float tuples[kMaxRels];
@@ -46,16 +48,20 @@ struct DevHeader {
     // fkselc_of_ec's value for a foreign key into relation i:
     // (float)(1.0 / (double)fmaxf(1.0f, tuples[i])) (gpuqo_row_estimation.cuh:36-38)
     float fksel[kMaxRels];
-    // tree_mode: parent of relation i in the query tree rooted at relation 0,
-    // relations of the subtree under i, and the classes on edge (parent, i)
-    int tparent[kMaxRels];
-    uint32_t tsub[kMaxRels];
+    // ec_masked: the classes on the edge between relation i and its parent
+    // when the query tree is rooted at relation 0
     uint32_t edge_ec[kMaxRels];
-    // tree_mode: relations before i in the query tree's preorder (children
-    // visited in increasing index order) and the proper ancestors of i
-    uint32_t tbefore[kMaxRels];
-    uint32_t tanc[kMaxRels];
 };
+
+// Tree tables (tree_mode), appended after the class arrays: for every root r
+// of the query tree and relation v, with children visited in increasing
+// index order,
+//   tab[0*n*n + r*n + v] = relations of v's subtree,
+//   tab[1*n*n + r*n + v] = relations preceding v in preorder,
+//   tab[2*n*n + r*n + v] = proper ancestors of v.
+// A connected set S is a subtree; the reference's block search walks it from
+// its lowest relation r in exactly this preorder.
+GQB_HD inline uint32_t tree_tab_words(int n) { return 3u * (uint32_t)n * (uint32_t)n; }
 
 struct DevInfoView {
     const DevHeader *h;

@@ -76,6 +76,7 @@ int gpuqo_dplin_threshold_lindp = 14;
 int gpuqo_dplin_threshold_idp = 100;
 
 int gpuqo_b200_profile_kernels = 0;
+int gpuqo_b200_batch_memory_mb = 32768;
 }
 
 namespace gqb {
@@ -329,9 +330,27 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     const int n_ec = (int)info.ec_relids.size();
     const int n_sels = (int)info.ec_sels.size();
     const int n_fks = (int)info.ec_fks.size();
-    std::vector<uint32_t> blob(blob_words_for(n_ec, n_sels, n_fks), 0u);
+    const int n = info.n;
+    // tree-shaped query graph: n - 1 edges, connected
+    int n_edges = 0;
+    for (int i = 0; i < n; i++) n_edges += popc64(info.edge[i]);
+    n_edges /= 2;
+    bool tree = (n_edges == n - 1);
+    if (tree) {
+        mask64 seen = 1, frontier = 1;
+        while (frontier) {
+            mask64 next = 0;
+            for (int i = 0; i < n; i++)
+                if (frontier & bit64(i)) next |= info.edge[i] >> 1;
+            frontier = next & ~seen;
+            seen |= next;
+        }
+        tree = (seen == (n == 64 ? ~0ull : (bit64(n) - 1)));
+    }
+    const uint32_t base_words = blob_words_for(n_ec, n_sels, n_fks);
+    std::vector<uint32_t> blob(base_words + (tree ? tree_tab_words(n) : 0u), 0u);
     DevHeader *h = reinterpret_cast<DevHeader *>(blob.data());
-    h->n = info.n;
+    h->n = n;
     h->n_ec = n_ec;
     h->n_sels = n_sels;
     h->n_fks = n_fks;
@@ -345,7 +364,7 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     h->composite_mask = 0;
     h->blob_words = (uint32_t)blob.size();
     h->max_block = (uint32_t)max_block_size(info);
-    for (int i = 0; i < info.n; i++) {
+    for (int i = 0; i < n; i++) {
         h->adj[i] = (uint32_t)(info.edge[i] >> 1);
         h->rows[i] = info.base[i].rows;
         h->tuples[i] = info.base[i].tuples;
@@ -355,63 +374,62 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         h->fksel[i] = (float)(1.0 / (double)std::fmax(1.0f, info.base[i].tuples));
         if (info.base[i].composite) h->composite_mask |= 1u << i;
     }
-    // Tree-shaped query graph (after BFS relabelling, every relation's parent
-    // is its only neighbour with a smaller index): parents, subtree masks and
-    // the classes sitting on each edge.
-    int n_edges = 0;
-    for (int i = 0; i < info.n; i++) n_edges += popc64(info.edge[i]);
-    n_edges /= 2;
-    bool tree = (n_edges == info.n - 1);
-    for (int i = 1; tree && i < info.n; i++) {
-        uint32_t lower = h->adj[i] & ((1u << i) - 1u);
-        if (popc64(lower) != 1) tree = false;
-        else h->tparent[i] = __builtin_ctz(lower);
-    }
-    h->tparent[0] = -1;
     h->tree_mode = tree ? 1u : 0u;
     h->ec_masked = 0u;
+    h->tree_tab = 0u;
     if (tree) {
-        for (int i = info.n - 1; i >= 0; i--) {
-            h->tsub[i] |= 1u << i;
-            if (i > 0) h->tsub[h->tparent[i]] |= h->tsub[i];
-        }
-        // preorder from relation 0, children in increasing index order (the
-        // order in which the reference's block search walks any subtree)
-        {
-            std::vector<int> stack(1, 0);
-            uint32_t seen_before = 0u;
+        h->tree_tab = base_words;
+        uint32_t *tab = blob.data() + base_words;
+        const int nn = n * n;
+        for (int r = 0; r < n; r++) {
+            // preorder from r, children in increasing index order
+            std::vector<int> parent(n, -1), order;
+            std::vector<int> stack(1, r);
+            std::vector<uint32_t> anc(n, 0u);
+            uint32_t before = 0u;
             while (!stack.empty()) {
                 int u = stack.back();
                 stack.pop_back();
-                h->tbefore[u] = seen_before;
-                seen_before |= 1u << u;
-                h->tanc[u] = (u == 0) ? 0u : (h->tanc[h->tparent[u]] | (1u << h->tparent[u]));
-                uint32_t kids = h->adj[u] & ~((2u << u) - 1u);   // children have larger indices
+                tab[nn + r * n + u] = before;
+                before |= 1u << u;
+                order.push_back(u);
+                tab[2 * nn + r * n + u] = anc[u];
+                uint32_t kids = h->adj[u];
+                if (parent[u] >= 0) kids &= ~(1u << parent[u]);
                 std::vector<int> ch;
                 while (kids) {
                     ch.push_back(__builtin_ctz(kids));
                     kids &= kids - 1u;
                 }
-                for (auto it = ch.rbegin(); it != ch.rend(); ++it) stack.push_back(*it);
+                for (auto it = ch.rbegin(); it != ch.rend(); ++it) {
+                    parent[*it] = u;
+                    anc[*it] = anc[u] | (1u << u);
+                    stack.push_back(*it);
+                }
             }
+            for (int v = 0; v < n; v++) tab[r * n + v] = 1u << v;
+            for (auto it = order.rbegin(); it != order.rend(); ++it)
+                if (parent[*it] >= 0) tab[r * n + parent[*it]] |= tab[r * n + *it];
         }
+        // classes on edges: every 2-member class must sit on an edge
         bool masked = n_ec <= 32;
         for (int e = 0; masked && e < n_ec; e++) {
-            uint32_t r = (uint32_t)(info.ec_relids[e] >> 1);
-            if (popc64(r) != 2) {
+            uint32_t rr = (uint32_t)(info.ec_relids[e] >> 1);
+            if (popc64(rr) != 2) {
                 masked = false;
                 break;
             }
-            int a = __builtin_ctz(r), b = 31 - __builtin_clz(r);   // a < b
-            if (h->tparent[b] != a) {
+            int a = __builtin_ctz(rr), b = 31 - __builtin_clz(rr);
+            if (!((h->adj[a] >> b) & 1u)) {
                 masked = false;   // a class between relations that are not adjacent
                 break;
             }
-            h->edge_ec[b] |= 1u << e;
+            int child0 = ((tab[2 * nn + 0 * n + b] >> a) & 1u) ? b : a;
+            h->edge_ec[child0] |= 1u << e;
         }
         if (masked) h->ec_masked = 1u;
         else
-            for (int i = 0; i < info.n; i++) h->edge_ec[i] = 0u;
+            for (int i = 0; i < n; i++) h->edge_ec[i] = 0u;
     }
     DevInfoView v = make_view(blob.data());
     uint32_t *relids = const_cast<uint32_t *>(v.ec_relids);
@@ -608,9 +626,70 @@ extern "C" int gpuqo_b200_time_resident(int gpuqo_algorithm_arg, GpuqoPlannerInf
 extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC **infos, int n_queries,
                                     QueryTreeC **out) {
     stats_reset();
+    t_last_error = GPUQO_B200_OK;
     if (!infos || !out || n_queries < 0) return GPUQO_B200_ERR_ARGS;
-    int status = GPUQO_B200_OK;
+    for (int i = 0; i < n_queries; i++) out[i] = NULL;
+    if (!algorithm_supported(gpuqo_algorithm_arg)) {
+        set_error(GPUQO_B200_ERR_UNSUPPORTED, "algorithm outside this library");
+        return GPUQO_B200_ERR_UNSUPPORTED;
+    }
+    const DpMode mode = mode_for(gpuqo_algorithm_arg);
+    // Prepare every query as gpuqo_run does (convert, BFS relabel); MPDP
+    // queries without IDP whose candidate count fits the batched kernel go to
+    // the level-synchronous batch, the rest run one by one.
+    struct Prep {
+        std::vector<int> order;
+        std::vector<uint32_t> blob;
+    };
+    std::vector<Prep> prep(n_queries);
+    std::vector<int> batched, single;
     for (int i = 0; i < n_queries; i++) {
+        GpuqoPlannerInfoC *c = infos[i];
+        const bool idp = c && gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < c->n_rels;
+        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp || mode != kModeMpdp) {
+            single.push_back(i);
+            continue;
+        }
+        HostInfo info;
+        std::string err;
+        if (!convert_info(c, info, err)) {
+            single.push_back(i);
+            continue;
+        }
+        prep[i].order = bfs_order(info);
+        if ((int)prep[i].order.size() != info.n) {
+            single.push_back(i);
+            continue;
+        }
+        HostInfo remapped = relabel(info, prep[i].order);
+        prep[i].blob = build_blob(remapped);
+        if (batch_eligible(prep[i].blob)) batched.push_back(i);
+        else single.push_back(i);
+    }
+    int status = GPUQO_B200_OK;
+    if (!batched.empty()) {
+        // larger queries first: a wave then runs only the levels it needs
+        std::stable_sort(batched.begin(), batched.end(), [&](int a, int b) {
+            return infos[a]->n_rels > infos[b]->n_rels;
+        });
+        std::vector<const std::vector<uint32_t> *> blobs;
+        for (int i : batched) blobs.push_back(&prep[i].blob);
+        std::vector<std::vector<TreeNode>> nodes;
+        std::vector<double> wave_ms;
+        EngineStats st;
+        std::string err;
+        const uint64_t budget = (uint64_t)std::max(gpuqo_b200_batch_memory_mb, 64) << 20;
+        int rc = engine_run_batch(blobs, budget, nodes, st, wave_ms, err);
+        if (rc) {
+            set_error(rc, err);
+            return rc;
+        }
+        stats_add(st);
+        t_stats.n_subproblems = (uint32_t)batched.size();
+        for (size_t j = 0; j < batched.size(); j++)
+            out[batched[j]] = nodes_to_c(nodes[j], 0, prep[batched[j]].order);
+    }
+    for (int i : single) {
         out[i] = run_one(gpuqo_algorithm_arg, infos[i]);
         if (!out[i]) status = t_last_error;
     }

@@ -366,3 +366,23 @@ SHAPES = {"star": star, "snowflake": snowflake, "clique": clique,
 
 def make(shape: str, n: int, seed: int, **kw) -> Query:
     return SHAPES[shape](n, seed, **kw)
+
+
+def batch_mix(n_queries: int, seed: int, nmin: int = 8, nmax: int = 28) -> List[Query]:
+    """The batched workload: relation counts uniform in [nmin, nmax], shapes
+    40% star / 40% snowflake / 10% chain / 10% cycle, each query seeded."""
+    rng = np.random.default_rng([seed, 8, n_queries, nmin, nmax])
+    out = []
+    for i in range(n_queries):
+        n = int(rng.integers(nmin, nmax + 1))
+        u = rng.uniform()
+        if u < 0.4:
+            q = star(n, seed * 100003 + i)
+        elif u < 0.8:
+            q = snowflake(n, seed * 100003 + i)
+        elif u < 0.9:
+            q = chain(max(n, 2), seed * 100003 + i)
+        else:
+            q = cycle(max(n, 3), seed * 100003 + i)
+        out.append(q)
+    return out
