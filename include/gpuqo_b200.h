@@ -265,6 +265,35 @@ extern int gpuqo_b200_batch_memory_mb;
 int gpuqo_b200_run_batch(int gpuqo_algorithm, GpuqoPlannerInfoC **infos,
                          int n_queries, QueryTreeC **out);
 
+/*
+ * Continuous-batching planner service (standalone planning processes; inside
+ * a Postgres backend use gpuqo_run).  Requests are planned concurrently, at
+ * most max_inflight at a time (later ones wait for a slot); every exact DP a
+ * request needs (one, or one per IDP2 / UnionDP iteration) is run by a single
+ * scheduler in level-synchronous waves together with the pending sub-problems
+ * of all other requests, each wave admitted by dense-memo bytes
+ * (wave_memory_mb).  A request's plan equals gpuqo_run's for the same query
+ * and the GUC settings current at submit time (gpuqo_algorithm argument,
+ * gpuqo_dpsub_bicc_enable, gpuqo_idp_n_iters, gpuqo_idp_type).
+ *
+ * submit copies what it needs from info (the caller may free it on return)
+ * and returns a ticket; wait blocks until that request is planned and hands
+ * back its tree (palloc'd) and its latency from submit to completion.
+ */
+typedef struct GpuqoB200ServerStats {
+    uint64_t completed;             /* requests planned */
+    uint64_t waves;                 /* batched waves run */
+    uint64_t batched_subproblems;   /* exact DPs run inside waves */
+    uint64_t single_subproblems;    /* exact DPs run one by one */
+    double device_ms;               /* device time of all waves and singles */
+} GpuqoB200ServerStats;
+
+int gpuqo_b200_server_start(int max_inflight, int wave_memory_mb);
+int gpuqo_b200_server_submit(int gpuqo_algorithm, GpuqoPlannerInfoC *info, uint64_t *ticket);
+int gpuqo_b200_server_wait(uint64_t ticket, QueryTreeC **out, double *latency_ms);
+int gpuqo_b200_server_stats(GpuqoB200ServerStats *out);
+int gpuqo_b200_server_stop(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -534,6 +534,7 @@ struct Ctx {
     Arena A;
     int err = 0;
     std::string msg;
+    SubSolver solve;        // exact DP of one remapped sub-problem
 };
 
 static QT *nodes_to_qt(const std::vector<TreeNode> &nodes, int idx, Arena &A) {
@@ -562,7 +563,7 @@ static QT *solve_sub(const GInfo &info, const std::vector<Entry> &list, Ctx &C) 
         return nullptr;
     }
     std::vector<TreeNode> nodes;
-    int rc = exact_dp(h, C.mode, nodes, C.msg);
+    int rc = C.solve ? C.solve(h, C.mode, nodes, C.msg) : exact_dp(h, C.mode, nodes, C.msg);
     if (rc) {
         C.err = rc;
         return nullptr;
@@ -831,6 +832,74 @@ static QueryTreeC *qt_to_c(const QT *q) {
     return o;
 }
 
+// One planning request (__gpuqo_run, gpuqo_main_internal.cu:82-160): BFS
+// relabel, IDP2 / UnionDP or one exact DP, plan mapped back to the caller's
+// numbering.  Settings are captured by the caller (no GUC reads here).
+struct Planner {
+    Ctx C;
+    GInfo g;
+    int idp_n_iters = 0, idp_type = GPUQO_IDP2;
+    QT *result = nullptr;
+
+    int run() {
+        std::vector<Entry> bl = bfs_list(g);
+        if ((int)bl.size() != g.n) {
+            C.msg = "query graph is not connected";
+            return GPUQO_B200_ERR_ARGS;
+        }
+        Remap R(bl, g.n);
+        GInfo rg = R.info(g);
+        const bool idp = idp_n_iters > 1 && idp_n_iters < g.n;
+        QT *qt = nullptr;
+        if (idp) {
+            if (idp_type == GPUQO_IDP2) qt = run_idp2(rg, idp_n_iters, C);
+            else if (idp_type == GPUQO_UNION) qt = union_rec(rg, identity_list(rg), idp_n_iters, C);
+            else {
+                C.msg = "gpuqo_idp_type: only IDP2 and UNION are provided";
+                return GPUQO_B200_ERR_UNSUPPORTED;
+            }
+        } else if (g.n <= 31) {
+            HostInfo h;
+            if (int rc = to_host_info(rg, h, C.msg)) return rc;
+            std::vector<TreeNode> nodes;
+            int rc = C.solve ? C.solve(h, C.mode, nodes, C.msg) : exact_dp(h, C.mode, nodes, C.msg);
+            if (rc) return rc;
+            qt = nodes_to_qt(nodes, 0, C.A);
+        } else {
+            C.msg = std::to_string(g.n) + " relations need IDP (set gpuqo_idp_n_iters between 2 and n-1)";
+            return GPUQO_B200_ERR_UNSUPPORTED;
+        }
+        if (!qt) return C.err ? C.err : GPUQO_B200_ERR_ARGS;
+        result = R.tree_back(qt, C.A);
+        return 0;
+    }
+};
+
+PlannerHandle *planner_new(int algorithm, const GpuqoPlannerInfoC *info_c, int idp_n_iters, int idp_type,
+                           SubSolver solver, std::string &err) {
+    Planner *p = new Planner();
+    if (!convert_big(info_c, p->g, err)) {
+        delete p;
+        return nullptr;
+    }
+    p->C.mode = mode_for(algorithm);
+    p->C.solve = std::move(solver);
+    p->idp_n_iters = idp_n_iters;
+    p->idp_type = idp_type;
+    return reinterpret_cast<PlannerHandle *>(p);
+}
+
+int planner_run(PlannerHandle *h, std::string &err) {
+    Planner *p = reinterpret_cast<Planner *>(h);
+    int rc = p->run();
+    if (rc) err = p->C.msg.empty() ? "planning failed" : p->C.msg;
+    return rc;
+}
+
+QueryTreeC *planner_result(PlannerHandle *h) { return qt_to_c(reinterpret_cast<Planner *>(h)->result); }
+
+void planner_free(PlannerHandle *h) { delete reinterpret_cast<Planner *>(h); }
+
 QueryTreeC *run_idp(int algorithm, GpuqoPlannerInfoC *info_c) {
     std::string err;
     const int n = info_c->n_rels;
@@ -844,29 +913,16 @@ QueryTreeC *run_idp(int algorithm, GpuqoPlannerInfoC *info_c) {
         set_error(GPUQO_B200_ERR_UNSUPPORTED, "gpuqo_idp_type: only IDP2 and UNION are provided");
         return nullptr;
     }
-    GInfo g;
-    if (!convert_big(info_c, g, err)) {
+    PlannerHandle *h = planner_new(algorithm, info_c, gpuqo_idp_n_iters, gpuqo_idp_type, nullptr, err);
+    if (!h) {
         set_error(GPUQO_B200_ERR_ARGS, err);
         return nullptr;
     }
-    Ctx C;
-    C.mode = mode_for(algorithm);
-    // __gpuqo_run (gpuqo_main_internal.cu:102-137): BFS relabel, IDP, map back
-    std::vector<Entry> bl = bfs_list(g);
-    if ((int)bl.size() != g.n) {
-        set_error(GPUQO_B200_ERR_ARGS, "query graph is not connected");
-        return nullptr;
-    }
-    Remap R(bl, g.n);
-    GInfo rg = R.info(g);
-    QT *qt = (gpuqo_idp_type == GPUQO_IDP2) ? run_idp2(rg, gpuqo_idp_n_iters, C)
-                                             : union_rec(rg, identity_list(rg), gpuqo_idp_n_iters, C);
-    if (!qt) {
-        set_error(C.err ? C.err : GPUQO_B200_ERR_ARGS, C.msg.empty() ? "IDP failed" : C.msg);
-        return nullptr;
-    }
-    QT *back = R.tree_back(qt, C.A);
-    return qt_to_c(back);
+    int rc = planner_run(h, err);
+    QueryTreeC *out = rc ? nullptr : planner_result(h);
+    planner_free(h);
+    if (rc) set_error(rc, err);
+    return out;
 }
 
 }  // namespace gqb

@@ -56,6 +56,17 @@ def load():
                                                  C.c_int, C.POINTER(C.c_double),
                                                  C.POINTER(C.POINTER(capi.QueryTreeC))]
         lib.gpuqo_b200_time_resident.restype = C.c_int
+        lib.gpuqo_b200_server_start.argtypes = [C.c_int, C.c_int]
+        lib.gpuqo_b200_server_start.restype = C.c_int
+        lib.gpuqo_b200_server_submit.argtypes = [C.c_int, C.POINTER(capi.GpuqoPlannerInfoC), C.POINTER(C.c_uint64)]
+        lib.gpuqo_b200_server_submit.restype = C.c_int
+        lib.gpuqo_b200_server_wait.argtypes = [C.c_uint64, C.POINTER(C.POINTER(capi.QueryTreeC)),
+                                               C.POINTER(C.c_double)]
+        lib.gpuqo_b200_server_wait.restype = C.c_int
+        lib.gpuqo_b200_server_stats.argtypes = [C.c_void_p]
+        lib.gpuqo_b200_server_stats.restype = C.c_int
+        lib.gpuqo_b200_server_stop.argtypes = []
+        lib.gpuqo_b200_server_stop.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -153,3 +164,57 @@ def get_stats() -> Dict:
     st = Stats()
     lib.gpuqo_b200_get_stats(C.byref(st))
     return st.to_dict()
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("waves", C.c_uint64), ("batched_subproblems", C.c_uint64),
+                ("single_subproblems", C.c_uint64), ("device_ms", C.c_double)]
+
+
+class Server:
+    """The library's continuous-batching planner service (C ABI
+    gpuqo_b200_server_*).  submit() captures the GUCs current at the call."""
+
+    def __init__(self, max_inflight: int = 16, wave_memory_mb: int = 32768):
+        self.lib = load()
+        rc = self.lib.gpuqo_b200_server_start(max_inflight, wave_memory_mb)
+        if rc:
+            raise RuntimeError(f"gpuqo_b200_server_start: {rc}")
+        self._keep = {}
+
+    def submit(self, q: Query, algorithm: int = capi.GPUQO_DPSUB, bicc: Optional[bool] = None,
+               idp_n_iters: int = 0, idp_type: int = capi.GPUQO_IDP2) -> int:
+        if bicc is not None:
+            capi.set_bool(self.lib, "gpuqo_dpsub_bicc_enable", bicc)
+        capi.set_int(self.lib, "gpuqo_idp_n_iters", idp_n_iters)
+        capi.set_int(self.lib, "gpuqo_idp_type", idp_type)
+        b = capi.PlannerInfoBuilder(q)
+        t = C.c_uint64(0)
+        rc = self.lib.gpuqo_b200_server_submit(algorithm, b.pointer(), C.byref(t))
+        if rc:
+            raise RuntimeError(f"gpuqo_b200_server_submit: {rc}")
+        return t.value
+
+    def submit_built(self, b: "capi.PlannerInfoBuilder", algorithm: int = capi.GPUQO_DPSUB) -> int:
+        t = C.c_uint64(0)
+        rc = self.lib.gpuqo_b200_server_submit(algorithm, b.pointer(), C.byref(t))
+        if rc:
+            raise RuntimeError(f"gpuqo_b200_server_submit: {rc}")
+        return t.value
+
+    def wait(self, ticket: int):
+        out = C.POINTER(capi.QueryTreeC)()
+        lat = C.c_double(0.0)
+        rc = self.lib.gpuqo_b200_server_wait(ticket, C.byref(out), C.byref(lat))
+        tree = capi.tree_to_py(out) if (rc == 0 and out) else None
+        if out:
+            self.lib.gpuqo_b200_free_query_tree(C.cast(out, C.c_void_p))
+        return rc, tree, lat.value
+
+    def stats(self) -> Dict:
+        st = ServerStats()
+        self.lib.gpuqo_b200_server_stats(C.byref(st))
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def stop(self):
+        self.lib.gpuqo_b200_server_stop()
