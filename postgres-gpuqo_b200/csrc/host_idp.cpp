@@ -85,7 +85,9 @@ struct BB {
     BB all_lower() const {
         BB b;
         int p = lowest_pos();
-        for (int i = 0; i < p; i++) b.set(i);
+        if (p < 0) return b;
+        for (int i = 0; i < (p >> 6); i++) b.w[i] = ~0ull;
+        if (p & 63) b.w[p >> 6] = (1ull << (p & 63)) - 1ull;
         return b;
     }
     BB operator|(const BB &o) const {
@@ -160,13 +162,18 @@ struct GInfo {
     std::vector<BB> fks;
     std::vector<VarInfo> vars;
     std::vector<int> ec_off_sels, ec_off_fks;
+    std::vector<std::vector<int>> rel_ecs;     // per relation: classes containing it, increasing
     void index() {
         ec_members.assign(ec.size(), {});
         ec_off_sels.assign(ec.size(), 0);
         ec_off_fks.assign(ec.size(), 0);
+        rel_ecs.assign(n, {});
         int os = 0, of = 0;
         for (size_t i = 0; i < ec.size(); i++) {
-            ec.at(i).for_each([&](int b) { ec_members[i].push_back(b - 1); });
+            ec.at(i).for_each([&](int b) {
+                ec_members[i].push_back(b - 1);
+                if (b - 1 < n) rel_ecs[b - 1].push_back((int)i);
+            });
             ec_off_sels[i] = os;
             ec_off_fks[i] = of;
             int s = (int)ec_members[i].size();
@@ -240,13 +247,22 @@ static float estimate_ec_selectivity(const GInfo &g, int e, const BB &l, const B
     return g.sels[g.ec_off_sels[e] + ec_index(il, ir, size)];
 }
 
-// :93-118
+// :93-118.  Only classes with a member on both sides contribute a factor
+// other than 1.0f; they are found through the smaller side's relations and
+// multiplied in increasing class order, as the reference's loop does.
 static float estimate_join_selectivity(const GInfo &g, const BB &l, const BB &r) {
+    const BB &small = (l.size() <= r.size()) ? l : r;
+    const BB &other = (&small == &l) ? r : l;
+    std::vector<int> hit;
+    small.for_each([&](int b) {
+        if (b - 1 >= g.n) return;
+        for (int e : g.rel_ecs[b - 1])
+            if (ec_hits(g, e, other)) hit.push_back(e);
+    });
+    std::sort(hit.begin(), hit.end());
+    hit.erase(std::unique(hit.begin(), hit.end()), hit.end());
     float sel = 1.0f;
-    for (size_t e = 0; e < g.ec.size(); e++) {
-        if (!ec_hits(g, (int)e, l) || !ec_hits(g, (int)e, r)) continue;   // factor 1.0f
-        sel *= estimate_ec_selectivity(g, (int)e, l, r);
-    }
+    for (int e : hit) sel *= estimate_ec_selectivity(g, e, l, r);
     return sel;
 }
 
@@ -326,11 +342,17 @@ class Remap {
 public:
     std::vector<Entry> list;
     std::vector<int> owner;     // relation index (bit - 1) -> entry position, -1 if none
+    std::vector<int> of_to;     // target index -> entry position, -1 if none
     Remap(const std::vector<Entry> &l, int n_from) : list(l), owner(n_from, -1) {
-        for (size_t k = 0; k < list.size(); k++)
+        int max_to = -1;
+        for (size_t k = 0; k < list.size(); k++) {
             list[k].from.for_each([&](int b) {
                 if (b - 1 < n_from) owner[b - 1] = (int)k;
             });
+            max_to = std::max(max_to, list[k].to);
+        }
+        of_to.assign(max_to + 1, -1);
+        for (size_t k = 0; k < list.size(); k++) of_to[list[k].to] = (int)k;
     }
     // remapRelid (:49-59)
     BB rel(const BB &id) const {
@@ -356,19 +378,26 @@ public:
     // remapRelidInv (:77-87)
     BB inv(const BB &id) const {
         BB out;
-        for (const Entry &e : list)
-            if (id.test(e.to + 1)) out |= e.from;
+        id.for_each([&](int b) {
+            int t = b - 1;
+            if (t < (int)of_to.size() && of_to[t] >= 0) out |= list[of_to[t]].from;
+        });
         return out;
     }
-    bool ec_inside_one_entry(const GInfo &g, int e) const {
-        int k0 = -2;
+    // Classes whose members fall into fewer than two entries: with entries
+    // covering every relation these are the reference's dropped classes (a
+    // subset of one entry, countEqClasses :19-47); for a sub-problem's remap
+    // they also include classes left with 0 or 1 member, which can never
+    // match a join pair.  Either way they are not needed downstream.
+    bool ec_below_two_entries(const GInfo &g, int e) const {
+        int k0 = -1;
         for (int m : g.ec_members[e]) {
             int k = owner[m];
-            if (k < 0) return false;
-            if (k0 == -2) k0 = k;
+            if (k < 0) continue;
+            if (k0 < 0) k0 = k;
             else if (k != k0) return false;
         }
-        return k0 >= 0;
+        return true;
     }
 
     // remapPlannerInfo (:201-277) with remapEdgeTable / remapBaseRels /
@@ -401,7 +430,7 @@ public:
             tb.composite = (e.from.size() == 1) ? from.base[e.from.lowest_pos() - 1].composite : true;
         }
         for (size_t i = 0; i < from.ec.size(); i++) {
-            if (ec_inside_one_entry(from, (int)i)) continue;
+            if (ec_below_two_entries(from, (int)i)) continue;
             const BB &ecf = from.ec[i];
             BB ect = rel(ecf);
             int s_from = (int)from.ec_members[i].size();
@@ -443,13 +472,14 @@ public:
         if (!qt) return nullptr;
         if (qt->id.size() == 1) {
             int idx = qt->id.lowest_pos() - 1;
-            for (const Entry &e : list)
-                if (e.qt && e.to == idx) return e.qt;
+            if (idx < (int)of_to.size() && of_to[idx] >= 0 && list[of_to[idx]].qt) return list[of_to[idx]].qt;
         }
         QT *o = A.make();
-        o->id = inv(qt->id);
         o->left = tree_back(qt->left, A);
         o->right = tree_back(qt->right, A);
+        // inv distributes over union: an internal node's set is its children's
+        if (o->left && o->right && (qt->left->id | qt->right->id) == qt->id) o->id = o->left->id | o->right->id;
+        else o->id = inv(qt->id);
         o->rows = qt->rows;
         o->cost = qt->cost;
         o->width = qt->width;
@@ -460,12 +490,24 @@ public:
     QT *tree_fwd(const QT *qt, Arena &A) const {
         if (!qt) return nullptr;
         QT *o = A.make();
-        o->id = rel(qt->id);
+        // rel distributes over union: an internal node's set is its children's
+        QT *l = nullptr, *r = nullptr;
+        if (qt->left && qt->right && (qt->left->id | qt->right->id) == qt->id) {
+            l = tree_fwd(qt->left, A);
+            r = tree_fwd(qt->right, A);
+            o->id = l->id | r->id;
+        } else {
+            o->id = rel(qt->id);
+            if (o->id.size() != 1) {
+                l = tree_fwd(qt->left, A);
+                r = tree_fwd(qt->right, A);
+            }
+        }
         if (o->id.size() == 1) {
             o->left = o->right = nullptr;
         } else {
-            o->left = tree_fwd(qt->left, A);
-            o->right = tree_fwd(qt->right, A);
+            o->left = l;
+            o->right = r;
         }
         o->rows = qt->rows;
         o->cost = qt->cost;
@@ -520,12 +562,24 @@ static int to_host_info(const GInfo &g, HostInfo &h, std::string &err) {
         h.base[i].cost = g.base[i].cost;
         h.base[i].composite = g.base[i].composite;
     }
+    // Classes with fewer than two members after remapping (the remapper keeps
+    // them, emptied) never match a join pair - they contribute a factor 1 to
+    // the selectivity, no quals, no bucket or index candidates - so the DP
+    // gets only the classes that can match; its results are unchanged.
     h.ec_relids.clear();
-    for (const BB &e : g.ec) h.ec_relids.push_back(m64(e));
-    h.ec_sels = g.sels;
+    h.ec_sels.clear();
     h.ec_fks.clear();
-    for (const BB &f : g.fks) h.ec_fks.push_back(m64(f));
-    h.ec_vars = g.vars;
+    h.ec_vars.clear();
+    for (size_t e = 0; e < g.ec.size(); e++) {
+        const int s = (int)g.ec_members[e].size();
+        if (s < 2) continue;
+        h.ec_relids.push_back(m64(g.ec[e]));
+        for (int j = 0; j < s * (s - 1) / 2; j++) h.ec_sels.push_back(g.sels[g.ec_off_sels[e] + j]);
+        for (int j = 0; j < s; j++) {
+            h.ec_fks.push_back(m64(g.fks[g.ec_off_fks[e] + j]));
+            h.ec_vars.push_back(g.vars[g.ec_off_fks[e] + j]);
+        }
+    }
     return 0;
 }
 
