@@ -8,14 +8,16 @@ the only collectives.
 
 Printed (rank 0, one JSON line):
   value  - ms per query of the device-resident DP: the planner info is on the
-           device, the captured DP graph is replayed, CUDA events on the
-           library's stream, L2 flushed (256 MB write) before every step;
+           device, the DP runs as one persistent cooperative launch
+           (k_dp_tree: every level's enumeration and evaluation, grid
+           barrier between levels), CUDA events on the library's stream, L2
+           flushed (256 MB write) before every step;
   e2e    - ms per query through the C ABI gpuqo_run with host structures
            (conversion, H2D of the planner info, the DP, D2H of the plan);
-  roofline - the evaluate kernel (k_eval): algorithmic memo bytes per launch
-           (32 B per evaluated csg-cmp pair: two 16 B memo reads; 20 B per
-           connected set written) over its event-timed launch duration,
-           against the measured HBM copy bandwidth;
+  roofline - k_dp_tree: algorithmic memo bytes per launch (32 B per
+           evaluated csg-cmp pair: two 16 B memo reads; 20 B per connected set
+           written) over its event-timed launch duration, against the
+           measured HBM copy bandwidth;
   cpu_baseline - the reference's parallel_cpu_dpsub_bicc (its own code,
            compiled from its sources into oracle/_ref) on the host cores.
 
@@ -56,8 +58,8 @@ def measured_peaks():
 
 
 def profiled_traffic():
-    """DRAM bytes per k_eval launch from the committed ncu summary, if any."""
-    p = os.path.join(REPO, "profiles", "k_eval_tree_snowflake25.md")
+    """DRAM bytes per k_dp_tree launch from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "k_dp_tree_snowflake25.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -150,7 +152,7 @@ def cpu_reference_sample(queries, steps=None, budget_s=20.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -282,7 +284,7 @@ def main():
             "pairs_per_s": pairs / (tot_ms / 1000.0) if tot_ms > 0 else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_eval_tree (MPDP)", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None},
+                         "kernel": "k_dp_tree (MPDP, persistent)", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None},
             "e2e": {"value": e2e_value, "unit": "ms/query", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": kernels,

@@ -207,6 +207,12 @@ void gpuqo_b200_get_stats(GpuqoB200Stats *out);
  * launch (for the kernel-time figures in the stats); off by default. */
 extern int gpuqo_b200_profile_kernels;
 
+/* When non-zero (default), MPDP on a tree-shaped query graph runs as one
+ * persistent cooperative kernel with a grid barrier between levels; zero
+ * selects the per-level launches (also used automatically when a cooperative
+ * launch is not possible or its barrier times out). */
+extern int gpuqo_b200_persistent;
+
 /*
  * Device-resident timing of the exact DP of one query (< 32 relations, no
  * IDP): the planner info is converted and uploaded once, then the captured DP

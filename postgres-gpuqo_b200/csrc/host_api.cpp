@@ -77,6 +77,7 @@ int gpuqo_dplin_threshold_idp = 100;
 
 int gpuqo_b200_profile_kernels = 0;
 int gpuqo_b200_batch_memory_mb = 32768;
+int gpuqo_b200_persistent = 1;
 }
 
 namespace gqb {

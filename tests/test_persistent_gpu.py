@@ -1,0 +1,84 @@
+"""GPU: the persistent tree-mode MPDP kernel (one cooperative launch per DP,
+grid barrier between levels) against the per-level launches and the oracle.
+
+gpuqo_b200_persistent selects the path (default 1).  Both paths must return
+bit-identical plans; the persistent one must report a single kernel launch,
+and queries that are not tree-shaped must keep the per-level path.
+"""
+import pytest
+
+from conftest import same_tree
+
+import harness
+from gpuqo_b200 import capi, lib, query
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(q, persistent):
+    capi.set_int(lib.load(), "gpuqo_b200_persistent", 1 if persistent else 0)
+    try:
+        r = lib.run(q, capi.GPUQO_DPSUB, bicc=True, ccc=True)
+    finally:
+        capi.set_int(lib.load(), "gpuqo_b200_persistent", 1)
+    assert r.error == 0, f"gpuqo_b200 error {r.error}"
+    return r
+
+
+TREES = ([query.star(n, 100 + n) for n in (2, 3, 8, 13, 18)] +
+         [query.snowflake(n, 200 + n, rich=(n % 2 == 0)) for n in (6, 11, 17, 22, 25)] +
+         [query.chain(n, 300 + n) for n in (4, 9, 20, 30)] +
+         [query.random_graph(n, 400 + n, extra_edge_p=0.0, rich=True) for n in (5, 12, 19, 24)] +
+         [query.random_graph(n, 500 + n, extra_edge_p=0.0, equal=True) for n in (7, 14, 21)])
+
+
+@pytest.mark.parametrize("q", TREES, ids=[q.name for q in TREES])
+def test_persistent_matches_level_launches(q):
+    a = _run(q, True)
+    b = _run(q, False)
+    assert same_tree(a.tree, b.tree)
+    assert a.stats["kernel_launches"] == 1
+    assert b.stats["kernel_launches"] > 1
+    assert a.stats["connected_sets"] == b.stats["connected_sets"]
+    assert a.stats["evaluated_pairs"] == b.stats["evaluated_pairs"]
+
+
+@pytest.mark.parametrize("q", [t for t in TREES if t.n <= 20], ids=[t.name for t in TREES if t.n <= 20])
+def test_persistent_vs_oracle(q):
+    want, _ = harness.run_port(q, 5)
+    assert same_tree(_run(q, True).tree, want)
+
+
+def test_persistent_sizes_in_a_row():
+    """Counters, the dedup bitmap and the barrier words are reset per run:
+    sizes up, down and repeated give the plans of fresh runs."""
+    qs = [query.snowflake(n, 700 + n) for n in (9, 20, 9, 15, 20, 4)]
+    want = {q.name: _run(q, False).tree for q in qs}
+    for q in qs:
+        assert same_tree(_run(q, True).tree, want[q.name])
+
+
+NOT_TREES = [query.cycle(12, 801), query.clique(7, 802),
+             # a class of three or more members joins every pair of them
+             query.multi_member_classes(6, 606), query.multi_member_classes(12, 612)]
+
+
+@pytest.mark.parametrize("q", NOT_TREES, ids=[q.name for q in NOT_TREES])
+def test_not_tree_keeps_level_launches(q):
+    r = _run(q, True)
+    assert r.stats["kernel_launches"] > 1
+    want, _ = harness.run_port(q, 5)
+    assert same_tree(r.tree, want)
+
+
+@pytest.mark.parametrize("warmup,iters", [(0, 1), (2, 3)])
+def test_time_resident_uses_persistent(warmup, iters):
+    """The device-resident timer takes the same single-launch path, with or
+    without warm-up replays, and returns the plan of gpuqo_run."""
+    q = query.snowflake(16, 901)
+    want = _run(q, False).tree
+    rc, ms, tree, st = lib.time_resident(q, capi.GPUQO_DPSUB, bicc=True, warmup=warmup, iters=iters)
+    assert rc == 0 and ms > 0.0
+    assert st["kernel_launches"] == 1
+    assert st["eval_kernel_launches"] == iters
+    assert same_tree(tree, want)
