@@ -2089,6 +2089,18 @@ struct BatchQ {
     unsigned long long seen_off;       // word offset into the dedup bitmap arena
 };
 
+// Sets of a level whose candidate count exceeds kOvfLimit (large biconnected
+// blocks: the full set of a cycle, dense sub-graphs), evaluated after the
+// level by every warp in chunks of kChunk candidates (kb_dp only).
+struct BatchOvf {
+    unsigned long long *item;          // [cap] query << 32 | set
+    uint32_t *P;                       // [cap] candidate count
+    uint32_t *off;                     // [cap] first chunk id (increases with the index)
+    unsigned long long *key;           // [cap] min (cost bits << 32 | candidate index) over chunks
+    unsigned long long *first;         // [cap] min (first valid candidate << 1 | its cost is NaN)
+    uint32_t cap;                      // 0: no overflow list (sets are evaluated by their group)
+};
+
 __global__ void kb_init(const BatchQ *__restrict__ qs, int nq, const uint32_t *__restrict__ blobs,
                         float4 *__restrict__ memo, uint32_t *__restrict__ memo_left,
                         unsigned long long *__restrict__ list1, LevelCounters *__restrict__ lvl1) {
@@ -2105,33 +2117,60 @@ __global__ void kb_init(const BatchQ *__restrict__ qs, int nq, const uint32_t *_
     if (threadIdx.x == 0) atomicAdd(&lvl1->n_sets, Q.n);
 }
 
-// connected k-sets of every query, by extension of its (k-1)-sets
-__global__ void __launch_bounds__(kBlock) kb_level_sets(const BatchQ *__restrict__ qs,
-                                                        const uint32_t *__restrict__ blobs,
-                                                        const unsigned long long *__restrict__ prev,
-                                                        const LevelCounters *__restrict__ prev_lc,
-                                                        uint32_t *__restrict__ seen,
-                                                        unsigned long long *__restrict__ out,
-                                                        LevelCounters *__restrict__ lc) {
-    __shared__ unsigned long long stage[kWarpsPerBlock][64];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long *st = stage[warp];
+// Warp-aggregated append of 64-bit items to a level list: lanes with ok set
+// stage their item in the warp's 64-slot area; every 32 staged items take one
+// atomicAdd on the level counter.  Call warp-uniformly; flush with
+// stage_flush64 at the end.
+__device__ __forceinline__ void stage_emit64(unsigned long long *st, uint32_t &cnt, bool ok,
+                                             unsigned long long item, unsigned long long *out, LevelCounters *lc) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t m = __ballot_sync(kFull, ok);
+    if (ok) st[cnt + __popc(m & ((1u << lane) - 1u))] = item;
+    cnt += __popc(m);
+    __syncwarp();
+    if (cnt >= 32) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&lc->n_sets, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        out[base + lane] = st[lane];
+        __syncwarp();
+        if (lane < cnt - 32) st[lane] = st[32 + lane];
+        cnt -= 32;
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ void stage_flush64(unsigned long long *st, uint32_t &cnt, unsigned long long *out,
+                                              LevelCounters *lc) {
+    const int lane = threadIdx.x & 31;
+    if (cnt > 0) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&lc->n_sets, cnt);
+        base = __shfl_sync(kFull, base, 0);
+        if (lane < cnt) out[base + lane] = st[lane];
+    }
+    cnt = 0;
+    __syncwarp();
+}
+
+// connected k-sets of every query, by extension of its (k-1)-sets (c_prev
+// items in prev); thread tid of nthreads
+__device__ __forceinline__ void batch_extend(const BatchQ *qs, const uint32_t *blobs, const unsigned long long *prev,
+                                             uint32_t c_prev, uint32_t *seen, unsigned long long *out,
+                                             LevelCounters *lc, unsigned long long *st, uint32_t tid,
+                                             uint32_t nthreads) {
     uint32_t cnt = 0;
-    const uint32_t c_prev = __ldcg(&prev_lc->n_sets);
-    const uint32_t nthreads = gridDim.x * blockDim.x;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t rounds = (c_prev + nthreads - 1u) / nthreads;
     for (uint32_t r = 0; r < rounds; r++) {
         const uint32_t idx = tid + r * nthreads;
         uint32_t S = 0u, N = 0u, q = 0u;
-        const uint32_t *adj = nullptr;
         unsigned long long seen_off = 0;
         if (idx < c_prev) {
             const unsigned long long it = __ldcg(prev + idx);
             q = (uint32_t)(it >> 32);
             S = (uint32_t)it;
             const BatchQ Q = qs[q];
-            adj = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->adj;
+            const uint32_t *adj = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->adj;
             seen_off = Q.seen_off;
             uint32_t x = S;
             while (x) {
@@ -2154,28 +2193,23 @@ __global__ void __launch_bounds__(kBlock) kb_level_sets(const BatchQ *__restrict
                 ok = !(atomicOr(&seen[seen_off + (T >> 5)], bm) & bm);
                 item = ((unsigned long long)q << 32) | T;
             }
-            uint32_t m = __ballot_sync(kFull, ok);
-            if (ok) st[cnt + __popc(m & ((1u << lane) - 1u))] = item;
-            cnt += __popc(m);
-            __syncwarp();
-            if (cnt >= 32) {
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&lc->n_sets, 32u);
-                base = __shfl_sync(kFull, base, 0);
-                out[base + lane] = st[lane];
-                __syncwarp();
-                if (lane < cnt - 32) st[lane] = st[32 + lane];
-                cnt -= 32;
-                __syncwarp();
-            }
+            stage_emit64(st, cnt, ok, item, out, lc);
         }
     }
-    if (cnt > 0) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&lc->n_sets, cnt);
-        base = __shfl_sync(kFull, base, 0);
-        if (lane < cnt) out[base + lane] = st[lane];
-    }
+    stage_flush64(st, cnt, out, lc);
+}
+
+__global__ void __launch_bounds__(kBlock) kb_level_sets(const BatchQ *__restrict__ qs,
+                                                        const uint32_t *__restrict__ blobs,
+                                                        const unsigned long long *__restrict__ prev,
+                                                        const LevelCounters *__restrict__ prev_lc,
+                                                        uint32_t *__restrict__ seen,
+                                                        unsigned long long *__restrict__ out,
+                                                        LevelCounters *__restrict__ lc) {
+    __shared__ unsigned long long stage[kWarpsPerBlock][64];
+    const int warp = threadIdx.x >> 5;
+    batch_extend(qs, blobs, prev, __ldcg(&prev_lc->n_sets), seen, out, lc, stage[warp],
+                 blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // candidate c of a tree-shaped query (see k_eval_tree): edge {a, b}, a < b
@@ -2225,7 +2259,8 @@ __device__ __forceinline__ void best_update(LaneBest &best, uint32_t p, uint32_t
 template <int G>
 __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *blobs, uint32_t first, uint32_t stride,
                                              const unsigned long long *items, uint32_t count, int k, float4 *memo_all,
-                                             uint32_t *memo_left_all, unsigned long long &pairs) {
+                                             uint32_t *memo_left_all, unsigned long long &pairs,
+                                             const BatchOvf &ovf, LevelCounters *lc) {
     const int lane = threadIdx.x & 31;
     const int grp = lane / G, gl = lane % G;
     const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
@@ -2253,6 +2288,23 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
             } else {
                 find_blocks(S, h.adj, B);
                 P = B.total;
+                if (ovf.cap != 0u && P > kOvfLimit) {
+                    // to the level's overflow list; one packed atomic assigns the
+                    // list index and the first chunk id in the same order
+                    if (gl == 0) {
+                        const uint32_t nch = (P + kChunk - 1u) / kChunk;
+                        const unsigned long long old = atomicAdd(&lc->ovf_packed, (1ull << 40) | nch);
+                        const uint32_t idx = (uint32_t)(old >> 40);
+                        if (idx < ovf.cap) {
+                            ovf.item[idx] = it;
+                            ovf.P[idx] = P;
+                            ovf.off[idx] = (uint32_t)(old & 0xFFFFFFFFFFull);
+                            ovf.key[idx] = ~0ull;
+                            ovf.first[idx] = ~0ull;
+                        }
+                    }
+                    P = 0u;   // no candidate here, no memo write
+                }
             }
         }
         __syncwarp();
@@ -2327,11 +2379,91 @@ __global__ void __launch_bounds__(kBlock) kb_eval(const BatchQ *__restrict__ qs,
     const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
     const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
     unsigned long long pairs = 0;
-    if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, items, count, k, memo, memo_left, pairs);
-    else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, items, count, k, memo, memo_left, pairs);
-    else batch_groups<32>(qs, blobs, gwarp, nwarps, items, count, k, memo, memo_left, pairs);
+    BatchOvf none;
+    none.cap = 0u;
+    LevelCounters *lcw = nullptr;
+    if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, items, count, k, memo, memo_left, pairs, none, lcw);
+    else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, items, count, k, memo, memo_left, pairs, none, lcw);
+    else batch_groups<32>(qs, blobs, gwarp, nwarps, items, count, k, memo, memo_left, pairs, none, lcw);
     pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
     if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
+}
+
+// Overflow chunks of level lc: every warp takes chunks of kChunk candidates
+// of a listed set (eval_range with the CCC queue) and folds its winner into
+// the set's keys with 64-bit atomicMin, as k_ovf_chunks does for one query.
+__device__ __forceinline__ void batch_ovf_chunks(const BatchQ *qs, const uint32_t *blobs, LevelCounters *lc,
+                                                 const float4 *memo_all, const BatchOvf &ovf, uint32_t *queue,
+                                                 unsigned long long &pairs) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long packed = __ldcg(&lc->ovf_packed);
+    const uint32_t n_ovf = (uint32_t)(packed >> 40);
+    const uint32_t n_chunks = (uint32_t)(packed & 0xFFFFFFFFFFull);
+    Blocks B;
+    B.nb = 0;
+    uint32_t cur_idx = kFull;
+    for (;;) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(&lc->chunk_next, 1u);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= n_chunks) break;
+        uint32_t lo_i = 0, hi_i = n_ovf - 1u;   // largest idx with off[idx] <= c
+        while (lo_i < hi_i) {
+            const uint32_t mid = (lo_i + hi_i + 1u) >> 1;
+            if (__ldcg(ovf.off + mid) <= c) lo_i = mid;
+            else hi_i = mid - 1u;
+        }
+        const uint32_t idx = lo_i;
+        const unsigned long long it = __ldcg(ovf.item + idx);
+        const uint32_t q = (uint32_t)(it >> 32), S = (uint32_t)it;
+        const uint32_t P = __ldcg(ovf.P + idx);
+        const BatchQ Q = qs[q];
+        const DevInfoView d = make_view(blobs + Q.blob_off);
+        if (idx != cur_idx) find_blocks(S, d.h->adj, B);
+        cur_idx = idx;
+        const uint32_t lo = (c - __ldcg(ovf.off + idx)) * kChunk;
+        const uint32_t hi = lo + kChunk < P ? lo + kChunk : P;
+        LaneBest best;
+        best.init();
+        eval_range<kModeMpdp>(d, d.h->adj, S, B, lo, hi, memo_all + Q.memo_off, queue, true, best);
+        unsigned long long mk, fk;
+        warp_winner(best, mk, fk);
+        if (lane == 0) {
+            if (mk != ~0ull) atomicMin(ovf.key + idx, mk);
+            atomicMin(ovf.first + idx, fk);
+        }
+        pairs += best.n_valid;
+    }
+}
+
+// Winner of every listed set: the candidate the keys name is evaluated again
+// and written to the memo (k_ovf_finalize for one query).
+__device__ __forceinline__ void batch_ovf_finalize(const BatchQ *qs, const uint32_t *blobs, LevelCounters *lc,
+                                                   float4 *memo_all, uint32_t *memo_left_all, const BatchOvf &ovf,
+                                                   uint32_t tid, uint32_t nthreads) {
+    const uint32_t n_ovf = (uint32_t)(__ldcg(&lc->ovf_packed) >> 40);
+    for (uint32_t idx = tid; idx < n_ovf; idx += nthreads) {
+        const unsigned long long it = __ldcg(ovf.item + idx);
+        const uint32_t q = (uint32_t)(it >> 32), S = (uint32_t)it;
+        const BatchQ Q = qs[q];
+        const DevInfoView d = make_view(blobs + Q.blob_off);
+        const uint32_t *adj = d.h->adj;
+        float4 *memo = memo_all + Q.memo_off;
+        const unsigned long long first = __ldcg(ovf.first + idx);
+        const uint32_t p = (first & 1ull) ? (uint32_t)(first >> 1) : (uint32_t)__ldcg(ovf.key + idx);
+        Blocks B;
+        find_blocks(S, adj, B);
+        int b = 0;
+        while (b + 1 < B.nb && B.prefix[b + 1] <= p) b++;
+        const uint32_t blk = B.mask[b];
+        const uint32_t lb = pdep32(p - B.prefix[b] + 1u, blk);
+        const uint32_t rb = blk ^ lb;
+        const uint32_t L = grow(lowest(lb), S & ~rb, adj);
+        const uint32_t R = grow(lowest(rb), S & ~lb, adj);
+        const RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+        const RelVal out = join_eval(d, L, l, R, r);
+        memo_write(memo, memo_left_all + Q.memo_off, S, out, L);
+    }
 }
 
 __global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const float4 *__restrict__ memo,
@@ -2386,6 +2518,101 @@ __global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const float4 *
     n_out[q] = n;
 }
 
+// kb_dp: a whole wave of queries in ONE cooperative, persistent launch.
+// Phase 0 writes every query's base relations and emits its level-2 sets
+// (one warp per query, one lane per relation: each edge once, from its lower
+// end).  Then, per level k, the grid evaluates level k of every query while
+// it enumerates level k+1, with a grid barrier between levels; the plans are
+// extracted (one thread per query) after the last level.  The grid barrier
+// is bounded (grid_barrier); on timeout the host reruns the wave with
+// per-level launches.
+__global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs, int nq, int maxn,
+                                                   const uint32_t *__restrict__ blobs, float4 *__restrict__ memo,
+                                                   uint32_t *__restrict__ memo_left, uint32_t *__restrict__ seen,
+                                                   unsigned long long *__restrict__ listA,
+                                                   unsigned long long *__restrict__ listB,
+                                                   LevelCounters *__restrict__ lvl, GlobalCounters *__restrict__ glob,
+                                                   TreeNode *__restrict__ tree, int *__restrict__ tree_n,
+                                                   unsigned *__restrict__ bar, uint32_t target_lanes,
+                                                   BatchOvf ovf) {
+    __shared__ unsigned long long stage[kWarpsPerBlock][64];
+    __shared__ uint32_t queues[kWarpsPerBlock][kQueueWords];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long *st = stage[warp];
+    const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
+    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nthreads = gridDim.x * blockDim.x;
+    unsigned long long pairs = 0;
+
+    // phase 0 (gpuqo_cpu_sequential.cu:80-92 for the base entries)
+    {
+        uint32_t cnt = 0;
+        for (uint32_t q = gwarp; q < (uint32_t)nq; q += nwarps) {
+            const BatchQ Q = qs[q];
+            const DevHeader *h = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off);
+            const int v = lane;
+            uint32_t nb = 0u;
+            if (v < (int)Q.n) {
+                memo[Q.memo_off + (1ull << v)] =
+                    make_float4(__ldg(h->rows + v), __ldg(h->startup + v), __ldg(h->total + v),
+                                __int_as_float(__ldg(h->width + v)));
+                memo_left[Q.memo_off + (1ull << v)] = 0u;
+                nb = __ldg(h->adj + v) & ~((2u << v) - 1u);
+            }
+            const int deg = __popc(nb);
+            const int maxdeg = (int)__reduce_max_sync(kFull, (uint32_t)deg);
+            for (int j = 0; j < maxdeg; j++) {
+                const bool ok = j < deg;
+                unsigned long long item = 0;
+                if (ok) {
+                    const int u = __ffs(nb) - 1;
+                    nb &= nb - 1u;
+                    item = ((unsigned long long)q << 32) | (1u << v) | (1u << u);
+                }
+                stage_emit64(st, cnt, ok, item, listA, lvl + 2);
+            }
+        }
+        stage_flush64(st, cnt, listA, lvl + 2);
+    }
+    if (!grid_barrier(bar)) return;
+
+    for (int k = 2; k <= maxn; k++) {
+        unsigned long long *cur = (k & 1) ? listB : listA;
+        unsigned long long *nxt = (k & 1) ? listA : listB;
+        const uint32_t count = __ldcg(&lvl[k].n_sets);
+        if (k < maxn) batch_extend(qs, blobs, cur, count, seen, nxt, lvl + k + 1, st, tid, nthreads);
+        int max_group = 1;
+        while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
+        int G = 2;
+        while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
+        G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
+        LevelCounters *lk = lvl + k;
+        if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs, ovf, lk);
+        else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
+        else batch_groups<32>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
+        if (!grid_barrier(bar)) return;
+        // overflow sets of level k: the counter is final after the barrier, so
+        // every block takes the same branch.  A list longer than its capacity
+        // is left to the host (the affected queries are rerun one by one).
+        const uint32_t n_ovf = (uint32_t)(__ldcg(&lk->ovf_packed) >> 40);
+        if (n_ovf != 0u && n_ovf <= ovf.cap) {
+            batch_ovf_chunks(qs, blobs, lk, memo, ovf, queues[warp], pairs);
+            if (!grid_barrier(bar)) return;
+            batch_ovf_finalize(qs, blobs, lk, memo, memo_left, ovf, tid, nthreads);
+            if (!grid_barrier(bar)) return;
+        }
+    }
+
+    for (uint32_t q = tid; q < (uint32_t)nq; q += nthreads) {
+        const BatchQ Q = qs[q];
+        const uint32_t full = (Q.n == 32) ? 0xFFFFFFFFu : ((1u << Q.n) - 1u);
+        extract_plan(memo + Q.memo_off, memo_left + Q.memo_off, full, tree + (size_t)q * 64, tree_n + q);
+    }
+    pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
+    if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
+}
+
 // Candidate bound of a query for the batch (the batch has no overflow path):
 // sum over blocks of 2^|b| - 2 with |b| <= the graph's largest block.
 static uint64_t mpdp_candidate_bound(int n, int max_block) {
@@ -2396,8 +2623,17 @@ static uint64_t mpdp_candidate_bound(int n, int max_block) {
 
 bool batch_eligible(const std::vector<uint32_t> &blob) {
     const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
-    return h->n >= 1 && h->n <= 30 && mpdp_candidate_bound(h->n, (int)h->max_block) <= kOvfLimit;
+    return h->n >= 1 && h->n <= 30;
 }
+
+// true when some set of the query may have more candidates than one group
+// evaluates: those sets need the overflow phase of kb_dp
+static bool batch_needs_ovf(const std::vector<uint32_t> &blob) {
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+    return mpdp_candidate_bound(h->n, (int)h->max_block) > kOvfLimit;
+}
+
+constexpr uint64_t kBatchOvfCap = 1ull << 22;   // overflow list entries per wave (32 B each)
 
 uint64_t batch_query_bytes(int n) {
     const uint64_t slots = 1ull << n;
@@ -2419,6 +2655,10 @@ struct BatchEngine {
     int *tree_n = nullptr;
     LevelCounters *lvl = nullptr;
     GlobalCounters *glob = nullptr;
+    unsigned *bar = nullptr, *h_bar = nullptr;   // grid barrier words of kb_dp (device, pinned copy)
+    int coop_grid = -1;                          // co-resident blocks of kb_dp (0: no cooperative launch)
+    BatchOvf ovf{};                              // overflow list of kb_dp
+    uint64_t cap_ovf = 0;
 
     int init(std::string &err) {
         if (stream) return 0;
@@ -2429,7 +2669,57 @@ struct BatchEngine {
         CK(cudaEventCreate(&ev1));
         CK(cudaMalloc(&lvl, 33 * sizeof(LevelCounters)));
         CK(cudaMalloc(&glob, sizeof(GlobalCounters)));
+        CK(cudaMalloc(&bar, 4 * sizeof(unsigned)));
+        CK(cudaMallocHost(&h_bar, 4 * sizeof(unsigned)));
+        int dev_coop = 0, occ = 0;
+        cudaDeviceGetAttribute(&dev_coop, cudaDevAttrCooperativeLaunch, device);
+        if (dev_coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb_dp, kBlock, 0) == cudaSuccess)
+            coop_grid = occ * sm_count;
+        else
+            coop_grid = 0;
+        cudaGetLastError();
         return 0;
+    }
+
+    // per-level launches of one wave (the queries, blobs and arena are staged)
+    uint32_t enqueue_levels(int nq, int maxn, uint64_t seen_words) {
+        cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
+        cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
+        cudaMemsetAsync(seen, 0, seen_words * 4, stream);
+        kb_init<<<nq, 32, 0, stream>>>(qs, nq, blobs, memo, memo_left, listA, lvl + 1);
+        uint32_t kernels = 1;
+        const uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
+        for (int k = 2; k <= maxn; k++) {
+            unsigned long long *prev = (k & 1) ? listB : listA;
+            unsigned long long *cur = (k & 1) ? listA : listB;
+            kb_level_sets<<<sm_count * 8, kBlock, 0, stream>>>(qs, blobs, prev, lvl + (k - 1), seen, cur, lvl + k);
+            int max_group = 1;
+            while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
+            kb_eval<<<sm_count * 4, kBlock, 0, stream>>>(qs, blobs, cur, lvl + k, k, memo, memo_left, glob,
+                                                         target_lanes, max_group);
+            kernels += 2;
+        }
+        kb_extract<<<(nq + 127) / 128, 128, 0, stream>>>(qs, nq, memo, memo_left, tree, tree_n);
+        return kernels + 1;
+    }
+
+    // the wave as one cooperative launch of kb_dp; false when it could not start
+    bool enqueue_persistent(int nq, int maxn, uint64_t seen_words) {
+        if (coop_grid <= 0 || gpuqo_b200_persistent == 0) return false;
+        cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
+        cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
+        cudaMemsetAsync(seen, 0, seen_words * 4, stream);
+        cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), stream);
+        uint32_t target_lanes = (uint32_t)coop_grid * kBlock;
+        void *args[] = {&qs, &nq, &maxn, &blobs, &memo, &memo_left, &seen, &listA, &listB,
+                        &lvl, &glob, &tree, &tree_n, &bar, &target_lanes, &ovf};
+        if (cudaLaunchCooperativeKernel((const void *)kb_dp, dim3(coop_grid), dim3(kBlock), args, 0, stream) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            coop_grid = 0;
+            return false;
+        }
+        return true;
     }
 
     template <class T> int grow(T *&p, uint64_t &cap, uint64_t need, std::string &err) {
@@ -2442,12 +2732,52 @@ struct BatchEngine {
         return 0;
     }
 
-    // One wave: all queries' memos fit.  blobs: per query planner-info blob.
+    bool persistent_ready() const { return coop_grid > 0 && gpuqo_b200_persistent != 0; }
+
+    // One wave: all queries' memos fit.  wb: per query planner-info blob.
+    // Queries that this wave could not finish (sets beyond the group limit
+    // without the overflow phase, or an overfull overflow list) are listed in
+    // redo (wave-local indices) for the single-query engine.
     int run_wave(const std::vector<const std::vector<uint32_t> *> &wb, std::vector<std::vector<TreeNode>> &out,
-                 EngineStats &st, double &ms, std::string &err) {
+                 std::vector<int> &redo, EngineStats &st, double &ms, std::string &err) {
+        redo.clear();
+        std::vector<int> need_ovf;
+        for (int q = 0; q < (int)wb.size(); q++)
+            if (batch_needs_ovf(*wb[q])) need_ovf.push_back(q);
+        if (!need_ovf.empty() && !persistent_ready()) {
+            // per-level launches cannot split a set: those queries run alone
+            std::vector<const std::vector<uint32_t> *> rest;
+            std::vector<int> idx;
+            size_t j = 0;
+            for (int q = 0; q < (int)wb.size(); q++) {
+                if (j < need_ovf.size() && need_ovf[j] == q) {
+                    j++;
+                    continue;
+                }
+                rest.push_back(wb[q]);
+                idx.push_back(q);
+            }
+            out.assign(wb.size(), {});
+            redo = need_ovf;
+            ms = 0.0;
+            if (rest.empty()) return 0;
+            std::vector<std::vector<TreeNode>> rout;
+            bool ovf_full = false;
+            if (int rc = stage_and_run(rest, rout, st, ms, ovf_full, err)) return rc;
+            for (size_t i = 0; i < idx.size(); i++) out[idx[i]] = std::move(rout[i]);
+            return 0;
+        }
+        bool ovf_full = false;
+        if (int rc = stage_and_run(wb, out, st, ms, ovf_full, err)) return rc;
+        if (ovf_full) redo = need_ovf;
+        return 0;
+    }
+
+    int stage_and_run(const std::vector<const std::vector<uint32_t> *> &wb, std::vector<std::vector<TreeNode>> &out,
+                      EngineStats &st, double &ms, bool &ovf_full, std::string &err) {
         const int nq = (int)wb.size();
         std::vector<BatchQ> hq(nq);
-        uint64_t slots = 0, words = 0, seen_words = 0, items = 0, base = 0;
+        uint64_t slots = 0, words = 0, seen_words = 0, items = 0, base = 0, ovf_need = 0;
         int maxn = 0;
         for (int q = 0; q < nq; q++) {
             const DevHeader *h = reinterpret_cast<const DevHeader *>(wb[q]->data());
@@ -2463,8 +2793,10 @@ struct BatchEngine {
             items += max_level_sets(n);
             base += (uint64_t)n;
             maxn = std::max(maxn, n);
+            if (batch_needs_ovf(*wb[q])) ovf_need += max_level_sets(n);
         }
         items = std::max(items, base);
+        ovf_need = std::min(ovf_need, kBatchOvfCap);
         uint64_t c1 = cap_slots, c2 = cap_slots, c3 = cap_words, c4 = cap_seen, c5 = cap_items, c6 = cap_items;
         if (int rc = grow(memo, c1, slots, err)) return rc;
         if (int rc = grow(memo_left, c2, slots, err)) return rc;
@@ -2476,6 +2808,16 @@ struct BatchEngine {
         if (int rc = grow(listA, c5, items, err)) return rc;
         if (int rc = grow(listB, c6, items, err)) return rc;
         cap_items = std::min(c5, c6);
+        if (ovf_need > cap_ovf) {
+            uint64_t a1 = cap_ovf, a2 = cap_ovf, a3 = cap_ovf, a4 = cap_ovf, a5 = cap_ovf;
+            if (int rc = grow(ovf.item, a1, ovf_need, err)) return rc;
+            if (int rc = grow(ovf.P, a2, ovf_need, err)) return rc;
+            if (int rc = grow(ovf.off, a3, ovf_need, err)) return rc;
+            if (int rc = grow(ovf.key, a4, ovf_need, err)) return rc;
+            if (int rc = grow(ovf.first, a5, ovf_need, err)) return rc;
+            cap_ovf = ovf_need;
+        }
+        ovf.cap = (uint32_t)ovf_need;
         if (nq > cap_q) {
             cudaFree(qs);
             cudaFree(tree);
@@ -2493,25 +2835,24 @@ struct BatchEngine {
         for (int q = 0; q < nq; q++) std::copy(wb[q]->begin(), wb[q]->end(), hblob.begin() + hq[q].blob_off);
         CK(cudaMemcpyAsync(blobs, hblob.data(), words * 4, cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(qs, hq.data(), nq * sizeof(BatchQ), cudaMemcpyHostToDevice, stream));
-        CK(cudaEventRecord(ev0, stream));
-        CK(cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream));
-        CK(cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream));
-        CK(cudaMemsetAsync(seen, 0, seen_words * 4, stream));
-        kb_init<<<nq, 32, 0, stream>>>(qs, nq, blobs, memo, memo_left, listA, lvl + 1);
         uint32_t kernels = 1;
-        const uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
-        for (int k = 2; k <= maxn; k++) {
-            unsigned long long *prev = (k & 1) ? listB : listA;
-            unsigned long long *cur = (k & 1) ? listA : listB;
-            kb_level_sets<<<sm_count * 8, kBlock, 0, stream>>>(qs, blobs, prev, lvl + (k - 1), seen, cur, lvl + k);
-            int max_group = 1;
-            while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
-            kb_eval<<<sm_count * 4, kBlock, 0, stream>>>(qs, blobs, cur, lvl + k, k, memo, memo_left, glob,
-                                                         target_lanes, max_group);
-            kernels += 2;
+        CK(cudaEventRecord(ev0, stream));
+        bool persistent = enqueue_persistent(nq, maxn, seen_words);
+        CK(cudaGetLastError());
+        if (persistent) {
+            CK(cudaMemcpyAsync(h_bar, bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            CK(cudaGetLastError());
+            if (h_bar[2] != 0u) {   // barrier timed out: rerun with per-level launches
+                persistent = false;
+                CK(cudaEventRecord(ev0, stream));
+            }
         }
-        kb_extract<<<(nq + 127) / 128, 128, 0, stream>>>(qs, nq, memo, memo_left, tree, tree_n);
-        kernels++;
+        if (!persistent) {
+            ovf.cap = 0u;
+            kernels = enqueue_levels(nq, maxn, seen_words);
+        }
+        CK(cudaGetLastError());
         CK(cudaEventRecord(ev1, stream));
         std::vector<TreeNode> htree((size_t)nq * 64);
         std::vector<int> hn(nq);
@@ -2526,13 +2867,19 @@ struct BatchEngine {
         float fms = 0.f;
         CK(cudaEventElapsedTime(&fms, ev0, ev1));
         ms = fms;
+        // kb_dp skipped the overflow phase of a level whose list outgrew its
+        // capacity; the per-level launches (ovf.cap 0) evaluate every set in
+        // its group and need no redo
+        ovf_full = false;
+        for (int k = 2; k <= maxn; k++)
+            if (persistent && (uint32_t)(hl[k].ovf_packed >> 40) > ovf.cap) ovf_full = true;
         out.resize(nq);
         for (int q = 0; q < nq; q++) {
-            if (hn[q] != 2 * (int)hq[q].n - 1) {
+            if (hn[q] != 2 * (int)hq[q].n - 1 && !(ovf_full && batch_needs_ovf(*wb[q]))) {
                 err = "batched plan extraction produced " + std::to_string(hn[q]) + " nodes";
                 return GPUQO_B200_ERR_CUDA;
             }
-            out[q].assign(htree.begin() + (size_t)q * 64, htree.begin() + (size_t)q * 64 + hn[q]);
+            out[q].assign(htree.begin() + (size_t)q * 64, htree.begin() + (size_t)q * 64 + std::max(hn[q], 0));
         }
         for (int k = 2; k <= maxn; k++) st.connected_sets += hl[k].n_sets;
         st.evaluated_pairs += hg.evaluated_pairs;
@@ -2574,10 +2921,22 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
             i++;
         }
         std::vector<std::vector<TreeNode>> wout;
+        std::vector<int> redo;
         double ms = 0;
-        if (int rc = be->run_wave(wave, wout, st, ms, err)) return rc;
+        if (int rc = be->run_wave(wave, wout, redo, st, ms, err)) return rc;
         wave_ms.push_back(ms);
         for (size_t j = 0; j < idx.size(); j++) out[idx[j]] = std::move(wout[j]);
+        if (!redo.empty()) {
+            auto &eng = g_engines[dev];
+            if (!eng) eng.reset(new Engine());
+            for (int r : redo) {
+                const std::vector<uint32_t> &b = *wave[r];
+                const int n = reinterpret_cast<const DevHeader *>(b.data())->n;
+                std::vector<TreeNode> nodes;
+                if (int rc = eng->run(b, n, kModeMpdp, true, false, nodes, st, err)) return rc;
+                out[idx[r]] = std::move(nodes);
+            }
+        }
     }
     return 0;
 }

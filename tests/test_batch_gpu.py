@@ -52,3 +52,52 @@ def test_batch_plain_dpsub_and_general_graphs():
         for q, t in zip(qs, trees):
             want, _ = harness.run_port(q, 5 if bicc else 3)
             assert same_tree(t, want), (q.name, bicc)
+
+
+def test_batch_persistent_matches_level_launches():
+    """One cooperative launch per wave (kb_dp) and the per-level launches
+    return the same plans, counters and pair counts."""
+    # n <= 11 keeps every cycle inside the batched kernel's candidate bound
+    qs = query.batch_mix(240, seed=5, nmin=2, nmax=11)
+    l = lib.load()
+    out = {}
+    try:
+        for p in (1, 0):
+            capi.set_int(l, "gpuqo_b200_persistent", p)
+            trees, rc = lib.run_batch(qs, capi.GPUQO_DPSUB, bicc=True)
+            assert rc == 0
+            out[p] = (trees, lib.get_stats())
+    finally:
+        capi.set_int(l, "gpuqo_b200_persistent", 1)
+    (tp, sp), (tl, sl) = out[1], out[0]
+    for q, a, b in zip(qs, tp, tl):
+        assert same_tree(a, b), q.name
+    assert sp["n_subproblems"] == len(qs)
+    assert sp["kernel_launches"] == 1          # one wave, one launch
+    assert sl["kernel_launches"] > 2 * 9
+    assert sp["connected_sets"] == sl["connected_sets"]
+    assert sp["evaluated_pairs"] == sl["evaluated_pairs"]
+
+
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_batch_large_blocks(persistent):
+    """Sets with more candidates than one group evaluates (the full set of a
+    cycle of 12+ relations, dense random graphs) take kb_dp's overflow phase;
+    without the persistent kernel those queries run on the single engine.
+    Either way every plan equals gpuqo_run's and the oracle's."""
+    qs = ([query.cycle(n, 60 + n) for n in (12, 13, 15, 18, 21)] +
+          [query.random_graph(n, 70 + n, extra_edge_p=0.45, rich=True) for n in (12, 14, 15)] +
+          [query.star(n, 80 + n) for n in (9, 14)] + [query.snowflake(16, 91)])
+    l = lib.load()
+    try:
+        capi.set_int(l, "gpuqo_b200_persistent", persistent)
+        trees, rc = lib.run_batch(qs, capi.GPUQO_DPSUB, bicc=True)
+    finally:
+        capi.set_int(l, "gpuqo_b200_persistent", 1)
+    assert rc == 0
+    for q, t in zip(qs, trees):
+        single = lib.run(q, capi.GPUQO_DPSUB, bicc=True)
+        assert same_tree(t, single.tree), q.name
+        if q.n <= 15:
+            want, _ = harness.run_port(q, 5)
+            assert same_tree(t, want), q.name
