@@ -19,7 +19,15 @@ Printed (rank 0, one JSON line):
            written) over its event-timed launch duration, against the
            measured HBM copy bandwidth;
   cpu_baseline - the reference's parallel_cpu_dpsub_bicc (its own code,
-           compiled from its sources into oracle/_ref) on the host cores.
+           compiled from its sources into oracle/_ref) on the host cores;
+  batched - 4096 queries of the mixed workload (40% star, 40% snowflake, 10%
+           chain, 10% cycle; relation counts uniform in [8,28], and [8,16])
+           through gpuqo_b200_run_batch against gpuqo_run one query per call,
+           queries per second and a bit-for-bit plan comparison;
+  served - IDP2 (k=25) snowflake queries of 30..1000 relations arriving as a
+           Poisson stream at 1x and 4x the plain capacity into the
+           continuous-batching service: queries/s, p50/p99 latency, against
+           one-at-a-time gpuqo_run (FIFO under the same arrivals).
 
 --impl reference times that reference CPU engine alone (rank 0 only).
 """
@@ -149,6 +157,134 @@ def cpu_reference_sample(queries, steps=None, budget_s=20.0):
     return statistics.mean(times), cores, len(times)
 
 
+def _prebuilt(qs):
+    import ctypes as C
+    from gpuqo_b200 import capi
+    bs = [capi.PlannerInfoBuilder(q) for q in qs]
+    arr = (C.POINTER(capi.GpuqoPlannerInfoC) * len(qs))(*[b.pointer() for b in bs])
+    return bs, arr
+
+
+def batched_section(seed=7):
+    """Batched MPDP (gpuqo_b200_run_batch) against the plain one-query-per-call
+    gpuqo_run on the same prebuilt planner infos; wall clock around the C
+    calls (host conversion, H2D, DP, D2H, plan output all included), plans
+    compared bit for bit."""
+    import ctypes as C
+    from gpuqo_b200 import capi, lib, query
+    L = lib.load()
+    capi.set_bool(L, "gpuqo_dpsub_bicc_enable", True)
+    capi.set_int(L, "gpuqo_idp_n_iters", 0)
+
+    def run_batch(arr, m):
+        out = (C.POINTER(capi.QueryTreeC) * m)()
+        t = time.perf_counter()
+        rc = L.gpuqo_b200_run_batch(capi.GPUQO_DPSUB, arr, m, out)
+        dt = time.perf_counter() - t
+        st = lib.get_stats()
+        trees = [capi.tree_to_py(out[i]) for i in range(m)]
+        for i in range(m):
+            L.gpuqo_b200_free_query_tree(C.cast(out[i], C.c_void_p))
+        if rc:
+            raise RuntimeError(f"gpuqo_b200_run_batch failed: {rc}")
+        return dt, st, trees
+
+    res = {}
+    for tag, nmin, nmax in (("n8_28", 8, 28), ("n8_16", 8, 16)):
+        qs = query.batch_mix(4096, seed=seed, nmin=nmin, nmax=nmax)
+        bs, arr = _prebuilt(qs)
+        _, warr = _prebuilt(query.batch_mix(64, seed=seed + 1, nmin=nmin, nmax=min(nmax, 20)))
+        run_batch(warr, 64)                                  # warm-up (engines, arenas)
+        dtb, st, trees = run_batch(arr, len(qs))
+        t = time.perf_counter()
+        same = True
+        for b, tb in zip(bs, trees):
+            r = L.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())
+            same = same and capi.same_plan(capi.tree_to_py(r), tb)
+            L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
+        dtp = time.perf_counter() - t
+        res[tag] = {"queries": len(qs), "batched_qps": len(qs) / dtb, "plain_qps": len(qs) / dtp,
+                    "speedup": dtp / dtb, "batched_device_ms": st["device_ms"],
+                    "batched_launches": st["kernel_launches"], "identical_plans": same}
+    return {"workload": "4096 MPDP queries, shapes 40% star / 40% snowflake / 10% chain / 10% cycle, "
+                        "relation counts uniform in the range (n8_28: the full [8,28] mix; n8_16: small queries)",
+            "arms": "batched = gpuqo_b200_run_batch of all queries (waves of one cooperative launch each); "
+                    "plain = gpuqo_run per query; both from host planner infos to palloc'd plans",
+            "by_range": res}
+
+
+def served_section(n_req=48, seed=5):
+    """Served IDP2 (k=25) over MPDP: Poisson arrivals of snowflake queries with
+    relation counts log-uniform in [30,1000] into the continuous-batching
+    service, against one-at-a-time plain gpuqo_run (FIFO under the same
+    arrivals, latencies from its measured service times)."""
+    import ctypes as C
+    import math
+    import threading
+    import numpy as np
+    from gpuqo_b200 import capi, lib, query
+    rng = np.random.default_rng(seed)
+    ns = [int(round(math.exp(rng.uniform(math.log(30), math.log(1000))))) for _ in range(n_req)]
+    qs = [query.snowflake(n, 9000 + i) for i, n in enumerate(ns)]
+    L = lib.load()
+    capi.set_bool(L, "gpuqo_dpsub_bicc_enable", True)
+    capi.set_int(L, "gpuqo_idp_n_iters", 25)
+    capi.set_int(L, "gpuqo_idp_type", capi.GPUQO_IDP2)
+    builders = [capi.PlannerInfoBuilder(q) for q in qs]
+    r = L.gpuqo_run(capi.GPUQO_DPSUB, builders[0].pointer())   # warm-up
+    L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
+    svc, plain = [], []
+    for b in builders:
+        t = time.perf_counter()
+        r = L.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())
+        svc.append(time.perf_counter() - t)
+        plain.append(capi.tree_to_py(r))
+        L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
+    plain_qps = n_req / sum(svc)
+    out = {"workload": f"{n_req} snowflake queries, relation counts log-uniform in [30,1000], IDP2 with "
+                       f"gpuqo_idp_n_iters=25 over MPDP, Poisson arrivals",
+           "plain_qps": plain_qps, "plain_mean_service_ms": 1e3 * sum(svc) / n_req, "rates": []}
+    for mult in (1.0, 4.0):
+        rate = plain_qps * mult
+        arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        fin, lats = 0.0, []
+        for a, sv in zip(arr, svc):
+            fin = max(a, fin) + sv
+            lats.append(fin - a)
+        srv = lib.Server(max_inflight=32, wave_memory_mb=32768)
+        res = [None] * n_req
+
+        def waiter(j, tk):
+            res[j] = srv.wait(tk)
+        ths = []
+        t0 = time.perf_counter()
+        for j in range(n_req):
+            now = time.perf_counter() - t0
+            if arr[j] > now:
+                time.sleep(arr[j] - now)
+            tk = srv.submit_built(builders[j], capi.GPUQO_DPSUB)
+            th = threading.Thread(target=waiter, args=(j, tk))
+            th.start()
+            ths.append(th)
+        for th in ths:
+            th.join()
+        makespan = time.perf_counter() - t0
+        st = srv.stats()
+        srv.stop()
+        lat = [x[2] for x in res]
+        out["rates"].append({
+            "arrival_qps": rate, "served_qps": n_req / makespan, "served_p50_ms": float(np.percentile(lat, 50)),
+            "served_p99_ms": float(np.percentile(lat, 99)),
+            "plain_fifo_p50_ms": 1e3 * float(np.percentile(lats, 50)),
+            "plain_fifo_p99_ms": 1e3 * float(np.percentile(lats, 99)),
+            "plain_fifo_qps": n_req / max(fin, arr[-1]),
+            "identical_plans": all(x[0] == 0 and capi.same_plan(x[1], p) for x, p in zip(res, plain)),
+            "waves": st["waves"], "batched_subproblems": st["batched_subproblems"],
+            "single_subproblems": st["single_subproblems"]})
+    capi.set_int(L, "gpuqo_idp_n_iters", 0)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -156,6 +292,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (4096-query) section")
+    ap.add_argument("--no-served", action="store_true", help="skip the served IDP2 section")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
 
@@ -290,6 +428,10 @@ def main():
             "gpu_launches": kernels,
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_batched:
+            line["batched"] = batched_section()
+        if world == 1 and not args.no_served:
+            line["served"] = served_section()
         if world == 1 and not args.no_cpu_baseline:
             cv, cores, ns = cpu_reference_sample(qs)
             line["cpu_baseline"] = {"value": cv, "unit": "ms/query", "cores": cores, "kind": "reference",

@@ -2635,6 +2635,45 @@ static bool batch_needs_ovf(const std::vector<uint32_t> &blob) {
 
 constexpr uint64_t kBatchOvfCap = 1ull << 22;   // overflow list entries per wave (32 B each)
 
+// Connected sets of a tree-shaped query graph (its connected subtrees): with
+// f(v) = prod over children c of (1 + f(c)) for the tree rooted at relation
+// 0, the count is the sum of f(v).  Exact, O(n).
+static double tree_connected_sets(const DevHeader *h) {
+    const int n = h->n;
+    int order[32], parent[32], m = 0;
+    uint32_t seen = 1u;
+    order[m++] = 0;
+    parent[0] = -1;
+    for (int i = 0; i < m; i++) {
+        uint32_t nb = h->adj[order[i]] & ~seen;
+        seen |= nb;
+        while (nb) {
+            const int c = __builtin_ctz(nb);
+            nb &= nb - 1u;
+            parent[c] = order[i];
+            order[m++] = c;
+        }
+    }
+    double f[32], total = 0.0;
+    for (int i = 0; i < n; i++) f[i] = 1.0;
+    for (int i = m - 1; i >= 0; i--) {
+        const int v = order[i];
+        total += f[v];
+        if (parent[v] >= 0) f[parent[v]] *= 1.0 + f[v];
+    }
+    return total;
+}
+
+// A tree-shaped query with this many connected sets fills the GPU on its own:
+// the single-query kernel (k_dp_tree, planner info in shared memory) then
+// evaluates more pairs per second than a batch wave, so the batch hands it over.
+constexpr double kBatchSingleSets = double(1u << 20);
+
+static bool batch_prefers_single(const std::vector<uint32_t> &blob) {
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+    return h->tree_mode != 0u && gpuqo_b200_persistent != 0 && tree_connected_sets(h) > kBatchSingleSets;
+}
+
 uint64_t batch_query_bytes(int n) {
     const uint64_t slots = 1ull << n;
     return slots * (sizeof(float4) + 4) + slots / 8 + 2 * max_level_sets(n) * 8 + 64 * sizeof(TreeNode) + 4096;
@@ -2905,20 +2944,33 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
     if (!be) be.reset(new BatchEngine());
     if (int rc = be->init(err)) return rc;
     out.assign(blobs.size(), {});
+    auto &eng = g_engines[dev];
+    // large tree-shaped queries: one persistent single-query launch each
+    std::vector<size_t> rest;
+    for (size_t i = 0; i < blobs.size(); i++) {
+        if (!batch_prefers_single(*blobs[i])) {
+            rest.push_back(i);
+            continue;
+        }
+        if (!eng) eng.reset(new Engine());
+        const int n = reinterpret_cast<const DevHeader *>(blobs[i]->data())->n;
+        if (int rc = eng->run(*blobs[i], n, kModeMpdp, true, false, out[i], st, err)) return rc;
+    }
     // waves: consecutive queries while the wave's memory stays within budget
-    size_t i = 0;
-    while (i < blobs.size()) {
+    size_t r = 0;
+    while (r < rest.size()) {
         std::vector<const std::vector<uint32_t> *> wave;
         std::vector<size_t> idx;
         uint64_t bytes = 0;
-        while (i < blobs.size()) {
+        while (r < rest.size()) {
+            const size_t i = rest[r];
             const int n = reinterpret_cast<const DevHeader *>(blobs[i]->data())->n;
             const uint64_t b = batch_query_bytes(n);
             if (!wave.empty() && bytes + b > wave_bytes) break;
             wave.push_back(blobs[i]);
             idx.push_back(i);
             bytes += b;
-            i++;
+            r++;
         }
         std::vector<std::vector<TreeNode>> wout;
         std::vector<int> redo;
@@ -2927,7 +2979,6 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
         wave_ms.push_back(ms);
         for (size_t j = 0; j < idx.size(); j++) out[idx[j]] = std::move(wout[j]);
         if (!redo.empty()) {
-            auto &eng = g_engines[dev];
             if (!eng) eng.reset(new Engine());
             for (int r : redo) {
                 const std::vector<uint32_t> &b = *wave[r];

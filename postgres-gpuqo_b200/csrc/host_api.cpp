@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dp_engine.h"
@@ -643,30 +644,36 @@ extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *
         std::vector<uint32_t> blob;
     };
     std::vector<Prep> prep(n_queries);
-    std::vector<int> batched, single;
-    for (int i = 0; i < n_queries; i++) {
+    std::vector<char> to_batch(n_queries, 0);
+    // reads the caller's structures and allocates with malloc only (no
+    // palloc), so the queries are prepared on several host threads
+    auto prepare = [&](int i) {
         GpuqoPlannerInfoC *c = infos[i];
         const bool idp = c && gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < c->n_rels;
-        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp || mode != kModeMpdp) {
-            single.push_back(i);
-            continue;
-        }
+        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp || mode != kModeMpdp) return;
         HostInfo info;
         std::string err;
-        if (!convert_info(c, info, err)) {
-            single.push_back(i);
-            continue;
-        }
+        if (!convert_info(c, info, err)) return;
         prep[i].order = bfs_order(info);
-        if ((int)prep[i].order.size() != info.n) {
-            single.push_back(i);
-            continue;
-        }
+        if ((int)prep[i].order.size() != info.n) return;
         HostInfo remapped = relabel(info, prep[i].order);
         prep[i].blob = build_blob(remapped);
-        if (batch_eligible(prep[i].blob)) batched.push_back(i);
-        else single.push_back(i);
+        to_batch[i] = batch_eligible(prep[i].blob) ? 1 : 0;
+    };
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int n_threads = n_queries >= 64 ? std::min({hw, 16, n_queries / 32}) : 1;
+    if (n_threads > 1) {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < n_threads; t++)
+            pool.emplace_back([&, t] {
+                for (int i = t; i < n_queries; i += n_threads) prepare(i);
+            });
+        for (auto &th : pool) th.join();
+    } else {
+        for (int i = 0; i < n_queries; i++) prepare(i);
     }
+    std::vector<int> batched, single;
+    for (int i = 0; i < n_queries; i++) (to_batch[i] ? batched : single).push_back(i);
     int status = GPUQO_B200_OK;
     if (!batched.empty()) {
         // larger queries first: a wave then runs only the levels it needs

@@ -230,3 +230,20 @@ def set_bool(lib, name: str, value: bool):
 
 def get_int(lib, name: str) -> int:
     return C.c_int.in_dll(lib, name).value
+
+
+def same_plan(a, b) -> bool:
+    """Two plans from tree_to_py are identical: relids, float32 bits of rows,
+    startup and total cost (any NaN equals any NaN: payloads differ between
+    x86 and GPU arithmetic, and Postgres never inspects them), width, shape."""
+    import math
+    import struct
+    if a is None or b is None:
+        return a is None and b is None
+
+    def same_f(x, y):
+        if math.isnan(x) or math.isnan(y):
+            return math.isnan(x) and math.isnan(y)
+        return struct.pack("<f", x) == struct.pack("<f", y)
+    return (a[0] == b[0] and a[4] == b[4] and all(same_f(a[i], b[i]) for i in (1, 2, 3))
+            and same_plan(a[5], b[5]) and same_plan(a[6], b[6]))
