@@ -839,10 +839,18 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar) {
     return s_ok != 0u;
 }
 
-// One enumeration phase (level k) with the block's shared adjacency, binomial
-// table and per-warp staging area.
+// One enumeration phase (level k) of a tree-shaped query graph with the
+// block's shared adjacency, binomial table and per-warp staging area.
+//
+// Extension without a dedup structure: adding a neighbour v to a connected
+// set S of a tree makes v a leaf of T = S + v (v has exactly one neighbour p
+// in S), and every connected T of two or more relations has one largest
+// leaf.  T is emitted only from the S whose added v is that largest leaf: the
+// other leaves of T are the leaves of S except p (p gains the neighbour v),
+// or S itself when S is a single relation.  So each connected k-set appears
+// exactly once, with no atomics and no bitmap to clear.
 __device__ __forceinline__ void level_sets_phase(const uint32_t *adj, const uint32_t *binom, uint32_t *st, int n,
-                                                 int k, const uint32_t *prev_sets, uint32_t c_prev, uint32_t *seen,
+                                                 int k, const uint32_t *prev_sets, uint32_t c_prev,
                                                  uint32_t *out_sets, LevelCounters *lc) {
     const int lane = threadIdx.x & 31;
     const uint64_t total = binom[n * 33 + k];
@@ -870,17 +878,20 @@ __device__ __forceinline__ void level_sets_phase(const uint32_t *adj, const uint
         const uint32_t rounds = (c_prev + nthreads - 1u) / nthreads;
         for (uint32_t r = 0; r < rounds; r++) {
             const uint32_t idx = tid + r * nthreads;
-            uint32_t S = 0u, N = 0u;
+            uint32_t S = 0u, N = 0u, leaves = 0u;
             if (idx < c_prev) {
                 S = (k == 2) ? (1u << idx) : __ldcg(prev_sets + idx);
                 uint32_t x = S;
                 while (x) {
                     int v = __ffs(x) - 1;
                     x &= x - 1u;
-                    N |= adj[v];
+                    const uint32_t a = adj[v];
+                    N |= a;
+                    if (__popc(a & S) == 1) leaves |= 1u << v;
                 }
                 N &= ~S;
             }
+            const bool single = (S & (S - 1u)) == 0u;
             const int deg = __popc(N);
             const int maxdeg = (int)__reduce_max_sync(kFull, (uint32_t)deg);
             for (int j = 0; j < maxdeg; j++) {
@@ -890,8 +901,9 @@ __device__ __forceinline__ void level_sets_phase(const uint32_t *adj, const uint
                     const uint32_t bitv = N & (0u - N);
                     N ^= bitv;
                     T = S | bitv;
-                    const uint32_t bm = 1u << (T & 31u);
-                    ok = !(atomicOr(&seen[T >> 5], bm) & bm);
+                    const uint32_t p = adj[__ffs(bitv) - 1] & S;            // v's only neighbour in S
+                    const uint32_t others = single ? S : (leaves & ~p);    // the other leaves of T
+                    ok = others < bitv;                                     // v is T's largest leaf
                 }
                 emit(ok, T);
             }
@@ -965,8 +977,7 @@ __device__ __forceinline__ void extract_plan(const float4 *memo, const uint32_t 
 __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restrict__ blob, uint32_t blob_words,
                                                        const uint32_t *__restrict__ binom_g, float4 *__restrict__ memo,
                                                        uint32_t *__restrict__ memo_left, uint32_t *__restrict__ setsA,
-                                                       uint32_t *__restrict__ setsB, uint32_t *__restrict__ seen,
-                                                       LevelCounters *__restrict__ lvl,
+                                                       uint32_t *__restrict__ setsB, LevelCounters *__restrict__ lvl,
                                                        GlobalCounters *__restrict__ glob, TreeNode *__restrict__ tree,
                                                        int *__restrict__ tree_n, unsigned *__restrict__ bar,
                                                        uint32_t target_lanes) {
@@ -993,13 +1004,13 @@ __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restric
         memo[1u << i] = make_float4(d.h->rows[i], d.h->startup[i], d.h->total[i], __int_as_float(d.h->width[i]));
         memo_left[1u << i] = 0u;
     }
-    if (n >= 2) level_sets_phase(adj, binom, st, n, 2, nullptr, (uint32_t)n, seen, setsA, lvl + 2);
+    if (n >= 2) level_sets_phase(adj, binom, st, n, 2, nullptr, (uint32_t)n, setsA, lvl + 2);
     if (!grid_barrier(bar)) return;
     for (int k = 2; k <= n; k++) {
         uint32_t *cur = (k & 1) ? setsB : setsA;
         uint32_t *nxt = (k & 1) ? setsA : setsB;
         const uint32_t count = __ldcg(&lvl[k].n_sets);
-        if (k < n) level_sets_phase(adj, binom, st, n, k + 1, cur, count, seen, nxt, lvl + k + 1);
+        if (k < n) level_sets_phase(adj, binom, st, n, k + 1, cur, count, nxt, lvl + k + 1);
         int max_group = 1;
         while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
         int G = 2;
@@ -1443,12 +1454,11 @@ public:
         if (grid <= 0) return 0;
         CK(cudaMemsetAsync(a.lvl, 0, 33 * sizeof(LevelCounters), stream));
         CK(cudaMemsetAsync(a.glob, 0, sizeof(GlobalCounters), stream));
-        CK(cudaMemsetAsync(a.seen, 0, std::max<uint64_t>((1ull << n) / 8, 4), stream));
         CK(cudaMemsetAsync(a.bar, 0, 4 * sizeof(unsigned), stream));
         CK(cudaMemsetAsync(a.tree_n, 0, sizeof(int), stream));
         uint32_t bwords = words;
         uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
-        void *args[] = {&a.blob, &bwords, &a.binom, &a.memo, &a.memo_left, &a.sets, &a.sets2, &a.seen,
+        void *args[] = {&a.blob, &bwords, &a.binom, &a.memo, &a.memo_left, &a.sets, &a.sets2,
                         &a.lvl, &a.glob, &a.tree, &a.tree_n, &a.bar, &target_lanes};
         cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_dp_tree, dim3(grid), dim3(kBlock), args,
                                                     smem, stream);

@@ -50,7 +50,7 @@ def test_persistent_vs_oracle(q):
 
 
 def test_persistent_sizes_in_a_row():
-    """Counters, the dedup bitmap and the barrier words are reset per run:
+    """Counters and the barrier words are reset per run:
     sizes up, down and repeated give the plans of fresh runs."""
     qs = [query.snowflake(n, 700 + n) for n in (9, 20, 9, 15, 20, 4)]
     want = {q.name: _run(q, False).tree for q in qs}
