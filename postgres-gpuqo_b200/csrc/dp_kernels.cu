@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_eval_tree(const uint32_t *__restr
 // launches.
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;   // 4 s of global time
-constexpr unsigned kBarrierSpinLimit = 1u << 26;                  // hard cap on polls as well
+constexpr unsigned kBarrierSpinLimit = 1u << 26;                  // hard cap on polls as well (~30 s)
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -804,35 +804,34 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// bar[0] = arrivals, bar[1] = generation, bar[2] = error flag.  Returns the
-// same verdict to every thread of the block (thread 0 decides); blocks may
-// disagree only after a timeout, and then every later barrier sees the error
-// flag and returns false at once, so all blocks leave.
-__device__ __forceinline__ bool grid_barrier(unsigned *bar) {
+// bar[0] = arrivals, bar[2] = error flag (both zero at launch).  The arrival
+// counter only grows: a block's e-th barrier of the launch completes when it
+// reaches e * gridDim.x, so nobody resets it and the last block to arrive has
+// nothing more to do.  Thread 0 arrives with a gpu-scope release reduction
+// (ordering every write its block made before the __syncthreads) and polls
+// with gpu-scope acquire loads.  The verdict is the same for every thread of
+// the block (thread 0 decides); blocks may disagree only after a timeout, and
+// then every later barrier sees the error flag and returns false at once, so
+// all blocks leave.  epoch: the caller's count of barriers passed (thread 0).
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &epoch) {
     __shared__ unsigned s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *vgen = bar + 1;
+        epoch++;
+        const unsigned target = epoch * gridDim.x;
         volatile unsigned *verr = bar + 2;
-        const unsigned gen = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            unsigned spins = 0;
-            while (*vgen == gen && *verr == 0u) {
-                if (++spins > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
-                    atomicExch(bar + 2, 1u);
-                    break;
-                }
-                __nanosleep(128);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+        const unsigned long long t0 = global_ns();
+        unsigned spins = 0;
+        for (;;) {
+            unsigned c;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(bar) : "memory");
+            if (c >= target || *verr != 0u) break;
+            if (++spins > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
+                atomicExch(bar + 2, 1u);
+                break;
             }
         }
-        __threadfence();
         s_ok = (*verr == 0u) ? 1u : 0u;
     }
     __syncthreads();
@@ -997,6 +996,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restric
     const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
     const bool masked = d.h->ec_masked != 0u;
     unsigned long long pairs = 0;
+    unsigned epoch = 0;   // grid barriers passed (thread 0)
 
     // phase 0: base relations (gpuqo_cpu_sequential.cu:80-92) and level-2 sets
     if (blockIdx.x == 0 && threadIdx.x < n) {
@@ -1005,7 +1005,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restric
         memo_left[1u << i] = 0u;
     }
     if (n >= 2) level_sets_phase(adj, binom, st, n, 2, nullptr, (uint32_t)n, setsA, lvl + 2);
-    if (!grid_barrier(bar)) return;
+    if (!grid_barrier(bar, epoch)) return;
     for (int k = 2; k <= n; k++) {
         uint32_t *cur = (k & 1) ? setsB : setsA;
         uint32_t *nxt = (k & 1) ? setsA : setsB;
@@ -1026,7 +1026,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restric
             if (masked) tree_groups<32, true>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
             else tree_groups<32, false>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
         }
-        if (!grid_barrier(bar)) return;
+        if (!grid_barrier(bar, epoch)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t full = (n == 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
@@ -2554,6 +2554,7 @@ __global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nthreads = gridDim.x * blockDim.x;
     unsigned long long pairs = 0;
+    unsigned epoch = 0;   // grid barriers passed (thread 0)
 
     // phase 0 (gpuqo_cpu_sequential.cu:80-92 for the base entries)
     {
@@ -2585,7 +2586,7 @@ __global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs
         }
         stage_flush64(st, cnt, listA, lvl + 2);
     }
-    if (!grid_barrier(bar)) return;
+    if (!grid_barrier(bar, epoch)) return;
 
     for (int k = 2; k <= maxn; k++) {
         unsigned long long *cur = (k & 1) ? listB : listA;
@@ -2601,16 +2602,16 @@ __global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs
         if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs, ovf, lk);
         else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
         else batch_groups<32>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
-        if (!grid_barrier(bar)) return;
+        if (!grid_barrier(bar, epoch)) return;
         // overflow sets of level k: the counter is final after the barrier, so
         // every block takes the same branch.  A list longer than its capacity
         // is left to the host (the affected queries are rerun one by one).
         const uint32_t n_ovf = (uint32_t)(__ldcg(&lk->ovf_packed) >> 40);
         if (n_ovf != 0u && n_ovf <= ovf.cap) {
             batch_ovf_chunks(qs, blobs, lk, memo, ovf, queues[warp], pairs);
-            if (!grid_barrier(bar)) return;
+            if (!grid_barrier(bar, epoch)) return;
             batch_ovf_finalize(qs, blobs, lk, memo, memo_left, ovf, tid, nthreads);
-            if (!grid_barrier(bar)) return;
+            if (!grid_barrier(bar, epoch)) return;
         }
     }
 
