@@ -393,15 +393,18 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = e2e_ms / (args.steps * world)
-    # bytes crossing the bus per step: the planner-info blob (header 208 words,
-    # 2 words per class, selectivities, 8 words per class member; staged in
-    # 512-word buckets) in; plan nodes + tree size + counters out
+    # bytes crossing the bus per step: the planner-info blob in (header 274
+    # words, 2 words per class, its selectivities, 9 words per class member,
+    # the 3 n^2 tree tables of a tree-shaped graph; staged in 512-word
+    # buckets); plan nodes (64 x 28 B), tree size, pair counter, 33 level
+    # counters (24 B) and the barrier words (16 B) out
     q0 = qs[0]
     n_ec = len(q0.eq_classes)
     n_sels = sum(len(e.sels) for e in q0.eq_classes)
     n_fks = sum(len(e.members) for e in q0.eq_classes)
-    h2d = 4 * ((208 + 2 * n_ec + n_sels + 8 * n_fks + 511) // 512 * 512)
-    d2h = 64 * 28 + 4 + 8 + 33 * 16
+    words = 274 + 2 * n_ec + n_sels + 9 * n_fks + 3 * N_RELS * N_RELS
+    h2d = 4 * ((words + 511) // 512 * 512)
+    d2h = 64 * 28 + 4 + 8 + 33 * 24 + 16
 
     if rank == 0:
         peak, peak_kind = measured_peaks()

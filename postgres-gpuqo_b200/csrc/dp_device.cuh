@@ -86,15 +86,26 @@ __device__ __forceinline__ uint32_t ord_float(float f) {
 struct RelVal {
     float rows, startup, total;
     int width;
+    uint32_t hz;   // packed hash table size of this set as an inner side, 0 if not stored
 };
 
-__device__ __forceinline__ RelVal load_rel(const float4 *memo, uint32_t s) {
+// Memo width word.  With DevHeader::hz_packed the low 21 bits hold the width,
+// bit 21 marks a stored hash table size, bits 22-26 log2(numbuckets) and
+// bits 27-31 log2(numbatches) of ExecChooseHashTableSize for the set as an
+// inner relation (a function of its rows and width only), computed once when
+// the entry is written instead of once per pair that reads it.
+constexpr uint32_t kWidthBits = 21;
+constexpr uint32_t kWidthMask = (1u << kWidthBits) - 1u;
+
+__device__ __forceinline__ RelVal load_rel(const float4 *memo, uint32_t s, uint32_t packed) {
     float4 v = __ldcg(memo + s);
     RelVal r;
     r.rows = v.x;
     r.startup = v.y;
     r.total = v.z;
-    r.width = __float_as_int(v.w);
+    const uint32_t w = __float_as_uint(v.w);
+    r.width = packed ? (int)(w & kWidthMask) : (int)w;
+    r.hz = packed ? (w >> kWidthBits) : 0u;
     return r;
 }
 
@@ -161,21 +172,12 @@ __device__ __forceinline__ Htsz exec_choose_hash_table_size(float ntuples, int t
     return res;
 }
 
-// :705-787 __estimate_hash_bucketsize
-__device__ __forceinline__ float bucketsize_one(const DevVar &v, float rel_rows, float rel_tuples, int nbuckets) {
-    float estfract, ndistinct, mcvfreq, avgfreq;
-    ndistinct = v.stadistinct;
-    if (ndistinct < 0.0f) ndistinct = -ndistinct * rel_tuples;
-    if (ndistinct <= 0.0f) return 0.1f;
-    avgfreq = (1.0f - v.stanullfrac) / ndistinct;
-    if (rel_tuples > 0.0f) {
-        ndistinct *= rel_rows / rel_tuples;
-        ndistinct = clamp_row_est(ndistinct);
-    }
-    if (ndistinct > (float)nbuckets) estfract = 1.0f / (float)nbuckets;
-    else estfract = 1.0f / ndistinct;
-    mcvfreq = v.mcvfreq;
-    if (avgfreq > 0.0f && mcvfreq > avgfreq) estfract *= mcvfreq / avgfreq;
+// :705-787 __estimate_hash_bucketsize; the relation-only terms come from
+// devvar_bucket_terms, only the bucket count depends on the pair
+__device__ __forceinline__ float bucketsize_one(const DevVar &v, int nbuckets) {
+    if (v.flags & kVarNoDistinct) return 0.1f;
+    float estfract = (v.bs_nd > (float)nbuckets) ? 1.0f / (float)nbuckets : v.bs_inv_nd;
+    if (v.flags & kVarMcvRatio) estfract *= v.bs_mcv_ratio;
     if (estfract < 1.0e-6f) estfract = 1.0e-6f;
     else if (estfract > 1.0f) estfract = 1.0f;
     return estfract;
@@ -304,6 +306,19 @@ __device__ __forceinline__ float ec_selectivity(const DevInfoView &d, int i, uin
     return d.sels[off_sels + idx];
 }
 
+// width word of a memo entry for a set of this rows and width (see kWidthBits)
+__device__ __forceinline__ uint32_t memo_width_word(const DevHeader &h, float rows, int width) {
+    if (!h.hz_packed) return (uint32_t)width;
+    const Htsz z = exec_choose_hash_table_size(rows, width, h.work_mem);
+    const uint32_t lb = 31u - (uint32_t)__clz(z.numbuckets), lt = 31u - (uint32_t)__clz(z.numbatches);
+    return (uint32_t)width | (1u << kWidthBits) | (lb << (kWidthBits + 1)) | (lt << (kWidthBits + 6));
+}
+
+// memo entry of base relation i (gpuqo_cpu_sequential.cu:80-92)
+__device__ __forceinline__ float4 base_entry(const DevHeader &h, int i) {
+    return make_float4(h.rows[i], h.startup[i], h.total[i], __uint_as_float(memo_width_word(h, h.rows[i], h.width[i])));
+}
+
 // ---------------------------------------------------------------------------
 // One join evaluation: estimate_join_rows + calc_join_cost + width
 // (gpuqo_cpu_common.cuh:169-186 make_join_relation; gpuqo_cost.cuh:81-157).
@@ -317,9 +332,15 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
                                               const RelVal &r, uint32_t ec_mask) {
     const DevHeader &h = *d.h;
     const bool inner_single = (R & (R - 1u)) == 0u;
-    // the hash table size depends on the inner side only; needed by the
-    // bucket-size estimate inside the class loop
-    Htsz hz = exec_choose_hash_table_size(r.rows, r.width, h.work_mem);
+    // the hash table size depends on the inner side only (stored with its memo
+    // entry when hz_packed); needed by the bucket-size estimate in the class loop
+    Htsz hz;
+    if (r.hz) {
+        hz.numbuckets = 1 << ((r.hz >> 1) & 31u);
+        hz.numbatches = 1 << (r.hz >> 6);
+    } else {
+        hz = exec_choose_hash_table_size(r.rows, r.width, h.work_mem);
+    }
     int nbuckets = f2i_x86((float)hz.numbuckets * (float)hz.numbatches);
 
     float sel = 1.0f;
@@ -354,8 +375,7 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
                 if (v.flags & 1u) any_index = true;
             }
             first = false;
-            int rel = lowest_idx(in_id);
-            float this_bs = bucketsize_one(v, h.rows[rel], h.tuples[rel], nbuckets);
+            float this_bs = bucketsize_one(v, nbuckets);
             if (bucketsize > this_bs) bucketsize = this_bs;
             if (mcvfreq > v.mcvfreq) mcvfreq = v.mcvfreq;
             m &= ~in_id;
@@ -371,7 +391,8 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
     extra.inner_unique = inner_unique;
     extra.indexed_join_quals = false;
     extra.joinrows = out.rows;
-    extra.outer_match_frac = out.rows / (l.rows * r.rows);
+    // read by the cost functions only for a unique inner side
+    extra.outer_match_frac = inner_unique ? out.rows / (l.rows * r.rows) : 0.0f;
     extra.match_count = r.rows;
 
     float min_s, min_t, s, t;

@@ -292,8 +292,8 @@ struct LaneBest {
 
 __device__ __forceinline__ void evaluate_pair(const DevInfoView &d, const float4 *memo, uint32_t p, uint32_t L,
                                               uint32_t R, LaneBest &b) {
-    RelVal l = load_rel(memo, L);
-    RelVal r = load_rel(memo, R);
+    RelVal l = load_rel(memo, L, d.h->hz_packed);
+    RelVal r = load_rel(memo, R, d.h->hz_packed);
     RelVal out = join_eval(d, L, l, R, r);
     bool nan = isnan(out.total);
     b.n_valid++;
@@ -422,9 +422,9 @@ __device__ __forceinline__ WarpWinner warp_winner(const LaneBest &b, unsigned lo
     return w;
 }
 
-__device__ __forceinline__ void memo_write(float4 *memo, uint32_t *memo_left, uint32_t S, const RelVal &v,
-                                           uint32_t left) {
-    memo[S] = make_float4(v.rows, v.startup, v.total, __int_as_float(v.width));
+__device__ __forceinline__ void memo_write(const DevHeader &h, float4 *memo, uint32_t *memo_left, uint32_t S,
+                                           const RelVal &v, uint32_t left) {
+    memo[S] = make_float4(v.rows, v.startup, v.total, __uint_as_float(memo_width_word(h, v.rows, v.width)));
     memo_left[S] = left;
 }
 
@@ -486,8 +486,8 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
         unsigned long long mk, fk;
         WarpWinner w = warp_winner(best, mk, fk);
         if (w.is_writer) {
-            if (w.use_nan) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
-            else memo_write(memo, memo_left, S, best.val, best.left);
+            if (w.use_nan) memo_write(*d.h, memo, memo_left, S, best.nan_val, best.nan_left);
+            else memo_write(*d.h, memo, memo_left, S, best.val, best.left);
         }
         pairs += best.n_valid;
     }
@@ -566,9 +566,9 @@ __device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t
         const unsigned long long gkey = ((unsigned long long)kh << 32) | kl;
         if (has && !ovf) {
             if (nm) {
-                if (nan_first) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
+                if (nan_first) memo_write(*d.h, memo, memo_left, S, best.nan_val, best.nan_left);
             } else if (best.key == gkey && best.key != ~0ull) {
-                memo_write(memo, memo_left, S, best.val, best.left);
+                memo_write(*d.h, memo, memo_left, S, best.val, best.left);
             }
         }
         pairs += best.n_valid;
@@ -697,7 +697,7 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
                     const int ch0 = ((tab[2 * nn + b] >> a) & 1u) ? b : a;   // child end w.r.t. relation 0
                     ecm = h.edge_ec[ch0];
                 }
-                RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+                RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
                 RelVal out = join_eval_t<MASKED>(d, L, l, R, r, ecm);
                 const bool nan = isnan(out.total);
                 best.n_valid++;
@@ -736,9 +736,9 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         const unsigned long long gkey = ((unsigned long long)kh << 32) | kl;
         if (has) {
             if (nm) {
-                if (nan_first) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
+                if (nan_first) memo_write(*d.h, memo, memo_left, S, best.nan_val, best.nan_left);
             } else if (best.key == gkey && best.key != ~0ull) {
-                memo_write(memo, memo_left, S, best.val, best.left);
+                memo_write(*d.h, memo, memo_left, S, best.val, best.left);
             }
         }
         pairs += best.n_valid;
@@ -930,7 +930,7 @@ __device__ __forceinline__ void level_sets_phase(const uint32_t *adj, const uint
 }
 
 __device__ __forceinline__ void extract_plan(const float4 *memo, const uint32_t *memo_left, uint32_t full,
-                                             TreeNode *out, int *n_out) {
+                                             uint32_t wmask, TreeNode *out, int *n_out) {
     int n = 0;
     uint32_t stack_set[64];
     int stack_parent[64], stack_side[64];
@@ -951,7 +951,7 @@ __device__ __forceinline__ void extract_plan(const float4 *memo, const uint32_t 
         t.rows = v.x;
         t.startup = v.y;
         t.total = v.z;
-        t.width = __float_as_int(v.w);
+        t.width = (int)(__float_as_uint(v.w) & wmask);
         const int me = n++;
         out[me] = t;
         if (parent >= 0) {
@@ -1001,7 +1001,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restric
     // phase 0: base relations (gpuqo_cpu_sequential.cu:80-92) and level-2 sets
     if (blockIdx.x == 0 && threadIdx.x < n) {
         const int i = threadIdx.x;
-        memo[1u << i] = make_float4(d.h->rows[i], d.h->startup[i], d.h->total[i], __int_as_float(d.h->width[i]));
+        memo[1u << i] = base_entry(*d.h, i);
         memo_left[1u << i] = 0u;
     }
     if (n >= 2) level_sets_phase(adj, binom, st, n, 2, nullptr, (uint32_t)n, setsA, lvl + 2);
@@ -1030,7 +1030,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restric
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t full = (n == 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
-        extract_plan(memo, memo_left, full, tree, tree_n);
+        extract_plan(memo, memo_left, full, d.h->hz_packed ? kWidthMask : 0xFFFFFFFFu, tree, tree_n);
     }
     pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
     if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
@@ -1128,9 +1128,9 @@ __global__ void __launch_bounds__(kBlock) k_ovf_finalize(const uint32_t *__restr
             L = grow(lowest(lb), S & ~rb, adj);
             R = grow(lowest(rb), S & ~lb, adj);
         }
-        RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+        RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
         RelVal out = join_eval(d, L, l, R, r);
-        memo_write(memo, memo_left, S, out, L);
+        memo_write(*d.h, memo, memo_left, S, out, L);
     }
 }
 
@@ -1143,14 +1143,15 @@ __global__ void k_init_base(const uint32_t *__restrict__ blob, float4 *__restric
     int i = threadIdx.x;
     if (i < h->n) {
         // gpuqo_cpu_sequential.cu:80-92: base relation memo entries
-        memo[1u << i] = make_float4(h->rows[i], h->startup[i], h->total[i], __int_as_float(h->width[i]));
+        memo[1u << i] = base_entry(*h, i);
         memo_left[1u << i] = 0u;
     }
 }
 
 __global__ void k_extract(const float4 *__restrict__ memo, const uint32_t *__restrict__ memo_left, uint32_t full,
-                          TreeNode *__restrict__ out, int *__restrict__ n_out) {
+                          const uint32_t *__restrict__ blob, TreeNode *__restrict__ out, int *__restrict__ n_out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t wmask = reinterpret_cast<const DevHeader *>(blob)->hz_packed ? kWidthMask : 0xFFFFFFFFu;
     // iterative preorder walk; node i's children are appended after it
     int n = 0;
     uint32_t stack_set[64];
@@ -1173,7 +1174,7 @@ __global__ void k_extract(const float4 *__restrict__ memo, const uint32_t *__res
         t.rows = v.x;
         t.startup = v.y;
         t.total = v.z;
-        t.width = __float_as_int(v.w);
+        t.width = (int)(__float_as_uint(v.w) & wmask);
         int me = n++;
         out[me] = t;
         if (parent >= 0) {
@@ -1418,7 +1419,7 @@ public:
             }
         }
         uint32_t full = (n == 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
-        k_extract<<<1, 32, 0, stream>>>(a.memo, a.memo_left, full, a.tree, a.tree_n);
+        k_extract<<<1, 32, 0, stream>>>(a.memo, a.memo_left, full, a.blob, a.tree, a.tree_n);
         n_kernels++;
         return 0;
     }
@@ -1892,6 +1893,13 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
     h->enable_hashjoin = enable_hashjoin ? 1 : 0;
     h->composite_mask = 0;
     h->blob_words = words;
+    long long width_sum = 0;
+    bool width_ok = true;
+    for (int t = 0; t < n; t++) {
+        width_sum += c->base_rels[t].width;
+        width_ok = width_ok && c->base_rels[t].width >= 0;
+    }
+    h->hz_packed = (width_ok && width_sum < (1ll << kWidthBits)) ? 1u : 0u;
     for (int t = 0; t < n; t++) {
         const BaseRelationC &b = c->base_rels[from_of_to[t]];
         h->adj[t] = (uint32_t)(remap(edge[from_of_to[t]]) & ~(1ull << t));
@@ -1928,13 +1936,13 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
             fks[off_fks + lt] = (uint32_t)remap(ec->fk ? na_bms(ec->fk[lf]) : 0ull);
             const VarInfo &vi = ec->vars[lf];
             DevVar &dv = vars[off_fks + lt];
-            dv.stadistinct = vi.stats.stadistinct;
-            dv.stanullfrac = vi.stats.stanullfrac;
-            dv.mcvfreq = vi.stats.mcvfreq;
+            const int rel_t = __builtin_ffsll((long long)id_lt) - 1;   // compact index of this member
             dv.idx_rows = vi.index.rows;
             dv.idx_startup = vi.index.cost.startup;
             dv.idx_total = vi.index.cost.total;
             dv.flags = (vi.index.available ? 1u : 0u) | (vi.index.unique ? 2u : 0u);
+            devvar_bucket_terms(dv, vi.stats.stadistinct, vi.stats.stanullfrac, vi.stats.mcvfreq, h->rows[rel_t],
+                                h->tuples[rel_t]);
         }
         off_sels += s * (s - 1) / 2;
         off_fks += s;
@@ -2048,7 +2056,7 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
             }
         }
     }
-    k_extract<<<1, 32, 0, stream>>>(memo, memo_left, (1u << n) - 1u, tree, tree_n);
+    k_extract<<<1, 32, 0, stream>>>(memo, memo_left, (1u << n) - 1u, d_blob, tree, tree_n);
     TreeNode host_nodes[64];
     int host_n = 0;
     cudaMemcpyAsync(host_nodes, tree, 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream);
@@ -2120,7 +2128,7 @@ __global__ void kb_init(const BatchQ *__restrict__ qs, int nq, const uint32_t *_
     const DevHeader *h = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off);
     for (int i = threadIdx.x; i < (int)Q.n; i += blockDim.x) {
         memo[Q.memo_off + (1ull << i)] =
-            make_float4(h->rows[i], h->startup[i], h->total[i], __int_as_float(h->width[i]));
+            base_entry(*h, i);
         memo_left[Q.memo_off + (1ull << i)] = 0u;
         list1[Q.first_base + i] = ((unsigned long long)q << 32) | (1u << i);
     }
@@ -2343,7 +2351,7 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
                 }
             }
             if (valid) {
-                RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+                RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
                 RelVal out = masked ? join_eval_t<true>(d, L, l, R, r, ecm) : join_eval_t<false>(d, L, l, R, r, 0u);
                 best_update(best, p, L, out);
             }
@@ -2365,9 +2373,9 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
         const unsigned long long gkey = ((unsigned long long)kh << 32) | kl;
         if (has) {
             if (nm) {
-                if (nan_first) memo_write(memo, memo_left, S, best.nan_val, best.nan_left);
+                if (nan_first) memo_write(*d.h, memo, memo_left, S, best.nan_val, best.nan_left);
             } else if (best.key == gkey && best.key != ~0ull) {
-                memo_write(memo, memo_left, S, best.val, best.left);
+                memo_write(*d.h, memo, memo_left, S, best.val, best.left);
             }
         }
         pairs += best.n_valid;
@@ -2470,18 +2478,20 @@ __device__ __forceinline__ void batch_ovf_finalize(const BatchQ *qs, const uint3
         const uint32_t rb = blk ^ lb;
         const uint32_t L = grow(lowest(lb), S & ~rb, adj);
         const uint32_t R = grow(lowest(rb), S & ~lb, adj);
-        const RelVal l = load_rel(memo, L), r = load_rel(memo, R);
+        const RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
         const RelVal out = join_eval(d, L, l, R, r);
-        memo_write(memo, memo_left_all + Q.memo_off, S, out, L);
+        memo_write(*d.h, memo, memo_left_all + Q.memo_off, S, out, L);
     }
 }
 
-__global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const float4 *__restrict__ memo,
-                           const uint32_t *__restrict__ memo_left, TreeNode *__restrict__ out,
-                           int *__restrict__ n_out) {
+__global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const uint32_t *__restrict__ blobs,
+                           const float4 *__restrict__ memo, const uint32_t *__restrict__ memo_left,
+                           TreeNode *__restrict__ out, int *__restrict__ n_out) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
     const BatchQ Q = qs[q];
+    const uint32_t wmask =
+        reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->hz_packed ? kWidthMask : 0xFFFFFFFFu;
     const uint32_t full = (Q.n == 32) ? 0xFFFFFFFFu : ((1u << Q.n) - 1u);
     TreeNode *o = out + (size_t)q * 64;
     const float4 *m = memo + Q.memo_off;
@@ -2506,7 +2516,7 @@ __global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const float4 *
         t.rows = v.x;
         t.startup = v.y;
         t.total = v.z;
-        t.width = __float_as_int(v.w);
+        t.width = (int)(__float_as_uint(v.w) & wmask);
         int me = n++;
         o[me] = t;
         if (parent >= 0) {
@@ -2565,9 +2575,7 @@ __global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs
             const int v = lane;
             uint32_t nb = 0u;
             if (v < (int)Q.n) {
-                memo[Q.memo_off + (1ull << v)] =
-                    make_float4(__ldg(h->rows + v), __ldg(h->startup + v), __ldg(h->total + v),
-                                __int_as_float(__ldg(h->width + v)));
+                memo[Q.memo_off + (1ull << v)] = base_entry(*h, v);
                 memo_left[Q.memo_off + (1ull << v)] = 0u;
                 nb = __ldg(h->adj + v) & ~((2u << v) - 1u);
             }
@@ -2618,7 +2626,9 @@ __global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs
     for (uint32_t q = tid; q < (uint32_t)nq; q += nthreads) {
         const BatchQ Q = qs[q];
         const uint32_t full = (Q.n == 32) ? 0xFFFFFFFFu : ((1u << Q.n) - 1u);
-        extract_plan(memo + Q.memo_off, memo_left + Q.memo_off, full, tree + (size_t)q * 64, tree_n + q);
+        const uint32_t wmask =
+            reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->hz_packed ? kWidthMask : 0xFFFFFFFFu;
+        extract_plan(memo + Q.memo_off, memo_left + Q.memo_off, full, wmask, tree + (size_t)q * 64, tree_n + q);
     }
     pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
     if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
@@ -2749,7 +2759,7 @@ struct BatchEngine {
                                                          target_lanes, max_group);
             kernels += 2;
         }
-        kb_extract<<<(nq + 127) / 128, 128, 0, stream>>>(qs, nq, memo, memo_left, tree, tree_n);
+        kb_extract<<<(nq + 127) / 128, 128, 0, stream>>>(qs, nq, blobs, memo, memo_left, tree, tree_n);
         return kernels + 1;
     }
 

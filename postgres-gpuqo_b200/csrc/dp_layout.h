@@ -2,6 +2,7 @@
 // code that builds it and the kernels that read it.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #ifndef __CUDACC__
@@ -21,12 +22,53 @@ constexpr int kWarp = 32;
 //   uint32 ec_relids[n_ec]; uint32 ec_off[n_ec] (off_sels << 16 | off_fks);
 //   float sels[n_sels]; uint32 fks[n_fks]; DevVar vars[n_fks]
 // ---------------------------------------------------------------------------
+// A class member's variable.  The bucket-size terms depend only on the
+// variable's statistics and its base relation's rows and tuples, so they are
+// computed once on the host (devvar_bucket_terms) instead of per join pair.
 struct DevVar {
-    float stadistinct, stanullfrac, mcvfreq;
+    float bs_nd;                          // ndistinct scaled to the relation's rows and clamped
+    float bs_inv_nd;                      // 1 / bs_nd
+    float bs_mcv_ratio;                   // mcvfreq / avgfreq (applies when flags bit3)
+    float mcvfreq;
     float idx_rows, idx_startup, idx_total;
-    uint32_t flags;                       // bit0 index.available, bit1 index.unique
+    uint32_t flags;                       // bit0 index.available, bit1 index.unique,
+                                          // bit2 no ndistinct (estimate 0.1), bit3 mcv ratio applies
 };
-static_assert(sizeof(DevVar) == 28, "DevVar layout");
+static_assert(sizeof(DevVar) == 32, "DevVar layout");
+
+constexpr uint32_t kVarNoDistinct = 4u;
+constexpr uint32_t kVarMcvRatio = 8u;
+
+// The relation-only part of __estimate_hash_bucketsize
+// (gpuqo_cost_postgres.cuh:705-787): every operation below is the
+// reference's, in its order, in IEEE single precision (built without
+// contraction on the host), so the terms equal those the device would
+// compute per pair.
+GQB_HD inline void devvar_bucket_terms(DevVar &v, float stadistinct, float stanullfrac, float mcvfreq,
+                                       float rel_rows, float rel_tuples) {
+    float ndistinct = stadistinct;
+    v.flags &= ~(kVarNoDistinct | kVarMcvRatio);
+    v.mcvfreq = mcvfreq;
+    v.bs_nd = 0.0f;
+    v.bs_inv_nd = 0.0f;
+    v.bs_mcv_ratio = 0.0f;
+    if (ndistinct < 0.0f) ndistinct = -ndistinct * rel_tuples;
+    if (ndistinct <= 0.0f) {
+        v.flags |= kVarNoDistinct;
+        return;
+    }
+    const float avgfreq = (1.0f - stanullfrac) / ndistinct;
+    if (rel_tuples > 0.0f) {
+        ndistinct *= rel_rows / rel_tuples;
+        ndistinct = ndistinct <= 1.0f ? 1.0f : rintf(ndistinct);   // clamp_row_est
+    }
+    v.bs_nd = ndistinct;
+    v.bs_inv_nd = 1.0f / ndistinct;
+    if (avgfreq > 0.0f && mcvfreq > avgfreq) {
+        v.flags |= kVarMcvRatio;
+        v.bs_mcv_ratio = mcvfreq / avgfreq;
+    }
+}
 
 struct DevHeader {
     int n, n_ec, n_sels, n_fks;
@@ -38,7 +80,9 @@ struct DevHeader {
     uint32_t tree_mode;                   // query graph is a tree (tree tables present)
     uint32_t ec_masked;                   // tree_mode and every class is a 2-member class on an edge
     uint32_t tree_tab;                    // word offset of the tree tables (see below), 0 if none
-    uint32_t pad;
+    // memo widths carry the inner hash table size (see memo_width_word): set
+    // when every width is >= 0 and all of them sum to less than 2^21
+    uint32_t hz_packed;
     uint32_t adj[kMaxRels];
     float rows[kMaxRels];
     float tuples[kMaxRels];

@@ -366,6 +366,13 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     h->composite_mask = 0;
     h->blob_words = (uint32_t)blob.size();
     h->max_block = (uint32_t)max_block_size(info);
+    long long width_sum = 0;
+    bool width_ok = true;
+    for (int i = 0; i < n; i++) {
+        width_sum += info.base[i].width;
+        width_ok = width_ok && info.base[i].width >= 0;
+    }
+    h->hz_packed = (width_ok && width_sum < (1ll << 21)) ? 1u : 0u;   // kWidthBits
     for (int i = 0; i < n; i++) {
         h->adj[i] = (uint32_t)(info.edge[i] >> 1);
         h->rows[i] = info.base[i].rows;
@@ -443,22 +450,25 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     for (int i = 0; i < n_ec; i++) {
         relids[i] = (uint32_t)(info.ec_relids[i] >> 1);
         offs[i] = ((uint32_t)off_sels << 16) | (uint32_t)off_fks;
+        // member j of the class (in relation order) owns fks/vars[off_fks + j]
+        mask64 m = info.ec_relids[i] >> 1;
+        for (int j = 0; m; j++, m &= m - 1) {
+            const int rel = __builtin_ctzll(m);
+            const int f = off_fks + j;
+            fks[f] = (uint32_t)(info.ec_fks[f] >> 1);
+            const VarInfo &vi = info.ec_vars[f];
+            vars[f].idx_rows = vi.index.rows;
+            vars[f].idx_startup = vi.index.cost.startup;
+            vars[f].idx_total = vi.index.cost.total;
+            vars[f].flags = (vi.index.available ? 1u : 0u) | (vi.index.unique ? 2u : 0u);
+            devvar_bucket_terms(vars[f], vi.stats.stadistinct, vi.stats.stanullfrac, vi.stats.mcvfreq, h->rows[rel],
+                                h->tuples[rel]);
+        }
         int s = popc64(info.ec_relids[i]);
         off_sels += ec_nsels(s);
         off_fks += s;
     }
     for (int i = 0; i < n_sels; i++) sels[i] = info.ec_sels[i];
-    for (int i = 0; i < n_fks; i++) {
-        fks[i] = (uint32_t)(info.ec_fks[i] >> 1);
-        const VarInfo &vi = info.ec_vars[i];
-        vars[i].stadistinct = vi.stats.stadistinct;
-        vars[i].stanullfrac = vi.stats.stanullfrac;
-        vars[i].mcvfreq = vi.stats.mcvfreq;
-        vars[i].idx_rows = vi.index.rows;
-        vars[i].idx_startup = vi.index.cost.startup;
-        vars[i].idx_total = vi.index.cost.total;
-        vars[i].flags = (vi.index.available ? 1u : 0u) | (vi.index.unique ? 2u : 0u);
-    }
     return blob;
 }
 
