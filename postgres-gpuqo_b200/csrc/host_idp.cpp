@@ -18,6 +18,7 @@
 // are identical.  The heaps and priority queues are the same libstdc++
 // algorithms fed in the same order, so their tie behaviour is the reference's.
 #include <algorithm>
+#include <csignal>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -36,6 +37,7 @@
 
 extern "C" int gpuqo_idp_n_iters;
 extern "C" int gpuqo_idp_type;
+extern "C" volatile sig_atomic_t InterruptPending;
 extern "C" void *palloc(size_t size);
 extern "C" void *palloc0(size_t size);
 
@@ -609,6 +611,14 @@ static QT *nodes_to_qt(const std::vector<TreeNode> &nodes, int idx, Arena &A) {
 // gpuqo_run_idp2_dp (gpuqo_idp.cu:123-141) / gpuqo_run_dpdp_union_dp
 // (gpuqo_dpdp_union.cu:254-272): remap, solve, map the plan back
 static QT *solve_sub(const GInfo &info, const std::vector<Entry> &list, Ctx &C) {
+    // a cancel request ends the IDP loop before its next DP; the drivers
+    // unwind normally and the entry point returns NULL with
+    // GPUQO_B200_ERR_CANCELLED (the caller's CHECK_FOR_INTERRUPTS then acts)
+    if (InterruptPending) {
+        C.err = GPUQO_B200_ERR_CANCELLED;
+        C.msg = "cancelled between IDP iterations";
+        return nullptr;
+    }
     Remap R(list, info.n);
     GInfo sub = R.info(info);
     HostInfo h;

@@ -40,3 +40,22 @@ def test_bitmapset_roundtrip():
     for bits in (0b10, 1 << 63, (1 << 64) | 2, (1 << 200) | (1 << 65) | 4):
         b = capi.make_bitmapset(bits)
         assert capi.read_bitmapset(C.addressof(b)) == bits
+
+
+def test_cancel_request_returns_null_before_any_device_work():
+    """With InterruptPending set (Postgres's cancel flag, a weak symbol that the
+    backend's own definition replaces), gpuqo_run returns NULL with
+    GPUQO_B200_ERR_CANCELLED before touching the GPU, so it runs here."""
+    from gpuqo_b200 import query
+    l = lib.load()
+    flag = C.c_int.in_dll(l, "InterruptPending")
+    b = capi.PlannerInfoBuilder(query.star(6, 1))
+    try:
+        flag.value = 1
+        for idp in (0, 3):   # exact DP, and the IDP driver
+            capi.set_int(l, "gpuqo_idp_n_iters", idp)
+            assert not l.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())
+            assert l.gpuqo_b200_last_error() == 6   # GPUQO_B200_ERR_CANCELLED
+    finally:
+        flag.value = 0
+        capi.set_int(l, "gpuqo_idp_n_iters", 0)
