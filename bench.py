@@ -56,6 +56,27 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def rank_seeds(rank):
+    """This rank's query seeds: every rank optimises its own queries (weak
+    scaling, no data-path collective)."""
+    return [s + 1000 * rank for s in SEEDS]
+
+
+def max_over_ranks(x, dist, device):
+    """The largest of every rank's x (device time of the timed region)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_ms_per_query(max_ms, steps, world):
+    """All ranks optimised steps queries each within max_ms."""
+    return max_ms / (steps * world)
+
+
 def measured_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -335,7 +356,7 @@ def main():
 
     from gpuqo_b200 import lib
     lib.load()
-    qs = [query.snowflake(N_RELS, s + 1000 * rank) for s in SEEDS]
+    qs = [query.snowflake(N_RELS, s) for s in rank_seeds(rank)]
 
     def barrier():
         torch.cuda.synchronize()
@@ -370,12 +391,8 @@ def main():
             pairs += st["evaluated_pairs"]
             csgs += st["connected_sets"]
     barrier()
-    max_ms = tot_ms
-    if dist is not None:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        max_ms = float(t.item())
-    value = max_ms / (args.steps * world)
+    max_ms = max_over_ranks(tot_ms, dist, "cuda")
+    value = whole_job_ms_per_query(max_ms, args.steps, world)
 
     # ---- e2e: the C ABI with host structures ----
     for i in range(args.warmup):
@@ -388,11 +405,8 @@ def main():
             raise RuntimeError(f"gpuqo_run failed: {r.error}")
         e2e_ms += r.seconds * 1000.0
     barrier()
-    if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = e2e_ms / (args.steps * world)
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
+    e2e_value = whole_job_ms_per_query(e2e_ms, args.steps, world)
     # bytes crossing the bus per step: the planner-info blob in (header 274
     # words, 2 words per class, its selectivities, 9 words per class member,
     # the 3 n^2 tree tables of a tree-shaped graph; staged in 512-word
