@@ -319,6 +319,37 @@ __device__ __forceinline__ float4 base_entry(const DevHeader &h, int i) {
     return make_float4(h.rows[i], h.startup[i], h.total[i], __uint_as_float(memo_width_word(h, h.rows[i], h.width[i])));
 }
 
+// Plain DPsub's enumeration index of the split (L, S - L): cpu_dpsub visits
+// the nonempty proper subsets L of S in nextSubset order
+// (gpuqo_cpu_dpsub.cu:32-78), i.e. L = pdep(p + 1, S), so p = pext(L, S) - 1.
+// Computed over the smaller side (pext(R, S) is the complement within the
+// |S| low bits).
+__device__ __forceinline__ uint32_t dpsub_index(uint32_t L, uint32_t S) {
+    const uint32_t R = S ^ L;
+    const bool left = __popc(L) <= __popc(R);
+    uint32_t x = left ? L : R, r = 0u;
+    while (x) {
+        const uint32_t b = x & (0u - x);
+        r |= 1u << __popc(S & (b - 1u));
+        x ^= b;
+    }
+    if (!left) {
+        const int k = __popc(S);
+        r ^= (k == 32) ? 0xFFFFFFFFu : ((1u << k) - 1u);
+    }
+    return r - 1u;
+}
+
+// The block enumeration (MPDP) produces exactly the valid csg-cmp pairs of S:
+// all edges between the two connected sides of a valid split lie on common
+// cycles, hence in one biconnected block B, and growing the two parts of B
+// inside S returns the two sides.  Keying each pair by its plain-DPsub index
+// therefore gives cpu_dpsub's first strict minimum (and its first NaN) while
+// skipping the invalid subsets DPsub would test.
+__device__ __forceinline__ uint32_t key_index(const DevHeader &h, uint32_t c, uint32_t L, uint32_t S) {
+    return h.index_order ? dpsub_index(L, S) : c;
+}
+
 // ---------------------------------------------------------------------------
 // One join evaluation: estimate_join_rows + calc_join_cost + width
 // (gpuqo_cpu_common.cuh:169-186 make_join_relation; gpuqo_cost.cuh:81-157).

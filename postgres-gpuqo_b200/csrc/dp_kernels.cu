@@ -367,6 +367,7 @@ __device__ __forceinline__ void eval_range(const DevInfoView &d, const uint32_t 
             }
         }
         uint32_t cp = p;
+        if (MODE == kModeMpdp && valid) cp = key_index(*d.h, p, cl, S);
         if (has) p++;
         if (!ccc) {
             if (valid) evaluate_pair(d, memo, cp, cl, cr, best);
@@ -545,7 +546,7 @@ __device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t
             const uint32_t p = (uint32_t)gl + it * G;
             if (p < myP) {
                 uint32_t L, R;
-                if (mpdp_candidate(S, B, adj, p, b, L, R)) evaluate_pair(d, memo, p, L, R, best);
+                if (mpdp_candidate(S, B, adj, p, b, L, R)) evaluate_pair(d, memo, key_index(*d.h, p, L, S), L, R, best);
             }
         }
         // group reduction: min key, min first candidate (NaN rule)
@@ -691,7 +692,7 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
                 const uint32_t R = S ^ L;
                 const uint32_t post = (uint32_t)(__popc(S & tab[nn + rt * n + ch]) - __popc(S & anc_r[ch]) +
                                                  __popc(comp_c) - 1);
-                const uint32_t p = 2u * post + side;
+                const uint32_t p = h.index_order ? dpsub_index(L, S) : 2u * post + side;
                 uint32_t ecm = 0u;
                 if (MASKED) {
                     const int ch0 = ((tab[2 * nn + b] >> a) & 1u) ? b : a;   // child end w.r.t. relation 0
@@ -1114,7 +1115,7 @@ __global__ void __launch_bounds__(kBlock) k_ovf_finalize(const uint32_t *__restr
         const unsigned long long first = ovf_first[idx];
         const uint32_t p = (first & 1ull) ? (uint32_t)(first >> 1) : (uint32_t)ovf_key[idx];
         uint32_t L, R;
-        if (MODE == kModeDpsub) {
+        if (MODE == kModeDpsub || d.h->index_order) {
             L = pdep32(p + 1u, S);
             R = S ^ L;
         } else {
@@ -2245,7 +2246,7 @@ __device__ __forceinline__ void tree_cand(const DevHeader &h, uint32_t S, int a,
     R = S ^ L;
     const uint32_t post =
         (uint32_t)(__popc(S & __ldg(tab + nn + rt * n + ch)) - __popc(S & __ldg(anc_r + ch)) + __popc(comp_c) - 1);
-    p = 2u * post + side;
+    p = h.index_order ? dpsub_index(L, S) : 2u * post + side;
     ecm = 0u;
     if (masked) {
         const int ch0 = ((__ldg(tab + 2 * nn + b) >> a) & 1u) ? b : a;
@@ -2346,8 +2347,8 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
                     tree_cand(h, S, ea, eb, c, L, R, p, ecm, masked);
                     valid = true;
                 } else {
-                    p = c;
                     valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R);
+                    p = valid ? key_index(h, c, L, S) : c;
                 }
             }
             if (valid) {
@@ -2469,15 +2470,21 @@ __device__ __forceinline__ void batch_ovf_finalize(const BatchQ *qs, const uint3
         float4 *memo = memo_all + Q.memo_off;
         const unsigned long long first = __ldcg(ovf.first + idx);
         const uint32_t p = (first & 1ull) ? (uint32_t)(first >> 1) : (uint32_t)__ldcg(ovf.key + idx);
-        Blocks B;
-        find_blocks(S, adj, B);
-        int b = 0;
-        while (b + 1 < B.nb && B.prefix[b + 1] <= p) b++;
-        const uint32_t blk = B.mask[b];
-        const uint32_t lb = pdep32(p - B.prefix[b] + 1u, blk);
-        const uint32_t rb = blk ^ lb;
-        const uint32_t L = grow(lowest(lb), S & ~rb, adj);
-        const uint32_t R = grow(lowest(rb), S & ~lb, adj);
+        uint32_t L, R;
+        if (d.h->index_order) {   // plain-DPsub index
+            L = pdep32(p + 1u, S);
+            R = S ^ L;
+        } else {
+            Blocks B;
+            find_blocks(S, adj, B);
+            int b = 0;
+            while (b + 1 < B.nb && B.prefix[b + 1] <= p) b++;
+            const uint32_t blk = B.mask[b];
+            const uint32_t lb = pdep32(p - B.prefix[b] + 1u, blk);
+            const uint32_t rb = blk ^ lb;
+            L = grow(lowest(lb), S & ~rb, adj);
+            R = grow(lowest(rb), S & ~lb, adj);
+        }
         const RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
         const RelVal out = join_eval(d, L, l, R, r);
         memo_write(*d.h, memo, memo_left_all + Q.memo_off, S, out, L);

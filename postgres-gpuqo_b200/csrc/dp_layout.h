@@ -83,6 +83,11 @@ struct DevHeader {
     // memo widths carry the inner hash table size (see memo_width_word): set
     // when every width is >= 0 and all of them sum to less than 2^21
     uint32_t hz_packed;
+    // key index of a candidate in the block (MPDP) enumeration: 0 = the MPDP
+    // index (block, subset of the block), 1 = the plain-DPsub index of the
+    // same split (gpuqo_dpsub_csg_enable: DPsub's winner from its valid
+    // pairs only, see dpsub_index)
+    uint32_t index_order;
     uint32_t adj[kMaxRels];
     float rows[kMaxRels];
     float tuples[kMaxRels];

@@ -483,10 +483,25 @@ int exact_dp(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, st
         return GPUQO_B200_ERR_ARGS;
     }
     std::vector<uint32_t> blob = build_blob(info);
+    apply_dpsub_csg(blob, mode);
     EngineStats st;
     int rc = engine_run(blob, info.n, mode, gpuqo_dpsub_ccc_enable, gpuqo_b200_profile_kernels != 0, nodes, st, err);
     if (rc == 0) stats_add(st);
     return rc;
+}
+
+void apply_dpsub_csg(std::vector<uint32_t> &blob, DpMode &mode) {
+    if (mode != kModeDpsub || !gpuqo_dpsub_csg_enable) return;
+    DevHeader *h = reinterpret_cast<DevHeader *>(blob.data());
+    // On a dense graph nearly every subset is a valid split, so the block
+    // enumeration saves nothing and only adds the index computation: keep
+    // the all-subsets enumeration at or above half of all possible edges.
+    // Either enumeration returns the same plan.
+    uint64_t degree_sum = 0;
+    for (int i = 0; i < h->n; i++) degree_sum += (uint64_t)__builtin_popcount(h->adj[i]);
+    if (2 * degree_sum >= (uint64_t)h->n * (uint64_t)(h->n - 1)) return;
+    h->index_order = 1u;
+    mode = kModeMpdp;
 }
 
 DpMode mode_for(int algorithm) {
@@ -622,10 +637,12 @@ extern "C" int gpuqo_b200_time_resident(int gpuqo_algorithm_arg, GpuqoPlannerInf
     std::vector<int> order = bfs_order(info);
     HostInfo remapped = relabel(info, order);
     std::vector<uint32_t> blob = build_blob(remapped);
+    DpMode mode = mode_for(gpuqo_algorithm_arg);
+    apply_dpsub_csg(blob, mode);
     std::vector<TreeNode> nodes;
     EngineStats st;
-    int rc = engine_time_resident(blob, remapped.n, mode_for(gpuqo_algorithm_arg), gpuqo_dpsub_ccc_enable, warmup,
-                                  iters, flush_l2 != 0, *ms_per_iter, nodes, st, err);
+    int rc = engine_time_resident(blob, remapped.n, mode, gpuqo_dpsub_ccc_enable, warmup, iters, flush_l2 != 0,
+                                  *ms_per_iter, nodes, st, err);
     if (rc) {
         set_error(rc, err);
         return rc;
@@ -660,7 +677,8 @@ extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *
     auto prepare = [&](int i) {
         GpuqoPlannerInfoC *c = infos[i];
         const bool idp = c && gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < c->n_rels;
-        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp || mode != kModeMpdp) return;
+        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp) return;
+        DpMode m = mode;
         HostInfo info;
         std::string err;
         if (!convert_info(c, info, err)) return;
@@ -668,7 +686,8 @@ extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *
         if ((int)prep[i].order.size() != info.n) return;
         HostInfo remapped = relabel(info, prep[i].order);
         prep[i].blob = build_blob(remapped);
-        to_batch[i] = batch_eligible(prep[i].blob) ? 1 : 0;
+        apply_dpsub_csg(prep[i].blob, m);
+        to_batch[i] = (m == kModeMpdp && batch_eligible(prep[i].blob)) ? 1 : 0;
     };
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int n_threads = n_queries >= 64 ? std::min({hw, 16, n_queries / 32}) : 1;

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "dp_engine.h"
 #include "gpuqo_b200.h"
 
 namespace gqb {
@@ -62,5 +63,12 @@ HostInfo relabel(const HostInfo &from, const std::vector<int> &from_of_to);
 
 // Device planner-info blob (compact masks, bit i = relation i); n <= 32.
 std::vector<uint32_t> build_blob(const HostInfo &info);
+
+// Plain DPsub with gpuqo_dpsub_csg_enable on a graph with fewer than half of
+// all possible edges: the DP runs on the block (MPDP) enumeration, which
+// visits only the valid csg-cmp pairs, with candidates keyed by their
+// plain-DPsub index (DevHeader::index_order), so the plan is cpu_dpsub's.
+// Switches mode to kModeMpdp and marks the blob; no change otherwise.
+void apply_dpsub_csg(std::vector<uint32_t> &blob, DpMode &mode);
 
 }  // namespace gqb

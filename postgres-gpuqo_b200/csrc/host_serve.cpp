@@ -42,7 +42,6 @@ extern "C" bool gpuqo_dpsub_ccc_enable;
 
 namespace gqb {
 
-std::vector<uint32_t> build_blob(const HostInfo &info);
 void set_error(int code, const std::string &msg);
 
 using Clock = std::chrono::steady_clock;
@@ -102,6 +101,7 @@ public:
     int solve(const HostInfo &h, DpMode mode, std::vector<TreeNode> &nodes, std::string &err) {
         SubTask t;
         t.blob = build_blob(h);
+        apply_dpsub_csg(t.blob, mode);
         t.mode = mode;
         t.n = h.n;
         {

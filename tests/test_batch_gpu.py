@@ -113,3 +113,15 @@ def test_batch_large_tree_runs_alone():
     assert lib.get_stats()["kernel_launches"] == 2   # k_dp_tree for the star, kb_dp for the wave
     for q, t in zip(qs, trees):
         assert same_tree(t, lib.run(q, capi.GPUQO_DPSUB, bicc=True).tree), q.name
+
+
+def test_batch_plain_dpsub_rides_the_batch():
+    """Plain DPsub (bicc off) with gpuqo_dpsub_csg_enable runs in the batched
+    kernel as well; every plan is cpu_dpsub's."""
+    qs = query.batch_mix(48, seed=8, nmin=6, nmax=13)   # sparse: below half of all possible edges
+    trees, rc = lib.run_batch(qs, capi.GPUQO_DPSUB, bicc=False)
+    assert rc == 0
+    assert lib.get_stats()["kernel_launches"] == 1
+    for q, t in zip(qs, trees):
+        want, _ = harness.run_port(q, 3)
+        assert same_tree(t, want), q.name

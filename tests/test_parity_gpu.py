@@ -130,3 +130,41 @@ def test_full_size_properties(shape, n, seed):
         r3 = gpu_run(q, 3)
         _check_tree_arithmetic(q, r3.tree)
         assert r3.tree[3] == r5.tree[3]             # same optimum, both enumerators
+
+
+DPSUB_GOLD = [c for c in GOLDEN if c["algorithm"] == 3]
+
+
+def _csg(flag):
+    C = __import__("ctypes")
+    C.c_bool.in_dll(lib.load(), "gpuqo_dpsub_csg_enable").value = bool(flag)
+
+
+@pytest.mark.parametrize("case", DPSUB_GOLD, ids=[f'{c["tag"]}-{c["name"]}' for c in DPSUB_GOLD])
+def test_dpsub_all_subsets_enumeration(case):
+    """gpuqo_dpsub_csg_enable off: plain DPsub tests every subset of every set
+    (the reference's all-subsets enumeration with CCC); on (the default): only
+    the valid csg-cmp pairs, keyed by their DPsub index.  Both return the
+    reference's plan and cost the same valid pairs."""
+    try:
+        _csg(False)
+        a = gpu_run(case["query"], 3)
+    finally:
+        _csg(True)
+    b = gpu_run(case["query"], 3)
+    assert same_tree(a.tree, case["expected"])
+    assert same_tree(b.tree, case["expected"])
+    assert a.stats["evaluated_pairs"] == b.stats["evaluated_pairs"]
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_dpsub_csg_ties_and_dense_graphs(seed):
+    """Cost ties (all-equal graphs) and dense random graphs, where the DPsub
+    and MPDP enumeration orders pick different winners among equal costs:
+    the CSG path keeps DPsub's winner (the oracle restatement of cpu_dpsub)."""
+    qs = [query.random_graph(9 + seed, 7000 + seed, equal=True),
+          query.random_graph(8 + seed, 7100 + seed, extra_edge_p=0.5, rich=True),
+          query.cycle(10 + seed, 7200 + seed), query.multi_member_classes(7 + seed, 7300 + seed)]
+    for q in qs:
+        want, _ = harness.run_port(q, 3)
+        assert same_tree(gpu_run(q, 3).tree, want), q.name
