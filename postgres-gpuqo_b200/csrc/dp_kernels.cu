@@ -2173,7 +2173,10 @@ __device__ __forceinline__ void stage_flush64(unsigned long long *st, uint32_t &
 }
 
 // connected k-sets of every query, by extension of its (k-1)-sets (c_prev
-// items in prev); thread tid of nthreads
+// items in prev); thread tid of nthreads.  TREE_ONLY (every query of the wave
+// tree-shaped): each set is emitted once by the largest-leaf rule of
+// level_sets_phase, without the dedup bitmap.
+template <bool TREE_ONLY>
 __device__ __forceinline__ void batch_extend(const BatchQ *qs, const uint32_t *blobs, const unsigned long long *prev,
                                              uint32_t c_prev, uint32_t *seen, unsigned long long *out,
                                              LevelCounters *lc, unsigned long long *st, uint32_t tid,
@@ -2182,23 +2185,27 @@ __device__ __forceinline__ void batch_extend(const BatchQ *qs, const uint32_t *b
     const uint32_t rounds = (c_prev + nthreads - 1u) / nthreads;
     for (uint32_t r = 0; r < rounds; r++) {
         const uint32_t idx = tid + r * nthreads;
-        uint32_t S = 0u, N = 0u, q = 0u;
+        uint32_t S = 0u, N = 0u, q = 0u, leaves = 0u;
         unsigned long long seen_off = 0;
+        const uint32_t *adj = nullptr;
         if (idx < c_prev) {
             const unsigned long long it = __ldcg(prev + idx);
             q = (uint32_t)(it >> 32);
             S = (uint32_t)it;
             const BatchQ Q = qs[q];
-            const uint32_t *adj = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->adj;
+            adj = reinterpret_cast<const DevHeader *>(blobs + Q.blob_off)->adj;
             seen_off = Q.seen_off;
             uint32_t x = S;
             while (x) {
                 int v = __ffs(x) - 1;
                 x &= x - 1u;
-                N |= __ldg(adj + v);
+                const uint32_t a = __ldg(adj + v);
+                N |= a;
+                if (TREE_ONLY && __popc(a & S) == 1) leaves |= 1u << v;
             }
             N &= ~S;
         }
+        const bool single = (S & (S - 1u)) == 0u;
         const int deg = __popc(N);
         const int maxdeg = (int)__reduce_max_sync(kFull, (uint32_t)deg);
         for (int j = 0; j < maxdeg; j++) {
@@ -2208,8 +2215,13 @@ __device__ __forceinline__ void batch_extend(const BatchQ *qs, const uint32_t *b
                 const uint32_t bitv = N & (0u - N);
                 N ^= bitv;
                 const uint32_t T = S | bitv;
-                const uint32_t bm = 1u << (T & 31u);
-                ok = !(atomicOr(&seen[seen_off + (T >> 5)], bm) & bm);
+                if (TREE_ONLY) {
+                    const uint32_t p = __ldg(adj + (__ffs(bitv) - 1)) & S;   // v's only neighbour in S
+                    ok = (single ? S : (leaves & ~p)) < bitv;                // v is T's largest leaf
+                } else {
+                    const uint32_t bm = 1u << (T & 31u);
+                    ok = !(atomicOr(&seen[seen_off + (T >> 5)], bm) & bm);
+                }
                 item = ((unsigned long long)q << 32) | T;
             }
             stage_emit64(st, cnt, ok, item, out, lc);
@@ -2227,7 +2239,7 @@ __global__ void __launch_bounds__(kBlock) kb_level_sets(const BatchQ *__restrict
                                                         LevelCounters *__restrict__ lc) {
     __shared__ unsigned long long stage[kWarpsPerBlock][64];
     const int warp = threadIdx.x >> 5;
-    batch_extend(qs, blobs, prev, __ldcg(&prev_lc->n_sets), seen, out, lc, stage[warp],
+    batch_extend<false>(qs, blobs, prev, __ldcg(&prev_lc->n_sets), seen, out, lc, stage[warp],
                  blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -2275,7 +2287,7 @@ __device__ __forceinline__ void best_update(LaneBest &best, uint32_t p, uint32_t
     }
 }
 
-template <int G>
+template <int G, bool TREE_ONLY>
 __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *blobs, uint32_t first, uint32_t stride,
                                              const unsigned long long *items, uint32_t count, int k, float4 *memo_all,
                                              uint32_t *memo_left_all, unsigned long long &pairs,
@@ -2297,14 +2309,14 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
         const DevHeader &h = *d.h;
         float4 *memo = memo_all + Q.memo_off;
         uint32_t *memo_left = memo_left_all + Q.memo_off;
-        const bool tree = has && h.tree_mode != 0u;
+        const bool tree = has && (TREE_ONLY || h.tree_mode != 0u);
         const bool masked = tree && h.ec_masked != 0u;
         uint32_t P = 0;
         B.nb = 0;
         if (has) {
             if (tree) {
                 P = 2u * (uint32_t)(k - 1);
-            } else {
+            } else if (!TREE_ONLY) {
                 find_blocks(S, h.adj, B);
                 P = B.total;
                 if (ovf.cap != 0u && P > kOvfLimit) {
@@ -2346,7 +2358,7 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
                     while (ei.e <= (c >> 1)) edge_next(h.adj, S, ei, ea, eb);
                     tree_cand(h, S, ea, eb, c, L, R, p, ecm, masked);
                     valid = true;
-                } else {
+                } else if (!TREE_ONLY) {
                     valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R);
                     p = valid ? key_index(h, c, L, S) : c;
                 }
@@ -2401,9 +2413,9 @@ __global__ void __launch_bounds__(kBlock) kb_eval(const BatchQ *__restrict__ qs,
     BatchOvf none;
     none.cap = 0u;
     LevelCounters *lcw = nullptr;
-    if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, items, count, k, memo, memo_left, pairs, none, lcw);
-    else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, items, count, k, memo, memo_left, pairs, none, lcw);
-    else batch_groups<32>(qs, blobs, gwarp, nwarps, items, count, k, memo, memo_left, pairs, none, lcw);
+    if (G == 2) batch_groups<2, false>(qs, blobs, gwarp * 16, nwarps * 16, items, count, k, memo, memo_left, pairs, none, lcw);
+    else if (G == 8) batch_groups<8, false>(qs, blobs, gwarp * 4, nwarps * 4, items, count, k, memo, memo_left, pairs, none, lcw);
+    else batch_groups<32, false>(qs, blobs, gwarp, nwarps, items, count, k, memo, memo_left, pairs, none, lcw);
     pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
     if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
 }
@@ -2553,7 +2565,8 @@ __global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const uint32_t
 // extracted (one thread per query) after the last level.  The grid barrier
 // is bounded (grid_barrier); on timeout the host reruns the wave with
 // per-level launches.
-__global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs, int nq, int maxn,
+template <bool TREE_ONLY>
+__global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ *__restrict__ qs, int nq, int maxn,
                                                    const uint32_t *__restrict__ blobs, float4 *__restrict__ memo,
                                                    uint32_t *__restrict__ memo_left, uint32_t *__restrict__ seen,
                                                    unsigned long long *__restrict__ listA,
@@ -2607,17 +2620,21 @@ __global__ void __launch_bounds__(kBlock, 2) kb_dp(const BatchQ *__restrict__ qs
         unsigned long long *cur = (k & 1) ? listB : listA;
         unsigned long long *nxt = (k & 1) ? listA : listB;
         const uint32_t count = __ldcg(&lvl[k].n_sets);
-        if (k < maxn) batch_extend(qs, blobs, cur, count, seen, nxt, lvl + k + 1, st, tid, nthreads);
+        if (k < maxn) batch_extend<TREE_ONLY>(qs, blobs, cur, count, seen, nxt, lvl + k + 1, st, tid, nthreads);
         int max_group = 1;
         while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
         int G = 2;
         while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
         G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
         LevelCounters *lk = lvl + k;
-        if (G == 2) batch_groups<2>(qs, blobs, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs, ovf, lk);
-        else if (G == 8) batch_groups<8>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
-        else batch_groups<32>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
+        if (G == 2)
+            batch_groups<2, TREE_ONLY>(qs, blobs, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs, ovf, lk);
+        else if (G == 8)
+            batch_groups<8, TREE_ONLY>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
+        else
+            batch_groups<32, TREE_ONLY>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
         if (!grid_barrier(bar, epoch)) return;
+        if (TREE_ONLY) continue;   // tree sets have 2(k - 1) candidates: never an overflow
         // overflow sets of level k: the counter is final after the barrier, so
         // every block takes the same branch.  A list longer than its capacity
         // is left to the host (the affected queries are rerun one by one).
@@ -2723,7 +2740,8 @@ struct BatchEngine {
     LevelCounters *lvl = nullptr;
     GlobalCounters *glob = nullptr;
     unsigned *bar = nullptr, *h_bar = nullptr;   // grid barrier words of kb_dp (device, pinned copy)
-    int coop_grid = -1;                          // co-resident blocks of kb_dp (0: no cooperative launch)
+    int coop_grid = -1;                          // co-resident blocks of kb_dp<false> (0: no cooperative launch)
+    int coop_grid_tree = -1;                     // co-resident blocks of kb_dp<true>
     BatchOvf ovf{};                              // overflow list of kb_dp
     uint64_t cap_ovf = 0;
 
@@ -2738,12 +2756,14 @@ struct BatchEngine {
         CK(cudaMalloc(&glob, sizeof(GlobalCounters)));
         CK(cudaMalloc(&bar, 4 * sizeof(unsigned)));
         CK(cudaMallocHost(&h_bar, 4 * sizeof(unsigned)));
-        int dev_coop = 0, occ = 0;
+        int dev_coop = 0, occ = 0, occ_tree = 0;
         cudaDeviceGetAttribute(&dev_coop, cudaDevAttrCooperativeLaunch, device);
-        if (dev_coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb_dp, kBlock, 0) == cudaSuccess)
+        coop_grid = coop_grid_tree = 0;
+        if (dev_coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb_dp<false>, kBlock, 0) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tree, kb_dp<true>, kBlock, 0) == cudaSuccess) {
             coop_grid = occ * sm_count;
-        else
-            coop_grid = 0;
+            coop_grid_tree = occ_tree * sm_count;
+        }
         cudaGetLastError();
         return 0;
     }
@@ -2770,20 +2790,22 @@ struct BatchEngine {
         return kernels + 1;
     }
 
-    // the wave as one cooperative launch of kb_dp; false when it could not start
-    bool enqueue_persistent(int nq, int maxn, uint64_t seen_words) {
-        if (coop_grid <= 0 || gpuqo_b200_persistent == 0) return false;
+    // the wave as one cooperative launch of kb_dp (kb_dp<true> when every query
+    // is tree-shaped); false when it could not start
+    bool enqueue_persistent(int nq, int maxn, uint64_t seen_words, bool tree_only) {
+        const int grid = tree_only ? coop_grid_tree : coop_grid;
+        if (grid <= 0 || gpuqo_b200_persistent == 0) return false;
         cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
         cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
-        cudaMemsetAsync(seen, 0, seen_words * 4, stream);
+        if (!tree_only) cudaMemsetAsync(seen, 0, seen_words * 4, stream);
         cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), stream);
-        uint32_t target_lanes = (uint32_t)coop_grid * kBlock;
+        uint32_t target_lanes = (uint32_t)grid * kBlock;
         void *args[] = {&qs, &nq, &maxn, &blobs, &memo, &memo_left, &seen, &listA, &listB,
                         &lvl, &glob, &tree, &tree_n, &bar, &target_lanes, &ovf};
-        if (cudaLaunchCooperativeKernel((const void *)kb_dp, dim3(coop_grid), dim3(kBlock), args, 0, stream) !=
-            cudaSuccess) {
+        const void *fn = tree_only ? (const void *)kb_dp<true> : (const void *)kb_dp<false>;
+        if (cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, stream) != cudaSuccess) {
             cudaGetLastError();
-            coop_grid = 0;
+            coop_grid = coop_grid_tree = 0;
             return false;
         }
         return true;
@@ -2799,7 +2821,7 @@ struct BatchEngine {
         return 0;
     }
 
-    bool persistent_ready() const { return coop_grid > 0 && gpuqo_b200_persistent != 0; }
+    bool persistent_ready() const { return coop_grid > 0 && coop_grid_tree > 0 && gpuqo_b200_persistent != 0; }
 
     // One wave: all queries' memos fit.  wb: per query planner-info blob.
     // Queries that this wave could not finish (sets beyond the group limit
@@ -2846,6 +2868,7 @@ struct BatchEngine {
         std::vector<BatchQ> hq(nq);
         uint64_t slots = 0, words = 0, seen_words = 0, items = 0, base = 0, ovf_need = 0;
         int maxn = 0;
+        bool tree_only = true;
         for (int q = 0; q < nq; q++) {
             const DevHeader *h = reinterpret_cast<const DevHeader *>(wb[q]->data());
             const int n = h->n;
@@ -2861,6 +2884,7 @@ struct BatchEngine {
             base += (uint64_t)n;
             maxn = std::max(maxn, n);
             if (batch_needs_ovf(*wb[q])) ovf_need += max_level_sets(n);
+            tree_only = tree_only && h->tree_mode != 0u;
         }
         items = std::max(items, base);
         ovf_need = std::min(ovf_need, kBatchOvfCap);
@@ -2904,7 +2928,7 @@ struct BatchEngine {
         CK(cudaMemcpyAsync(qs, hq.data(), nq * sizeof(BatchQ), cudaMemcpyHostToDevice, stream));
         uint32_t kernels = 1;
         CK(cudaEventRecord(ev0, stream));
-        bool persistent = enqueue_persistent(nq, maxn, seen_words);
+        bool persistent = enqueue_persistent(nq, maxn, seen_words, tree_only);
         CK(cudaGetLastError());
         if (persistent) {
             CK(cudaMemcpyAsync(h_bar, bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
@@ -2984,17 +3008,25 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
         const int n = reinterpret_cast<const DevHeader *>(blobs[i]->data())->n;
         if (int rc = eng->run(*blobs[i], n, kModeMpdp, true, false, out[i], st, err)) return rc;
     }
+    // tree-shaped queries first (waves of kb_dp<true>), then the others; the
+    // order within each part is the caller's (largest first)
+    std::stable_partition(rest.begin(), rest.end(), [&](size_t i) {
+        return reinterpret_cast<const DevHeader *>(blobs[i]->data())->tree_mode != 0u;
+    });
     // waves: consecutive queries while the wave's memory stays within budget
+    // and its queries are all tree-shaped or all not
     size_t r = 0;
     while (r < rest.size()) {
         std::vector<const std::vector<uint32_t> *> wave;
         std::vector<size_t> idx;
         uint64_t bytes = 0;
+        const bool wave_tree = reinterpret_cast<const DevHeader *>(blobs[rest[r]]->data())->tree_mode != 0u;
         while (r < rest.size()) {
             const size_t i = rest[r];
-            const int n = reinterpret_cast<const DevHeader *>(blobs[i]->data())->n;
+            const DevHeader *hi = reinterpret_cast<const DevHeader *>(blobs[i]->data());
+            const int n = hi->n;
             const uint64_t b = batch_query_bytes(n);
-            if (!wave.empty() && bytes + b > wave_bytes) break;
+            if (!wave.empty() && (bytes + b > wave_bytes || (hi->tree_mode != 0u) != wave_tree)) break;
             wave.push_back(blobs[i]);
             idx.push_back(i);
             bytes += b;
