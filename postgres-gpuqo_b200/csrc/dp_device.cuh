@@ -172,11 +172,21 @@ __device__ __forceinline__ Htsz exec_choose_hash_table_size(float ntuples, int t
     return res;
 }
 
+// 1 / v for v = +-2^m, exactly (sign and exponent bits); the bucket counts
+// of the cost model are products of powers of two, or INT_MIN after the x86
+// conversion of 2^31 and above.  Equal to the IEEE quotient, which is exact.
+__device__ __forceinline__ float recip_pow2(int v) {
+    const uint32_t a = v < 0 ? 0u - (uint32_t)v : (uint32_t)v;
+    if (a == 0u || (a & (a - 1u)) != 0u) return 1.0f / (float)v;   // not a power of two
+    const uint32_t m = 31u - (uint32_t)__clz(a);
+    return __uint_as_float((v < 0 ? 0x80000000u : 0u) | ((127u - m) << 23));
+}
+
 // :705-787 __estimate_hash_bucketsize; the relation-only terms come from
 // devvar_bucket_terms, only the bucket count depends on the pair
 __device__ __forceinline__ float bucketsize_one(const DevVar &v, int nbuckets) {
     if (v.flags & kVarNoDistinct) return 0.1f;
-    float estfract = (v.bs_nd > (float)nbuckets) ? 1.0f / (float)nbuckets : v.bs_inv_nd;
+    float estfract = (v.bs_nd > (float)nbuckets) ? recip_pow2(nbuckets) : v.bs_inv_nd;
     if (v.flags & kVarMcvRatio) estfract *= v.bs_mcv_ratio;
     if (estfract < 1.0e-6f) estfract = 1.0e-6f;
     else if (estfract > 1.0f) estfract = 1.0f;
@@ -250,8 +260,6 @@ __device__ __forceinline__ void cost_hashjoin(const DevHeader &h, const RelVal &
         startup_cost += h.seq_page_cost * innerpages;
         run_cost += h.seq_page_cost * (innerpages + 2.0f * outerpages);
     }
-    float virtualbuckets = (float)hz.numbuckets * (float)hz.numbatches;
-    (void)virtualbuckets;
     if (relation_byte_size(clamp_row_est(inner_path_rows * bs_mcvfreq), inner.width) >
         (float)((long long)h.work_mem * 1024LL))
         startup_cost += h.disable_cost;
@@ -262,7 +270,11 @@ __device__ __forceinline__ void cost_hashjoin(const DevHeader &h, const RelVal &
         run_cost += qual_per_tuple * outer_matched_rows *
                     clamp_row_est(inner_path_rows * bs_bucketsize * inner_scan_frac) * 0.5f;
         run_cost += qual_per_tuple * (outer_path_rows - outer_matched_rows) *
-                    clamp_row_est(inner_path_rows / virtualbuckets) * 0.05f;
+                    // virtualbuckets = 2^(log2 numbuckets + log2 numbatches): dividing by it is
+                    // multiplying by its exact reciprocal (same real value, same rounding)
+                    clamp_row_est(inner_path_rows * __uint_as_float(
+                                      (127u - (31u - (uint32_t)__clz(hz.numbuckets)) -
+                                       (31u - (uint32_t)__clz(hz.numbatches))) << 23)) * 0.05f;
         hashjointuples = outer_matched_rows;
     } else {
         startup_cost += 0.0f;

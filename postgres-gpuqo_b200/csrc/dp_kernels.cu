@@ -855,7 +855,9 @@ __device__ __forceinline__ void level_sets_phase(const uint32_t *adj, const uint
     const int lane = threadIdx.x & 31;
     const uint64_t total = binom[n * 33 + k];
     const uint32_t nthreads = gridDim.x * blockDim.x;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // from the far end of the grid: the first warps evaluate the first sets
+    // of the level in the same phase, so small levels split the two jobs
+    const uint32_t tid = nthreads - 1u - (blockIdx.x * blockDim.x + threadIdx.x);
     uint32_t cnt = 0;
     auto emit = [&](bool ok, uint32_t s) {
         uint32_t m = __ballot_sync(kFull, ok);
@@ -2620,7 +2622,8 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
         unsigned long long *cur = (k & 1) ? listB : listA;
         unsigned long long *nxt = (k & 1) ? listA : listB;
         const uint32_t count = __ldcg(&lvl[k].n_sets);
-        if (k < maxn) batch_extend<TREE_ONLY>(qs, blobs, cur, count, seen, nxt, lvl + k + 1, st, tid, nthreads);
+        // enumeration from the far end of the grid, evaluation from the start
+        if (k < maxn) batch_extend<TREE_ONLY>(qs, blobs, cur, count, seen, nxt, lvl + k + 1, st, nthreads - 1u - tid, nthreads);
         int max_group = 1;
         while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
         int G = 2;
