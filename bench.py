@@ -407,7 +407,7 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     e2e_value = whole_job_ms_per_query(e2e_ms, args.steps, world)
-    # bytes crossing the bus per step: the planner-info blob in (header 274
+    # bytes crossing the bus per step: the planner-info blob in (header 339
     # words, 2 words per class, its selectivities, 9 words per class member,
     # the 3 n^2 tree tables of a tree-shaped graph; staged in 512-word
     # buckets); plan nodes (64 x 28 B), tree size, pair counter, 33 level
@@ -416,7 +416,7 @@ def main():
     n_ec = len(q0.eq_classes)
     n_sels = sum(len(e.sels) for e in q0.eq_classes)
     n_fks = sum(len(e.members) for e in q0.eq_classes)
-    words = 274 + 2 * n_ec + n_sels + 9 * n_fks + 3 * N_RELS * N_RELS
+    words = 339 + 2 * n_ec + n_sels + 9 * n_fks + 3 * N_RELS * N_RELS
     h2d = 4 * ((words + 511) // 512 * 512)
     d2h = 64 * 28 + 4 + 8 + 33 * 24 + 16
 

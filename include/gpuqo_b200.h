@@ -292,6 +292,8 @@ typedef struct GpuqoB200ServerStats {
     uint64_t batched_subproblems;   /* exact DPs run inside waves */
     uint64_t single_subproblems;    /* exact DPs run one by one */
     double device_ms;               /* device time of all waves and singles */
+    double busy_ms;                 /* wall time the scheduler spent running waves and singles */
+    double starved_ms;              /* wall time the scheduler waited for sub-problems while requests were open */
 } GpuqoB200ServerStats;
 
 int gpuqo_b200_server_start(int max_inflight, int wave_memory_mb);

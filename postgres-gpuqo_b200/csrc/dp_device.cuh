@@ -403,7 +403,9 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
         uint32_t ec = d.ec_relids[i];
         uint32_t ml = ec & L, mr = ec & R;
         if (!ml || !mr) continue;
-        sel *= ec_selectivity(d, i, ec, ml, mr);
+        // MASKED: a two-member class with one member on each side; its
+        // ec_selectivity for this orientation is tabulated in the header
+        sel *= MASKED ? h.edge_sel[ml > mr ? 1 : 0][i] : ec_selectivity(d, i, ec, ml, mr);
         per_tuple += h.cpu_operator_cost;
         n_quals++;
         int off_fks = (int)(d.ec_off[i] & 0xFFFFu);

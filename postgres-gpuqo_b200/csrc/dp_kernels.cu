@@ -2814,11 +2814,22 @@ struct BatchEngine {
         return true;
     }
 
+    // grows geometrically (twice the old capacity when that is more than the
+    // need) so that waves of changing composition do not reallocate the arena
+    // every time; falls back to the exact need when the larger block does
+    // not fit
     template <class T> int grow(T *&p, uint64_t &cap, uint64_t need, std::string &err) {
         if (need <= cap) return 0;
         if (p) cudaFree(p);
         p = nullptr;
+        const uint64_t want = std::max(need, 2 * cap);
         cap = 0;
+        if (want > need && cudaMalloc(&p, want * sizeof(T)) == cudaSuccess) {
+            cap = want;
+            return 0;
+        }
+        cudaGetLastError();
+        p = nullptr;
         CK(cudaMalloc(&p, need * sizeof(T)));
         cap = need;
         return 0;

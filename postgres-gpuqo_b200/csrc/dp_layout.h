@@ -100,6 +100,11 @@ struct DevHeader {
     // ec_masked: the classes on the edge between relation i and its parent
     // when the query tree is rooted at relation 0
     uint32_t edge_ec[kMaxRels];
+    // ec_masked: ec_selectivity of two-member class i (members x < y) with x
+    // on the outer side (edge_sel[0][i]) and with y there (edge_sel[1][i]);
+    // gpuqo_row_estimation.cuh:49-88 returns a FK selectivity or the class's
+    // stored selectivity, no arithmetic, so the host fills the table exactly
+    float edge_sel[2][kMaxRels];
 };
 
 // Tree tables (tree_mode), appended after the class arrays: for every root r

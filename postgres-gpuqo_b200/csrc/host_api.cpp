@@ -469,6 +469,21 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         off_fks += s;
     }
     for (int i = 0; i < n_sels; i++) sels[i] = info.ec_sels[i];
+    if (h->ec_masked) {
+        // ec_selectivity (gpuqo_row_estimation.cuh:49-88) of each two-member
+        // class in both orientations: the FK selectivity of the outer member's
+        // key into the inner member, else the reverse key, else sels[0]
+        for (int i = 0; i < n_ec; i++) {
+            const uint32_t rr = relids[i];
+            const int x = __builtin_ctz(rr), y = 31 - __builtin_clz(rr);
+            const int off_f = (int)(offs[i] & 0xFFFFu), off_s = (int)(offs[i] >> 16);
+            const bool fk_xy = (fks[off_f + 0] >> y) & 1u;   // member x's key matches y
+            const bool fk_yx = (fks[off_f + 1] >> x) & 1u;   // member y's key matches x
+            const float s = sels[off_s];
+            h->edge_sel[0][i] = fk_xy ? h->fksel[y] : (fk_yx ? h->fksel[x] : s);
+            h->edge_sel[1][i] = fk_yx ? h->fksel[x] : (fk_xy ? h->fksel[y] : s);
+        }
+    }
     return blob;
 }
 

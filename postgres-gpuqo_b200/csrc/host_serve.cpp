@@ -86,7 +86,7 @@ public:
 
     // counters
     uint64_t completed = 0, waves = 0, wave_items = 0, singles = 0;
-    double device_ms = 0.0;
+    double device_ms = 0.0, busy_ms = 0.0, starved_ms = 0.0;
 
     int start(std::string &err) {
         if (cudaGetDevice(&device) != cudaSuccess) {
@@ -124,7 +124,10 @@ public:
             std::vector<SubTask *> tasks;
             {
                 std::unique_lock<std::mutex> lk(mu);
+                const bool open = running > 0;
+                const Clock::time_point t_wait = Clock::now();
                 cv_sched.wait(lk, [&] { return stopping || !pending.empty(); });
+                if (open) starved_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_wait).count();
                 if (stopping && pending.empty()) return;
                 // admit pending sub-problems while the wave's memory fits
                 uint64_t bytes = 0;
@@ -137,6 +140,7 @@ public:
                     bytes += b;
                 }
             }
+            const Clock::time_point t_busy = Clock::now();
             std::vector<SubTask *> batch, one;
             for (SubTask *t : tasks)
                 if (t->mode == kModeMpdp && t->n <= 30 && batch_eligible(t->blob)) batch.push_back(t);
@@ -175,6 +179,8 @@ public:
                 t->done = true;
                 cv_sub.notify_all();
             }
+            std::lock_guard<std::mutex> lk(mu);
+            busy_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_busy).count();
         }
     }
 
@@ -311,6 +317,8 @@ extern "C" int gpuqo_b200_server_stats(GpuqoB200ServerStats *out) {
     out->batched_subproblems = g_server->wave_items;
     out->single_subproblems = g_server->singles;
     out->device_ms = g_server->device_ms;
+    out->busy_ms = g_server->busy_ms;
+    out->starved_ms = g_server->starved_ms;
     return GPUQO_B200_OK;
 }
 

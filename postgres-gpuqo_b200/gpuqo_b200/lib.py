@@ -168,7 +168,8 @@ def get_stats() -> Dict:
 
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("waves", C.c_uint64), ("batched_subproblems", C.c_uint64),
-                ("single_subproblems", C.c_uint64), ("device_ms", C.c_double)]
+                ("single_subproblems", C.c_uint64), ("device_ms", C.c_double), ("busy_ms", C.c_double),
+                ("starved_ms", C.c_double)]
 
 
 class Server:
