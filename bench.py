@@ -356,6 +356,7 @@ def main():
 
     from gpuqo_b200 import lib
     lib.load()
+    tuning = lib.autotune()   # kernel-variant and batch hand-off crossovers of this device (about a second)
     qs = [query.snowflake(N_RELS, s) for s in rank_seeds(rank)]
 
     def barrier():
@@ -433,7 +434,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "b200",
             "config": {"workload": WORKLOAD, "seeds": SEEDS, "queries_per_step_per_gpu": 1,
-                       "l2": "flushed before every step (256 MB write)", "parallelism": f"query-sharded x{world}"},
+                       "l2": "flushed before every step (256 MB write)", "parallelism": f"query-sharded x{world}",
+                       "autotuned": {k: tuning[k] for k in ("single_wide_sets", "batch_single_sets", "tune_ms")}},
             "evaluated_pairs_per_step": pairs / args.steps,
             "connected_sets_per_step": csgs / args.steps,
             "pairs_per_s": pairs / (tot_ms / 1000.0) if tot_ms > 0 else None,

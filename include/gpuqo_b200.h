@@ -296,6 +296,24 @@ typedef struct GpuqoB200ServerStats {
     double starved_ms;              /* wall time the scheduler waited for sub-problems while requests were open */
 } GpuqoB200ServerStats;
 
+/*
+ * Autotuner (no reference counterpart).  Kernel variants and the hand-off
+ * between batch waves and single launches are chosen by connected-set count;
+ * gpuqo_b200_autotune measures both crossovers on the current device (about a
+ * second, synthetic star queries of 14 to 24 relations) and installs them for
+ * later calls.  Plans never depend on these choices.  Until it runs,
+ * gpuqo_b200_get_tuning reports the built-in defaults (tuned = 0).
+ */
+typedef struct GpuqoB200Tuning {
+    double single_wide_sets;   /* tree queries above this many connected sets run the 4-blocks-per-SM kernel */
+    double batch_single_sets;  /* batches run tree queries above this many connected sets as single launches */
+    double tune_ms;            /* wall time of the last gpuqo_b200_autotune, 0 if it never ran */
+    int tuned;
+} GpuqoB200Tuning;
+
+int gpuqo_b200_autotune(GpuqoB200Tuning *out);
+int gpuqo_b200_get_tuning(GpuqoB200Tuning *out);
+
 int gpuqo_b200_server_start(int max_inflight, int wave_memory_mb);
 int gpuqo_b200_server_submit(int gpuqo_algorithm, GpuqoPlannerInfoC *info, uint64_t *ticket);
 int gpuqo_b200_server_wait(uint64_t ticket, QueryTreeC **out, double *latency_ms);

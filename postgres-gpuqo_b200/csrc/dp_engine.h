@@ -60,4 +60,11 @@ uint64_t batch_query_bytes(int n);
 // Device-memory estimate (bytes) of one exact DP over n relations.
 uint64_t engine_bytes_needed(int n);
 
+// Measures, on the given tree-shaped blobs (growing sizes), the connected-set
+// counts from which the 4-blocks-per-SM tree kernel and single launches (over
+// batch waves) win, and installs them for the current device.
+int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_wide_sets,
+                    double &batch_single_sets, std::string &err);
+void engine_get_tuning(double &single_wide_sets, double &batch_single_sets, bool &tuned);
+
 }  // namespace gqb

@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -976,7 +977,12 @@ __device__ __forceinline__ void extract_plan(const float4 *memo, const uint32_t 
     *n_out = n;
 }
 
-__global__ void __launch_bounds__(kBlock, 3) k_dp_tree(const uint32_t *__restrict__ blob, uint32_t blob_words,
+// MINB: blocks per SM the register budget is set for (3: 80 registers, the
+// shorter latency chain for small queries; 4: 64 registers, more warps to
+// hide latency on large levels); chosen per query from its connected-set
+// count (Tuning::single_wide_sets)
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__restrict__ blob, uint32_t blob_words,
                                                        const uint32_t *__restrict__ binom_g, float4 *__restrict__ memo,
                                                        uint32_t *__restrict__ memo_left, uint32_t *__restrict__ setsA,
                                                        uint32_t *__restrict__ setsB, LevelCounters *__restrict__ lvl,
@@ -1241,6 +1247,17 @@ struct GraphKey {
     }
 };
 
+// Parameters the autotuner (engine_autotune) measures; these defaults apply
+// until it runs.  Neither changes a plan, only which kernel variant runs.
+struct Tuning {
+    double single_wide_sets = 1e30;            // tree queries above this many connected sets run k_dp_tree<4>
+    double batch_single_sets = double(1u << 20);   // a batch hands larger tree queries to k_dp_tree
+    bool tuned = false;
+};
+static std::map<int, Tuning> g_tuning;          // per device, guarded by g_mu
+
+static double tree_connected_sets(const DevHeader *h);
+
 class Engine {
 public:
     int device = -1;
@@ -1260,7 +1277,8 @@ public:
     std::vector<cudaEvent_t> kev;      // per-level eval events (profile mode)
     int n_kernels = 0;                 // kernels per DP run
     unsigned *h_bar = nullptr;         // pinned copy of the barrier words
-    std::map<size_t, int> coop_blocks; // dynamic shared bytes -> co-resident blocks of k_dp_tree (0: none)
+    std::map<size_t, int> coop_blocks; // (dynamic shared bytes, variant) -> co-resident blocks of k_dp_tree (0: none)
+    int force_minb = 0;                // autotuner: run this k_dp_tree variant (3 or 4); 0 = by the tuning record
     bool coop_off = false;             // cooperative launch refused on this device
     std::map<GraphKey, int> graph_kernels;
     float *flush = nullptr;            // L2 flush buffer (timing only)
@@ -1441,18 +1459,24 @@ public:
         launched = false;
         const size_t smem = (size_t)(((words + 3u) & ~3u) + 33 * 33 + 3 + kWarpsPerBlock * 64) * 4u;
         if (coop_off) return 0;
-        auto cb = coop_blocks.find(smem);
+        int minb = force_minb;
+        if (minb == 0)
+            minb = tree_connected_sets(reinterpret_cast<const DevHeader *>(h_blob)) > g_tuning[device].single_wide_sets
+                       ? 4
+                       : 3;
+        const void *fn = minb == 4 ? (const void *)k_dp_tree<4> : (const void *)k_dp_tree<3>;
+        const size_t key = smem * 8u + (size_t)minb;
+        auto cb = coop_blocks.find(key);
         if (cb == coop_blocks.end()) {
             int blocks = 0, dev_coop = 0, occ = 0;
             cudaDeviceGetAttribute(&dev_coop, cudaDevAttrCooperativeLaunch, device);
             bool ok = dev_coop != 0;
             if (ok && smem > 48 * 1024)
-                ok = cudaFuncSetAttribute(k_dp_tree, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-                     cudaSuccess;
-            if (ok) ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dp_tree, kBlock, smem) == cudaSuccess;
+                ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
+            if (ok) ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBlock, smem) == cudaSuccess;
             if (ok) blocks = occ * sm_count;
             cudaGetLastError();
-            cb = coop_blocks.emplace(smem, blocks).first;
+            cb = coop_blocks.emplace(key, blocks).first;
         }
         const int grid = cb->second;
         if (grid <= 0) return 0;
@@ -1461,11 +1485,10 @@ public:
         CK(cudaMemsetAsync(a.bar, 0, 4 * sizeof(unsigned), stream));
         CK(cudaMemsetAsync(a.tree_n, 0, sizeof(int), stream));
         uint32_t bwords = words;
-        uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
+        uint32_t target_lanes = (uint32_t)grid * (uint32_t)kBlock;
         void *args[] = {&a.blob, &bwords, &a.binom, &a.memo, &a.memo_left, &a.sets, &a.sets2,
                         &a.lvl, &a.glob, &a.tree, &a.tree_n, &a.bar, &target_lanes};
-        cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_dp_tree, dim3(grid), dim3(kBlock), args,
-                                                    smem, stream);
+        cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, smem, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             coop_off = true;   // do not retry on this engine
@@ -2715,11 +2738,11 @@ static double tree_connected_sets(const DevHeader *h) {
 // A tree-shaped query with this many connected sets fills the GPU on its own:
 // the single-query kernel (k_dp_tree, planner info in shared memory) then
 // evaluates more pairs per second than a batch wave, so the batch hands it over.
-constexpr double kBatchSingleSets = double(1u << 20);
-
-static bool batch_prefers_single(const std::vector<uint32_t> &blob) {
+// (Tuning::batch_single_sets, 2^20 until the autotuner measures it)
+static bool batch_prefers_single(const std::vector<uint32_t> &blob, int device) {
     const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
-    return h->tree_mode != 0u && gpuqo_b200_persistent != 0 && tree_connected_sets(h) > kBatchSingleSets;
+    return h->tree_mode != 0u && gpuqo_b200_persistent != 0 &&
+           tree_connected_sets(h) > g_tuning[device].batch_single_sets;
 }
 
 uint64_t batch_query_bytes(int n) {
@@ -3014,7 +3037,7 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
     // large tree-shaped queries: one persistent single-query launch each
     std::vector<size_t> rest;
     for (size_t i = 0; i < blobs.size(); i++) {
-        if (!batch_prefers_single(*blobs[i])) {
+        if (!batch_prefers_single(*blobs[i], dev)) {
             rest.push_back(i);
             continue;
         }
@@ -3064,6 +3087,83 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
         }
     }
     return 0;
+}
+
+
+// ---------------------------------------------------------------------------
+// Autotuner.  On tree-shaped blobs of growing size (the host passes synthetic
+// stars) it times k_dp_tree<3> and k_dp_tree<4> device-resident, and one
+// batch wave holding about 2^24 connected sets against single launches, then
+// installs in the device's tuning record the two crossovers: from which
+// connected-set count the 4-blocks variant wins at that size and every larger
+// one, and from which count a single launch beats its share of a wave.
+// ---------------------------------------------------------------------------
+static double crossover(const std::vector<double> &sets, const std::vector<bool> &wins) {
+    size_t i = wins.size();
+    while (i > 0 && wins[i - 1]) i--;
+    if (i == wins.size()) return 1e30;     // never wins
+    if (i == 0) return 0.0;                // wins from the smallest size on
+    return std::sqrt(sets[i - 1] * sets[i]);
+}
+
+int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_wide_sets,
+                    double &batch_single_sets, std::string &err) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        err = "cudaGetDevice failed";
+        return GPUQO_B200_ERR_CUDA;
+    }
+    auto &eng = g_engines[dev];
+    if (!eng) eng.reset(new Engine());
+    auto &be = g_batch[dev];
+    if (!be) be.reset(new BatchEngine());
+    if (int rc = be->init(err)) return rc;
+    std::vector<double> sets;
+    std::vector<bool> wide_wins, single_wins;
+    for (const auto &blob : blobs) {
+        const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+        if (!h->tree_mode) continue;
+        double t[2] = {0.0, 0.0};
+        for (int v = 0; v < 2; v++) {
+            eng->force_minb = 3 + v;
+            std::vector<TreeNode> nodes;
+            EngineStats st;
+            const int rc = eng->time_resident(blob, h->n, kModeMpdp, true, 1, 3, false, t[v], nodes, st, err);
+            eng->force_minb = 0;
+            if (rc) return rc;
+        }
+        const double cs = tree_connected_sets(h);
+        const int m = (int)std::min(256.0, std::max(2.0, std::ceil(double(1u << 24) / cs)));
+        std::vector<const std::vector<uint32_t> *> wave(m, &blob);
+        double wms = 0.0;
+        for (int rep = 0; rep < 2; rep++) {   // the first wave sizes the arena
+            std::vector<std::vector<TreeNode>> wout;
+            std::vector<int> redo;
+            EngineStats st;
+            if (int rc = be->run_wave(wave, wout, redo, st, wms, err)) return rc;
+        }
+        sets.push_back(cs);
+        wide_wins.push_back(t[1] < t[0]);
+        single_wins.push_back(std::min(t[0], t[1]) < wms / m);
+    }
+    single_wide_sets = crossover(sets, wide_wins);
+    batch_single_sets = crossover(sets, single_wins);
+    Tuning &tu = g_tuning[dev];
+    tu.single_wide_sets = single_wide_sets;
+    tu.batch_single_sets = batch_single_sets;
+    tu.tuned = true;
+    return 0;
+}
+
+void engine_get_tuning(double &single_wide_sets, double &batch_single_sets, bool &tuned) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const Tuning &tu = g_tuning[dev];
+    single_wide_sets = tu.single_wide_sets;
+    batch_single_sets = tu.batch_single_sets;
+    tuned = tu.tuned;
 }
 
 }  // namespace gqb

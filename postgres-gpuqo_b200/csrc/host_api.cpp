@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
 #include <string>
 #include <thread>
 #include <vector>
@@ -574,6 +575,8 @@ static QueryTreeC *nodes_to_c(const std::vector<TreeNode> &nodes, int idx, const
     return q;
 }
 
+static double g_tune_ms = 0.0;
+
 QueryTreeC *run_one(int algorithm, GpuqoPlannerInfoC *info_c) {
     t_last_error = GPUQO_B200_OK;
     std::string err;
@@ -664,6 +667,68 @@ extern "C" int gpuqo_b200_time_resident(int gpuqo_algorithm_arg, GpuqoPlannerInf
     }
     stats_add(st);
     if (tree) *tree = nodes_to_c(nodes, 0, order);
+    return GPUQO_B200_OK;
+}
+
+// A seeded star of n relations in the shape of the synthetic workloads: fact
+// table 1e7 rows, dimensions log-uniform in [1e2, 1e5], FK-PK classes.
+static HostInfo synthetic_star(int n, uint32_t seed) {
+    HostInfo h;
+    h.n = n;
+    h.p = read_params();
+    uint32_t x = seed * 2654435761u + 12345u;
+    auto uniform = [&]() {
+        x ^= x << 13;
+        x ^= x >> 17;
+        x ^= x << 5;
+        return (float)(x & 0xFFFFFFu) / 16777216.0f;
+    };
+    for (int i = 0; i < n; i++) {
+        HostBaseRel b{};
+        b.id = bit64(i + 1);
+        b.rows = i == 0 ? 1e7f : std::floor(100.0f * std::pow(1000.0f, uniform()));
+        b.tuples = b.rows;
+        b.width = 8;
+        b.cost.startup = 0.0f;
+        b.cost.total = b.rows * 0.01f;
+        b.composite = false;
+        h.base.push_back(b);
+    }
+    h.edge.assign(n, 0);
+    for (int i = 1; i < n; i++) {
+        h.edge[0] |= bit64(i + 1);
+        h.edge[i] |= bit64(1);
+        h.ec_relids.push_back(bit64(1) | bit64(i + 1));
+        h.ec_sels.push_back(1.0f / h.base[i].rows);
+        h.ec_fks.push_back(bit64(i + 1));   // the fact's key references dimension i
+        h.ec_fks.push_back(0);
+        h.ec_vars.push_back(VarInfo{});
+        h.ec_vars.push_back(VarInfo{});
+    }
+    return h;
+}
+
+extern "C" int gpuqo_b200_autotune(GpuqoB200Tuning *out) {
+    t_last_error = GPUQO_B200_OK;
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::vector<uint32_t>> blobs;
+    for (int n : {14, 16, 18, 19, 20, 21, 22, 23, 24}) blobs.push_back(build_blob(synthetic_star(n, 7u + n)));
+    double wide = 0.0, single = 0.0;
+    std::string err;
+    if (int rc = engine_autotune(blobs, wide, single, err)) {
+        set_error(rc, err);
+        return rc;
+    }
+    g_tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return gpuqo_b200_get_tuning(out);
+}
+
+extern "C" int gpuqo_b200_get_tuning(GpuqoB200Tuning *out) {
+    if (!out) return GPUQO_B200_ERR_ARGS;
+    bool tuned = false;
+    engine_get_tuning(out->single_wide_sets, out->batch_single_sets, tuned);
+    out->tuned = tuned ? 1 : 0;
+    out->tune_ms = tuned ? g_tune_ms : 0.0;
     return GPUQO_B200_OK;
 }
 

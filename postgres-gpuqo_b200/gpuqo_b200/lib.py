@@ -166,6 +166,32 @@ def get_stats() -> Dict:
     return st.to_dict()
 
 
+class Tuning(C.Structure):
+    _fields_ = [("single_wide_sets", C.c_double), ("batch_single_sets", C.c_double), ("tune_ms", C.c_double),
+                ("tuned", C.c_int)]
+
+    def to_dict(self) -> Dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+def autotune() -> Dict:
+    """Measure and install the kernel-variant and batch hand-off crossovers
+    on the current device (gpuqo_b200_autotune); returns them."""
+    lib = load()
+    t = Tuning()
+    rc = lib.gpuqo_b200_autotune(C.byref(t))
+    if rc:
+        raise RuntimeError(f"gpuqo_b200_autotune failed: {rc}")
+    return t.to_dict()
+
+
+def get_tuning() -> Dict:
+    lib = load()
+    t = Tuning()
+    lib.gpuqo_b200_get_tuning(C.byref(t))
+    return t.to_dict()
+
+
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("waves", C.c_uint64), ("batched_subproblems", C.c_uint64),
                 ("single_subproblems", C.c_uint64), ("device_ms", C.c_double), ("busy_ms", C.c_double),
