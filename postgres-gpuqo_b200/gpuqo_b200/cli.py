@@ -30,6 +30,7 @@ def main(argv=None):
     ap.add_argument("--mix", action="store_true", help="batch of the mixed workload instead of one shape")
     ap.add_argument("--idp", type=int, default=0, help="gpuqo_idp_n_iters (IDP2 when > 1)")
     ap.add_argument("--persistent", type=int, default=1, help="gpuqo_b200_persistent")
+    ap.add_argument("--autotune", action="store_true", help="run gpuqo_b200_autotune first")
     a = ap.parse_args(argv)
 
     L = lib.load()
@@ -38,6 +39,8 @@ def main(argv=None):
     capi.set_int(L, "gpuqo_idp_n_iters", a.idp)
     capi.set_int(L, "gpuqo_idp_type", capi.GPUQO_IDP2)
     capi.set_int(L, "gpuqo_b200_persistent", a.persistent)
+    if a.autotune:
+        print("tuning:", lib.autotune(), flush=True)
     if a.batch:
         qs = (query.batch_mix(a.batch, seed=a.seed, nmin=a.nmin, nmax=a.n) if a.mix else
               [query.make(a.shape, a.n, a.seed + i) for i in range(a.batch)])
