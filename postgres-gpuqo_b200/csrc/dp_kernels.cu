@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1258,6 +1259,18 @@ static std::map<int, Tuning> g_tuning;          // per device, guarded by g_mu
 
 static double tree_connected_sets(const DevHeader *h);
 
+// Per-run control words of the single-query engine, contiguous so that one
+// memset clears the counters and one copy brings everything back.
+struct EngineCtl {
+    LevelCounters lvl[33];
+    GlobalCounters glob;
+    unsigned bar[4];                   // grid barrier of k_dp_tree: arrivals, -, error flag
+    int tree_n;
+    int pad;
+    TreeNode tree[64];
+};
+constexpr size_t kCtlClearBytes = offsetof(EngineCtl, pad);   // lvl .. tree_n
+
 class Engine {
 public:
     int device = -1;
@@ -1268,7 +1281,9 @@ public:
     uint64_t cap_sets = 0;
     uint32_t blob_cap_words = 0;
     uint32_t *h_blob = nullptr;        // pinned staging
-    TreeNode *h_tree = nullptr;        // pinned
+    EngineCtl *d_ctl = nullptr;        // device control words (a.lvl, a.glob, a.bar, a.tree_n, a.tree point here)
+    EngineCtl *h_ctl = nullptr;        // pinned copy
+    TreeNode *h_tree = nullptr;        // views into h_ctl
     int *h_tree_n = nullptr;
     GlobalCounters *h_glob = nullptr;
     LevelCounters *h_lvl = nullptr;
@@ -1292,16 +1307,18 @@ public:
         CK(cudaEventCreate(&ev1));
         kev.resize(2 * 34);
         for (auto &e : kev) CK(cudaEventCreate(&e));
-        CK(cudaMallocHost(&h_tree, 64 * sizeof(TreeNode)));
-        CK(cudaMallocHost(&h_tree_n, sizeof(int)));
-        CK(cudaMallocHost(&h_glob, sizeof(GlobalCounters)));
-        CK(cudaMallocHost(&h_lvl, 33 * sizeof(LevelCounters)));
-        CK(cudaMalloc(&a.lvl, 33 * sizeof(LevelCounters)));
-        CK(cudaMalloc(&a.glob, sizeof(GlobalCounters)));
-        CK(cudaMalloc(&a.tree, 64 * sizeof(TreeNode)));
-        CK(cudaMalloc(&a.tree_n, sizeof(int)));
-        CK(cudaMalloc(&a.bar, 4 * sizeof(unsigned)));
-        CK(cudaMallocHost(&h_bar, 4 * sizeof(unsigned)));
+        CK(cudaMalloc(&d_ctl, sizeof(EngineCtl)));
+        CK(cudaMallocHost(&h_ctl, sizeof(EngineCtl)));
+        a.lvl = d_ctl->lvl;
+        a.glob = &d_ctl->glob;
+        a.bar = d_ctl->bar;
+        a.tree_n = &d_ctl->tree_n;
+        a.tree = d_ctl->tree;
+        h_lvl = h_ctl->lvl;
+        h_glob = &h_ctl->glob;
+        h_bar = h_ctl->bar;
+        h_tree_n = &h_ctl->tree_n;
+        h_tree = h_ctl->tree;
         CK(cudaMalloc(&a.binom, 33 * 33 * sizeof(uint32_t)));
         std::vector<uint32_t> bt(33 * 33, 0);
         for (int i = 0; i <= 32; i++)
@@ -1369,8 +1386,7 @@ public:
         const uint32_t max_block = reinterpret_cast<const DevHeader *>(h_blob)->max_block;
         const bool tree_mode = reinterpret_cast<const DevHeader *>(h_blob)->tree_mode != 0u;
         const int eval_max_blocks = sm_count * 4;
-        CK(cudaMemsetAsync(a.lvl, 0, 33 * sizeof(LevelCounters), stream));
-        CK(cudaMemsetAsync(a.glob, 0, sizeof(GlobalCounters), stream));
+        CK(cudaMemsetAsync(d_ctl, 0, kCtlClearBytes, stream));
         CK(cudaMemsetAsync(a.seen, 0, std::max<uint64_t>((1ull << n) / 8, 4), stream));
         n_kernels = 0;
         k_init_base<<<1, 32, 0, stream>>>(a.blob, a.memo, a.memo_left);
@@ -1446,10 +1462,7 @@ public:
     }
 
     int download(std::string &err) {
-        CK(cudaMemcpyAsync(h_tree, a.tree, 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(h_tree_n, a.tree_n, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(h_glob, a.glob, sizeof(GlobalCounters), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(h_lvl, a.lvl, 33 * sizeof(LevelCounters), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream));
         return 0;
     }
 
@@ -1480,10 +1493,7 @@ public:
         }
         const int grid = cb->second;
         if (grid <= 0) return 0;
-        CK(cudaMemsetAsync(a.lvl, 0, 33 * sizeof(LevelCounters), stream));
-        CK(cudaMemsetAsync(a.glob, 0, sizeof(GlobalCounters), stream));
-        CK(cudaMemsetAsync(a.bar, 0, 4 * sizeof(unsigned), stream));
-        CK(cudaMemsetAsync(a.tree_n, 0, sizeof(int), stream));
+        CK(cudaMemsetAsync(d_ctl, 0, kCtlClearBytes, stream));   // counters, barrier words, tree size
         uint32_t bwords = words;
         uint32_t target_lanes = (uint32_t)grid * (uint32_t)kBlock;
         void *args[] = {&a.blob, &bwords, &a.binom, &a.memo, &a.memo_left, &a.sets, &a.sets2,
@@ -1499,9 +1509,10 @@ public:
         return 0;
     }
 
-    // true when the last persistent run's grid barrier timed out
+    // brings the control words back (one copy) and reports whether the last
+    // persistent run's grid barrier timed out
     int barrier_failed(bool &failed, std::string &err) {
-        CK(cudaMemcpyAsync(h_bar, a.bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        if (int rc = download(err)) return rc;
         CK(cudaStreamSynchronize(stream));
         failed = h_bar[2] != 0u;
         return 0;
@@ -1576,8 +1587,10 @@ public:
     }
 
     // Copies the plan and counters back and fills nodes / stats.
-    int finish(int n, bool profile, std::vector<TreeNode> &nodes, EngineStats &st, std::string &err) {
-        if (int rc = download(err)) return rc;
+    int finish(int n, bool profile, std::vector<TreeNode> &nodes, EngineStats &st, std::string &err,
+               bool downloaded = false) {
+        if (!downloaded)
+            if (int rc = download(err)) return rc;
         CK(cudaStreamSynchronize(stream));
         CK(cudaGetLastError());
         if (profile)
@@ -1632,7 +1645,7 @@ public:
                 if (int rc = barrier_failed(failed, err)) return rc;
             }
             if (launched && !failed) {
-                if (int rc = finish(n, false, nodes, st, err)) return rc;
+                if (int rc = finish(n, false, nodes, st, err, true)) return rc;
                 float ms = 0.f;
                 CK(cudaEventElapsedTime(&ms, ev0, ev1));
                 st.device_ms += ms;
@@ -1695,7 +1708,7 @@ public:
             if (usable && iters > 0) {
                 ms_per_iter = total / iters;
                 st.device_ms += ms_per_iter;
-                return finish(n, false, nodes, st, err);
+                return finish(n, false, nodes, st, err, true);
             }
             st.eval_kernel_ms = 0.0;
             st.eval_kernel_launches = 0;
