@@ -392,34 +392,35 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         uint32_t *tab = blob.data() + base_words;
         const int nn = n * n;
         for (int r = 0; r < n; r++) {
-            // preorder from r, children in increasing index order
-            std::vector<int> parent(n, -1), order;
-            std::vector<int> stack(1, r);
-            std::vector<uint32_t> anc(n, 0u);
+            // preorder from r, children in increasing index order (pushed from
+            // the highest index, so the lowest is visited first); n <= 32, so
+            // fixed arrays
+            int parent[32], order[32], stack[32];
+            uint32_t anc[32];
+            int sp = 0, no = 0;
+            for (int v = 0; v < n; v++) parent[v] = -1;
+            anc[r] = 0u;
+            stack[sp++] = r;
             uint32_t before = 0u;
-            while (!stack.empty()) {
-                int u = stack.back();
-                stack.pop_back();
+            while (sp > 0) {
+                const int u = stack[--sp];
                 tab[nn + r * n + u] = before;
                 before |= 1u << u;
-                order.push_back(u);
+                order[no++] = u;
                 tab[2 * nn + r * n + u] = anc[u];
                 uint32_t kids = h->adj[u];
                 if (parent[u] >= 0) kids &= ~(1u << parent[u]);
-                std::vector<int> ch;
                 while (kids) {
-                    ch.push_back(__builtin_ctz(kids));
-                    kids &= kids - 1u;
-                }
-                for (auto it = ch.rbegin(); it != ch.rend(); ++it) {
-                    parent[*it] = u;
-                    anc[*it] = anc[u] | (1u << u);
-                    stack.push_back(*it);
+                    const int c = 31 - __builtin_clz(kids);
+                    kids &= ~(1u << c);
+                    parent[c] = u;
+                    anc[c] = anc[u] | (1u << u);
+                    stack[sp++] = c;
                 }
             }
             for (int v = 0; v < n; v++) tab[r * n + v] = 1u << v;
-            for (auto it = order.rbegin(); it != order.rend(); ++it)
-                if (parent[*it] >= 0) tab[r * n + parent[*it]] |= tab[r * n + *it];
+            for (int i = no - 1; i >= 0; i--)
+                if (parent[order[i]] >= 0) tab[r * n + parent[order[i]]] |= tab[r * n + order[i]];
         }
         // classes on edges: every 2-member class must sit on an edge
         bool masked = n_ec <= 32;
@@ -563,8 +564,7 @@ static QueryTreeC *nodes_to_c(const std::vector<TreeNode> &nodes, int idx, const
     const TreeNode &t = nodes[idx];
     QueryTreeC *q = (QueryTreeC *)palloc(sizeof(QueryTreeC));
     mask64 orig = 0;
-    for (size_t k = 0; k < from_of_to.size(); k++)
-        if (t.set & (1u << k)) orig |= bit64(from_of_to[k] + 1);
+    for (uint32_t x = t.set; x; x &= x - 1u) orig |= bit64(from_of_to[__builtin_ctz(x)] + 1);
     q->id = make_bms(orig);
     q->left = nodes_to_c(nodes, t.left, from_of_to);
     q->right = nodes_to_c(nodes, t.right, from_of_to);
