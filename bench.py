@@ -24,10 +24,10 @@ Printed (rank 0, one JSON line):
            chain, 10% cycle; relation counts uniform in [8,28], and [8,16])
            through gpuqo_b200_run_batch against gpuqo_run one query per call,
            queries per second and a bit-for-bit plan comparison;
-  served - IDP2 (k=25) snowflake queries of 30..1000 relations arriving as a
-           Poisson stream at 1x and 4x the plain capacity into the
-           continuous-batching service: queries/s, p50/p99 latency, against
-           one-at-a-time gpuqo_run (FIFO under the same arrivals).
+  served - IDP2 and UnionDP (k=25) snowflake queries of 30..1000 relations
+           arriving as a Poisson stream at 1x and 4x the plain capacity into
+           the continuous-batching service: queries/s, p50/p99 latency,
+           against one-at-a-time gpuqo_run (FIFO under the same arrivals).
 
 --impl reference times that reference CPU engine alone (rank 0 only).
 """
@@ -235,10 +235,10 @@ def batched_section(seed=7):
 
 
 def served_section(n_req=48, seed=5):
-    """Served IDP2 (k=25) over MPDP: Poisson arrivals of snowflake queries with
-    relation counts log-uniform in [30,1000] into the continuous-batching
-    service, against one-at-a-time plain gpuqo_run (FIFO under the same
-    arrivals, latencies from its measured service times)."""
+    """Served IDP2 and UnionDP (k=25) over MPDP: Poisson arrivals of snowflake
+    queries with relation counts log-uniform in [30,1000] into the
+    continuous-batching service, against one-at-a-time plain gpuqo_run (FIFO
+    under the same arrivals, latencies from its measured service times)."""
     import ctypes as C
     import math
     import threading
@@ -250,59 +250,62 @@ def served_section(n_req=48, seed=5):
     L = lib.load()
     capi.set_bool(L, "gpuqo_dpsub_bicc_enable", True)
     capi.set_int(L, "gpuqo_idp_n_iters", 25)
-    capi.set_int(L, "gpuqo_idp_type", capi.GPUQO_IDP2)
     builders = [capi.PlannerInfoBuilder(q) for q in qs]
-    r = L.gpuqo_run(capi.GPUQO_DPSUB, builders[0].pointer())   # warm-up
-    L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
-    svc, plain = [], []
-    for b in builders:
-        t = time.perf_counter()
-        r = L.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())
-        svc.append(time.perf_counter() - t)
-        plain.append(capi.tree_to_py(r))
+    out = {"workload": f"{n_req} snowflake queries, relation counts log-uniform in [30,1000], gpuqo_idp_n_iters=25 "
+                       f"over MPDP, Poisson arrivals at 1x and 4x the plain capacity", "by_idp_type": {}}
+    for idp_type, tag in ((capi.GPUQO_IDP2, "idp2"), (capi.GPUQO_UNION, "union")):
+        capi.set_int(L, "gpuqo_idp_type", idp_type)
+        r = L.gpuqo_run(capi.GPUQO_DPSUB, builders[0].pointer())   # warm-up
         L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
-    plain_qps = n_req / sum(svc)
-    out = {"workload": f"{n_req} snowflake queries, relation counts log-uniform in [30,1000], IDP2 with "
-                       f"gpuqo_idp_n_iters=25 over MPDP, Poisson arrivals",
-           "plain_qps": plain_qps, "plain_mean_service_ms": 1e3 * sum(svc) / n_req, "rates": []}
-    for mult in (1.0, 4.0):
-        rate = plain_qps * mult
-        arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
-        fin, lats = 0.0, []
-        for a, sv in zip(arr, svc):
-            fin = max(a, fin) + sv
-            lats.append(fin - a)
-        srv = lib.Server(max_inflight=32, wave_memory_mb=32768)
-        res = [None] * n_req
+        svc, plain = [], []
+        for b in builders:
+            t = time.perf_counter()
+            r = L.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())
+            svc.append(time.perf_counter() - t)
+            plain.append(capi.tree_to_py(r))
+            L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
+        plain_qps = n_req / sum(svc)
+        res_t = {"plain_qps": plain_qps, "plain_mean_service_ms": 1e3 * sum(svc) / n_req, "rates": []}
+        for mult in (1.0, 4.0):
+            rate = plain_qps * mult
+            arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
+            fin, lats = 0.0, []
+            for a, sv in zip(arr, svc):
+                fin = max(a, fin) + sv
+                lats.append(fin - a)
+            srv = lib.Server(max_inflight=32, wave_memory_mb=32768)
+            res = [None] * n_req
 
-        def waiter(j, tk):
-            res[j] = srv.wait(tk)
-        ths = []
-        t0 = time.perf_counter()
-        for j in range(n_req):
-            now = time.perf_counter() - t0
-            if arr[j] > now:
-                time.sleep(arr[j] - now)
-            tk = srv.submit_built(builders[j], capi.GPUQO_DPSUB)
-            th = threading.Thread(target=waiter, args=(j, tk))
-            th.start()
-            ths.append(th)
-        for th in ths:
-            th.join()
-        makespan = time.perf_counter() - t0
-        st = srv.stats()
-        srv.stop()
-        lat = [x[2] for x in res]
-        out["rates"].append({
-            "arrival_qps": rate, "served_qps": n_req / makespan, "served_p50_ms": float(np.percentile(lat, 50)),
-            "served_p99_ms": float(np.percentile(lat, 99)),
-            "plain_fifo_p50_ms": 1e3 * float(np.percentile(lats, 50)),
-            "plain_fifo_p99_ms": 1e3 * float(np.percentile(lats, 99)),
-            "plain_fifo_qps": n_req / max(fin, arr[-1]),
-            "identical_plans": all(x[0] == 0 and capi.same_plan(x[1], p) for x, p in zip(res, plain)),
-            "waves": st["waves"], "batched_subproblems": st["batched_subproblems"],
-            "single_subproblems": st["single_subproblems"]})
+            def waiter(j, tk):
+                res[j] = srv.wait(tk)
+            ths = []
+            t0 = time.perf_counter()
+            for j in range(n_req):
+                now = time.perf_counter() - t0
+                if arr[j] > now:
+                    time.sleep(arr[j] - now)
+                tk = srv.submit_built(builders[j], capi.GPUQO_DPSUB)
+                th = threading.Thread(target=waiter, args=(j, tk))
+                th.start()
+                ths.append(th)
+            for th in ths:
+                th.join()
+            makespan = time.perf_counter() - t0
+            st = srv.stats()
+            srv.stop()
+            lat = [x[2] for x in res]
+            res_t["rates"].append({
+                "arrival_qps": rate, "served_qps": n_req / makespan,
+                "served_p50_ms": float(np.percentile(lat, 50)), "served_p99_ms": float(np.percentile(lat, 99)),
+                "plain_fifo_p50_ms": 1e3 * float(np.percentile(lats, 50)),
+                "plain_fifo_p99_ms": 1e3 * float(np.percentile(lats, 99)),
+                "plain_fifo_qps": n_req / max(fin, arr[-1]),
+                "identical_plans": all(x[0] == 0 and capi.same_plan(x[1], p) for x, p in zip(res, plain)),
+                "waves": st["waves"], "batched_subproblems": st["batched_subproblems"],
+                "device_ms": st["device_ms"], "busy_ms": st["busy_ms"], "starved_ms": st["starved_ms"]})
+        out["by_idp_type"][tag] = res_t
     capi.set_int(L, "gpuqo_idp_n_iters", 0)
+    capi.set_int(L, "gpuqo_idp_type", capi.GPUQO_IDP2)
     return out
 
 
