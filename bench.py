@@ -216,7 +216,11 @@ def batched_section(seed=7):
         bs, arr = _prebuilt(qs)
         _, warr = _prebuilt(query.batch_mix(64, seed=seed + 1, nmin=nmin, nmax=min(nmax, 20)))
         run_batch(warr, 64)                                  # warm-up (engines, arenas)
-        dtb, st, trees = run_batch(arr, len(qs))
+        # the short batches (host-heavy: tens of ms) take the median of three
+        # runs; the long one runs once
+        runs = [run_batch(arr, len(qs)) for _ in range(3 if nmax <= 20 else 1)]
+        runs.sort(key=lambda x: x[0])
+        dtb, st, trees = runs[len(runs) // 2]
         t = time.perf_counter()
         same = True
         for b, tb in zip(bs, trees):
@@ -224,7 +228,8 @@ def batched_section(seed=7):
             same = same and capi.same_plan(capi.tree_to_py(r), tb)
             L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
         dtp = time.perf_counter() - t
-        res[tag] = {"queries": len(qs), "batched_qps": len(qs) / dtb, "plain_qps": len(qs) / dtp,
+        res[tag] = {"queries": len(qs), "batched_runs": len(runs), "batched_qps": len(qs) / dtb,
+                    "plain_qps": len(qs) / dtp,
                     "speedup": dtp / dtb, "batched_device_ms": st["device_ms"],
                     "batched_launches": st["kernel_launches"], "identical_plans": same}
     return {"workload": "4096 MPDP queries, shapes 40% star / 40% snowflake / 10% chain / 10% cycle, "
