@@ -60,3 +60,46 @@ def test_large_query_needs_idp():
     q = query.snowflake(70, 3)
     r = lib.run(q, capi.GPUQO_DPSUB, bicc=True, idp_n_iters=0)
     assert r.tree is None and r.error == 5      # GPUQO_B200_ERR_UNSUPPORTED, as the reference returns NULL
+
+
+def test_cancel_between_idp_iterations():
+    """A cancel request (Postgres's InterruptPending) raised while an IDP2 run
+    is in flight ends it before its next sub-problem: NULL and
+    GPUQO_B200_ERR_CANCELLED, nothing left running; with the flag cleared the
+    same query plans normally afterwards."""
+    import ctypes as C
+    import threading
+    import time
+    l = lib.load()
+    flag = C.c_int.in_dll(l, "InterruptPending")
+    q = query.snowflake(1000, 77)
+    capi.set_bool(l, "gpuqo_dpsub_bicc_enable", True)
+    capi.set_int(l, "gpuqo_idp_n_iters", 25)
+    capi.set_int(l, "gpuqo_idp_type", capi.GPUQO_IDP2)
+    b = capi.PlannerInfoBuilder(q)
+    warm = l.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())        # engine and device set-up
+    l.gpuqo_b200_free_query_tree(C.cast(warm, C.c_void_p))
+    t0 = time.perf_counter()
+    full = l.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())        # uncancelled, for its duration
+    full_s = time.perf_counter() - t0
+    assert full
+    want = capi.tree_to_py(full)
+    l.gpuqo_b200_free_query_tree(C.cast(full, C.c_void_p))
+    out = {}
+
+    def run():
+        out["tree"] = l.gpuqo_run(capi.GPUQO_DPSUB, b.pointer())   # ctypes releases the GIL
+        out["err"] = l.gpuqo_b200_last_error()
+    try:
+        th = threading.Thread(target=run)
+        th.start()
+        time.sleep(full_s / 4)
+        flag.value = 1
+        th.join(timeout=60)
+        assert not th.is_alive()
+    finally:
+        flag.value = 0
+    assert not out["tree"] and out["err"] == 6          # GPUQO_B200_ERR_CANCELLED
+    again = lib.run(q, capi.GPUQO_DPSUB, bicc=True, idp_n_iters=25, idp_type=capi.GPUQO_IDP2)
+    capi.set_int(l, "gpuqo_idp_n_iters", 0)
+    assert again.error == 0 and same_tree(again.tree, want)
