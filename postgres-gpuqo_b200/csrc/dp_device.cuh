@@ -487,13 +487,51 @@ __device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, co
 // sides of the split are exactly sub[b] and S - sub[b], which is what the
 // reference's grow() calls return for it (gpuqo_cpu_dpsub_bicc.cu:188-195).
 // ---------------------------------------------------------------------------
+// Two index spaces per set: the reference's (prefix/total: block b owns the
+// 2^|b| - 2 indices of its subsets, in nextSubset order; candidates are keyed
+// and tie-broken by it) and the enumerated one (eprefix/etotal): a block that
+// is a simple cycle of four or more relations enumerates only its
+// |b|(|b| - 1) arcs, the only subsets with both sides connected.
 struct Blocks {
     int nb;
     uint32_t total;               // sum of 2^|b| - 2
+    uint32_t etotal;              // candidates enumerated
+    uint32_t cyc;                 // bit b: block b is a simple cycle of 4+ relations
     uint32_t mask[kMaxRels];
     uint32_t sub[kMaxRels];
     uint32_t prefix[kMaxRels + 1];
+    uint32_t eprefix[kMaxRels + 1];
 };
+
+// pext: the bits of x at the positions of mask, packed (x within mask)
+__device__ __forceinline__ uint32_t pext32(uint32_t x, uint32_t mask) {
+    uint32_t r = 0u;
+    for (; x; x &= x - 1u) r |= 1u << __popc(mask & ((x & (0u - x)) - 1u));
+    return r;
+}
+
+// Arc j of cycle block blk (m relations): start s = j / (m - 1), length
+// j % (m - 1) + 1, walking from the block's lowest relation towards its lower
+// neighbour.  Every nonempty proper connected subset of a cycle is one arc.
+__device__ __forceinline__ uint32_t cycle_arc(uint32_t blk, const uint32_t *adj, uint32_t j, uint32_t m) {
+    const uint32_t s = j / (m - 1u), len = j % (m - 1u) + 1u;
+    int v = __ffs(blk) - 1;
+    const uint32_t nb0 = adj[v] & blk;
+    int prev = 31 - __clz(nb0);   // the higher neighbour: the walk goes to the lower one
+    for (uint32_t i = 0; i < s; i++) {
+        const int nx = __ffs(adj[v] & blk & ~(1u << prev)) - 1;
+        prev = v;
+        v = nx;
+    }
+    uint32_t arc = 1u << v;
+    for (uint32_t i = 1; i < len; i++) {
+        const int nx = __ffs(adj[v] & blk & ~(1u << prev)) - 1;
+        prev = v;
+        v = nx;
+        arc |= 1u << v;
+    }
+    return arc;
+}
 
 __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blocks &B) {
     uint8_t disc[kMaxRels], low[kMaxRels], parent[kMaxRels];
@@ -505,6 +543,8 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
     uint32_t visited = 0;
     B.nb = 0;
     B.total = 0;
+    B.etotal = 0;
+    B.cyc = 0;
     int root = lowest_idx(S);
     visited |= 1u << root;
     disc[root] = (uint8_t)t++;
@@ -529,10 +569,16 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
                         w = vstk[--vsp];
                         blk |= 1u << w;
                     } while (w != u);
+                    const uint32_t m = (uint32_t)popc(blk);
+                    bool cycle = m >= 4u;
+                    for (uint32_t x = blk; cycle && x; x &= x - 1u) cycle = popc(adj[lowest_idx(x)] & blk) == 2;
                     B.prefix[B.nb] = B.total;
+                    B.eprefix[B.nb] = B.etotal;
+                    if (cycle) B.cyc |= 1u << B.nb;
                     B.sub[B.nb] = desc[u];
                     B.mask[B.nb++] = blk;
-                    B.total += (1u << popc(blk)) - 2u;
+                    B.total += (1u << m) - 2u;
+                    B.etotal += cycle ? m * (m - 1u) : (1u << m) - 2u;
                 }
                 if (low[u] < low[p]) low[p] = low[u];
                 desc[p] |= desc[u];
@@ -559,21 +605,23 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
         }
     }
     B.prefix[B.nb] = B.total;
+    B.eprefix[B.nb] = B.etotal;
 }
 
-// Candidate p (0-based, reference enumeration order) of set S with blocks B:
-// the block subset lb is the (p - prefix[b] + 1)-th subset of block b in
-// nextSubset order; left/right are the reference's grow() results.
-// `b` is the caller's cursor (p must not decrease between calls).
-__device__ __forceinline__ bool mpdp_candidate(uint32_t S, const Blocks &B, const uint32_t *adj, uint32_t p, int &b,
-                                               uint32_t &L, uint32_t &R) {
-    while (b + 1 < B.nb && B.prefix[b + 1] <= p) b++;
+// Enumerated candidate c of set S with blocks B (see Blocks): block b and its
+// subset lb (for a cycle block an arc, otherwise the (c - eprefix[b] + 1)-th
+// subset in nextSubset order); left/right are the reference's grow() results
+// and key the candidate's reference index prefix[b] + pext(lb, block) - 1.
+// `b` is the caller's cursor (c must not decrease between calls).
+__device__ __forceinline__ bool mpdp_candidate(uint32_t S, const Blocks &B, const uint32_t *adj, uint32_t c, int &b,
+                                               uint32_t &L, uint32_t &R, uint32_t &key) {
+    while (b + 1 < B.nb && B.eprefix[b + 1] <= c) b++;
     const uint32_t blk = B.mask[b];
-    const uint32_t kk = p - B.prefix[b] + 1u;
+    const uint32_t j = c - B.eprefix[b];
     if (popc(blk) == 2) {
-        // bridge {u, v}: kk = 1 -> lb = lowest vertex, kk = 2 -> the other
+        // bridge {u, v}: j = 0 -> lb = lowest vertex, j = 1 -> the other
         const uint32_t lo = lowest(blk);
-        const uint32_t lb = (kk == 1u) ? lo : (blk ^ lo);
+        const uint32_t lb = (j == 0u) ? lo : (blk ^ lo);
         const uint32_t sub = B.sub[b];
         if (lb & sub) {
             L = sub;
@@ -582,9 +630,18 @@ __device__ __forceinline__ bool mpdp_candidate(uint32_t S, const Blocks &B, cons
             L = S ^ sub;
             R = sub;
         }
+        key = B.prefix[b] + j;
         return true;
     }
-    const uint32_t lb = pdep32(kk, blk), rb = blk ^ lb;
+    uint32_t lb;
+    if ((B.cyc >> b) & 1u) {
+        lb = cycle_arc(blk, adj, j, (uint32_t)popc(blk));
+        key = B.prefix[b] + pext32(lb, blk) - 1u;
+    } else {
+        lb = pdep32(j + 1u, blk);
+        key = B.prefix[b] + j;
+    }
+    const uint32_t rb = blk ^ lb;
     L = grow(lowest(lb), S & ~rb, adj);
     R = grow(lowest(rb), S & ~lb, adj);
     return (L | R) == S;

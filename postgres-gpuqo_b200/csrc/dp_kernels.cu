@@ -336,12 +336,15 @@ __device__ __forceinline__ void eval_range(const DevInfoView &d, const uint32_t 
     uint32_t L = 0;           // MODE 0: current left subset
     int b = 0;                // MODE 1: block index
     uint32_t lb = 0;          // MODE 1: current subset of block b
+    uint32_t key = 0;         // MODE 1: the reference's index of the candidate
     if (p < my_hi) {
         if (MODE == kModeDpsub) {
             L = pdep32(p + 1u, S);
         } else {
-            while (b + 1 < B.nb && B.prefix[b + 1] <= p) b++;
-            lb = pdep32(p - B.prefix[b] + 1u, B.mask[b]);
+            // p counts enumerated candidates (Blocks::eprefix); cycle blocks
+            // decode their arcs per candidate, other blocks walk nextSubset
+            while (b + 1 < B.nb && B.eprefix[b + 1] <= p) b++;
+            if (!((B.cyc >> b) & 1u)) lb = pdep32(p - B.eprefix[b] + 1u, B.mask[b]);
         }
     }
     int qn = 0;   // warp-uniform queue length
@@ -356,20 +359,25 @@ __device__ __forceinline__ void eval_range(const DevInfoView &d, const uint32_t 
                 valid = is_connected(cl, adj) && is_connected(cr, adj);
                 L = next_subset(L, S);
             } else {
-                uint32_t blk = B.mask[b];
+                const uint32_t blk = B.mask[b];
+                const bool cyc = (B.cyc >> b) & 1u;
+                if (cyc) lb = cycle_arc(blk, adj, p - B.eprefix[b], (uint32_t)popc(blk));
                 uint32_t rb = blk ^ lb;
                 cl = grow(lowest(lb), S & ~rb, adj);
                 cr = grow(lowest(rb), S & ~lb, adj);
                 valid = (cl | cr) == S;
-                lb = next_subset(lb, blk);
-                if (lb == blk && b + 1 < B.nb) {
+                // the reference's index of this candidate (Blocks::prefix space)
+                key = B.prefix[b] + (cyc ? pext32(lb, blk) - 1u : p - B.eprefix[b]);
+                if (p + 1u < B.eprefix[b + 1]) {
+                    if (!cyc) lb = next_subset(lb, blk);
+                } else if (b + 1 < B.nb) {
                     b++;
                     lb = lowest(B.mask[b]);
                 }
             }
         }
-        uint32_t cp = p;
-        if (MODE == kModeMpdp && valid) cp = key_index(*d.h, p, cl, S);
+        uint32_t cp = (MODE == kModeMpdp) ? key : p;
+        if (MODE == kModeMpdp && valid) cp = key_index(*d.h, key, cl, S);
         if (has) p++;
         if (!ccc) {
             if (valid) evaluate_pair(d, memo, cp, cl, cr, best);
@@ -468,7 +476,7 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
             P = (1u << k) - 2u;
         } else {
             find_blocks(S, adj, B);
-            P = B.total;
+            P = B.etotal;
         }
         if (P > kOvfLimit) {
             if (lane == 0) {
@@ -525,7 +533,7 @@ __device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t
         B.nb = 0;
         if (has) {
             find_blocks(S, adj, B);
-            P = B.total;
+            P = B.etotal;
         }
         __syncwarp();
         const bool ovf = has && P > kOvfLimit;
@@ -548,7 +556,8 @@ __device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t
             const uint32_t p = (uint32_t)gl + it * G;
             if (p < myP) {
                 uint32_t L, R;
-                if (mpdp_candidate(S, B, adj, p, b, L, R)) evaluate_pair(d, memo, key_index(*d.h, p, L, S), L, R, best);
+                uint32_t key;
+                if (mpdp_candidate(S, B, adj, p, b, L, R, key)) evaluate_pair(d, memo, key_index(*d.h, key, L, S), L, R, best);
             }
         }
         // group reduction: min key, min first candidate (NaN rule)
@@ -2360,7 +2369,7 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
                 P = 2u * (uint32_t)(k - 1);
             } else if (!TREE_ONLY) {
                 find_blocks(S, h.adj, B);
-                P = B.total;
+                P = B.etotal;
                 if (ovf.cap != 0u && P > kOvfLimit) {
                     // to the level's overflow list; one packed atomic assigns the
                     // list index and the first chunk id in the same order
@@ -2401,8 +2410,9 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
                     tree_cand(h, S, ea, eb, c, L, R, p, ecm, masked);
                     valid = true;
                 } else if (!TREE_ONLY) {
-                    valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R);
-                    p = valid ? key_index(h, c, L, S) : c;
+                    uint32_t key;
+                    valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R, key);
+                    p = valid ? key_index(h, key, L, S) : key;
                 }
             }
             if (valid) {
