@@ -510,29 +510,6 @@ __device__ __forceinline__ uint32_t pext32(uint32_t x, uint32_t mask) {
     return r;
 }
 
-// Arc j of cycle block blk (m relations): start s = j / (m - 1), length
-// j % (m - 1) + 1, walking from the block's lowest relation towards its lower
-// neighbour.  Every nonempty proper connected subset of a cycle is one arc.
-__device__ __forceinline__ uint32_t cycle_arc(uint32_t blk, const uint32_t *adj, uint32_t j, uint32_t m) {
-    const uint32_t s = j / (m - 1u), len = j % (m - 1u) + 1u;
-    int v = __ffs(blk) - 1;
-    const uint32_t nb0 = adj[v] & blk;
-    int prev = 31 - __clz(nb0);   // the higher neighbour: the walk goes to the lower one
-    for (uint32_t i = 0; i < s; i++) {
-        const int nx = __ffs(adj[v] & blk & ~(1u << prev)) - 1;
-        prev = v;
-        v = nx;
-    }
-    uint32_t arc = 1u << v;
-    for (uint32_t i = 1; i < len; i++) {
-        const int nx = __ffs(adj[v] & blk & ~(1u << prev)) - 1;
-        prev = v;
-        v = nx;
-        arc |= 1u << v;
-    }
-    return arc;
-}
-
 __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blocks &B) {
     uint8_t disc[kMaxRels], low[kMaxRels], parent[kMaxRels];
     uint8_t stk_u[kMaxRels];
@@ -608,13 +585,45 @@ __device__ __forceinline__ void find_blocks(uint32_t S, const uint32_t *adj, Blo
     B.eprefix[B.nb] = B.etotal;
 }
 
+// Arcs of one cycle block (m relations) in O(1).  The cycle is walked from
+// its lowest relation towards that relation's lower neighbour; pre[i] holds
+// the first i relations of the walk (filled once per block).  Arc j starts at
+// walk position s = j / (m - 1) and has length j % (m - 1) + 1, wrapping
+// around; every nonempty proper connected subset of a cycle is one arc.
+struct CycleCache {
+    int b = -1;                   // block the prefixes belong to
+    uint32_t set = 0u;            // ... of this set
+    uint32_t m = 0u;
+    uint32_t pre[kMaxRels + 1];
+};
+
+__device__ __forceinline__ uint32_t cached_arc(CycleCache &cc, uint32_t S, int b, uint32_t blk, const uint32_t *adj,
+                                               uint32_t j) {
+    if (cc.b != b || cc.set != S) {
+        cc.b = b;
+        cc.set = S;
+        cc.m = (uint32_t)__popc(blk);
+        int v = __ffs(blk) - 1;
+        int prev = 31 - __clz(adj[v] & blk);
+        cc.pre[0] = 0u;
+        for (uint32_t i = 0; i < cc.m; i++) {
+            cc.pre[i + 1] = cc.pre[i] | (1u << v);
+            const int nx = __ffs(adj[v] & blk & ~(1u << prev)) - 1;
+            prev = v;
+            v = nx;
+        }
+    }
+    const uint32_t m = cc.m, s = j / (m - 1u), e = s + j % (m - 1u) + 1u;
+    return e <= m ? (cc.pre[e] ^ cc.pre[s]) : ((cc.pre[m] ^ cc.pre[s]) | cc.pre[e - m]);
+}
+
 // Enumerated candidate c of set S with blocks B (see Blocks): block b and its
 // subset lb (for a cycle block an arc, otherwise the (c - eprefix[b] + 1)-th
 // subset in nextSubset order); left/right are the reference's grow() results
 // and key the candidate's reference index prefix[b] + pext(lb, block) - 1.
 // `b` is the caller's cursor (c must not decrease between calls).
 __device__ __forceinline__ bool mpdp_candidate(uint32_t S, const Blocks &B, const uint32_t *adj, uint32_t c, int &b,
-                                               uint32_t &L, uint32_t &R, uint32_t &key) {
+                                               uint32_t &L, uint32_t &R, uint32_t &key, CycleCache &cc) {
     while (b + 1 < B.nb && B.eprefix[b + 1] <= c) b++;
     const uint32_t blk = B.mask[b];
     const uint32_t j = c - B.eprefix[b];
@@ -635,8 +644,13 @@ __device__ __forceinline__ bool mpdp_candidate(uint32_t S, const Blocks &B, cons
     }
     uint32_t lb;
     if ((B.cyc >> b) & 1u) {
-        lb = cycle_arc(blk, adj, j, (uint32_t)popc(blk));
+        lb = cached_arc(cc, S, b, blk, adj, j);
         key = B.prefix[b] + pext32(lb, blk) - 1u;
+        if (blk == S) {   // the set is the cycle: arc and complement are the two sides
+            L = lb;
+            R = S ^ lb;
+            return true;
+        }
     } else {
         lb = pdep32(j + 1u, blk);
         key = B.prefix[b] + j;

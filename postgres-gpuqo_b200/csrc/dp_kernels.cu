@@ -337,6 +337,7 @@ __device__ __forceinline__ void eval_range(const DevInfoView &d, const uint32_t 
     int b = 0;                // MODE 1: block index
     uint32_t lb = 0;          // MODE 1: current subset of block b
     uint32_t key = 0;         // MODE 1: the reference's index of the candidate
+    CycleCache cc;            // MODE 1: arcs of the current cycle block
     if (p < my_hi) {
         if (MODE == kModeDpsub) {
             L = pdep32(p + 1u, S);
@@ -361,10 +362,15 @@ __device__ __forceinline__ void eval_range(const DevInfoView &d, const uint32_t 
             } else {
                 const uint32_t blk = B.mask[b];
                 const bool cyc = (B.cyc >> b) & 1u;
-                if (cyc) lb = cycle_arc(blk, adj, p - B.eprefix[b], (uint32_t)popc(blk));
+                if (cyc) lb = cached_arc(cc, S, b, blk, adj, p - B.eprefix[b]);
                 uint32_t rb = blk ^ lb;
-                cl = grow(lowest(lb), S & ~rb, adj);
-                cr = grow(lowest(rb), S & ~lb, adj);
+                if (cyc && blk == S) {   // the set is the cycle: arc and complement
+                    cl = lb;
+                    cr = rb;
+                } else {
+                    cl = grow(lowest(lb), S & ~rb, adj);
+                    cr = grow(lowest(rb), S & ~lb, adj);
+                }
                 valid = (cl | cr) == S;
                 // the reference's index of this candidate (Blocks::prefix space)
                 key = B.prefix[b] + (cyc ? pext32(lb, blk) - 1u : p - B.eprefix[b]);
@@ -525,6 +531,7 @@ __device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t
     const int grp = lane / G, gl = lane % G;
     const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
     Blocks B;
+    CycleCache cc;
     for (uint32_t base = first_set; base < count; base += stride_sets) {
         const uint32_t i = base + (uint32_t)grp;
         const bool has = i < count;
@@ -557,7 +564,8 @@ __device__ __forceinline__ void mpdp_groups(const DevInfoView &d, const uint32_t
             if (p < myP) {
                 uint32_t L, R;
                 uint32_t key;
-                if (mpdp_candidate(S, B, adj, p, b, L, R, key)) evaluate_pair(d, memo, key_index(*d.h, key, L, S), L, R, best);
+                if (mpdp_candidate(S, B, adj, p, b, L, R, key, cc))
+                    evaluate_pair(d, memo, key_index(*d.h, key, L, S), L, R, best);
             }
         }
         // group reduction: min key, min first candidate (NaN rule)
@@ -821,10 +829,16 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // reaches e * gridDim.x, so nobody resets it and the last block to arrive has
 // nothing more to do.  Thread 0 arrives with a gpu-scope release reduction
 // (ordering every write its block made before the __syncthreads) and polls
-// with gpu-scope acquire loads.  The verdict is the same for every thread of
-// the block (thread 0 decides); blocks may disagree only after a timeout, and
-// then every later barrier sees the error flag and returns false at once, so
-// all blocks leave.  epoch: the caller's count of barriers passed (thread 0).
+// with gpu-scope acquire loads (ACQUIRE_POLL), or with relaxed loads and one
+// fence once the count is reached: an acquire load also drops the SM's L1
+// contents, which a kernel that keeps its working data in shared memory does
+// not mind (k_dp_tree: the faster barrier) but which costs the batch kernel,
+// whose per-query data is read through L1 while waiting blocks poll on the
+// same SM.  The verdict is the same for every thread of the block (thread 0
+// decides); blocks may disagree only after a timeout, and then every later
+// barrier sees the error flag and returns false at once, so all blocks leave.
+// epoch: the caller's count of barriers passed (thread 0).
+template <bool ACQUIRE_POLL>
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &epoch) {
     __shared__ unsigned s_ok;
     __syncthreads();
@@ -837,8 +851,15 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &epoch) {
         unsigned spins = 0;
         for (;;) {
             unsigned c;
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(bar) : "memory");
-            if (c >= target || *verr != 0u) break;
+            if (ACQUIRE_POLL) {
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(bar) : "memory");
+            } else {
+                asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(bar) : "memory");
+            }
+            if (c >= target || *verr != 0u) {
+                if (!ACQUIRE_POLL) __threadfence();
+                break;
+            }
             if (++spins > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
                 atomicExch(bar + 2, 1u);
                 break;
@@ -1024,7 +1045,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
         memo_left[1u << i] = 0u;
     }
     if (n >= 2) level_sets_phase(adj, binom, st, n, 2, nullptr, (uint32_t)n, setsA, lvl + 2);
-    if (!grid_barrier(bar, epoch)) return;
+    if (!grid_barrier<true>(bar, epoch)) return;
     for (int k = 2; k <= n; k++) {
         uint32_t *cur = (k & 1) ? setsB : setsA;
         uint32_t *nxt = (k & 1) ? setsA : setsB;
@@ -1045,7 +1066,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
             if (masked) tree_groups<32, true>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
             else tree_groups<32, false>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
         }
-        if (!grid_barrier(bar, epoch)) return;
+        if (!grid_barrier<true>(bar, epoch)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t full = (n == 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
@@ -1752,43 +1773,6 @@ public:
 static std::mutex g_mu;
 static std::map<int, std::unique_ptr<Engine>> g_engines;
 
-int engine_run(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, bool profile,
-               std::vector<TreeNode> &nodes, EngineStats &stats, std::string &err) {
-    if (n < 1 || n > 31) {
-        err = "exact DP supports 1..31 relations";
-        return GPUQO_B200_ERR_TOO_LARGE;
-    }
-    std::lock_guard<std::mutex> lk(g_mu);
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-        return GPUQO_B200_ERR_CUDA;
-    }
-    auto &eng = g_engines[dev];
-    if (!eng) eng.reset(new Engine());
-    return eng->run(blob, n, mode, ccc, profile, nodes, stats, err);
-}
-
-int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, int warmup, int iters,
-                         bool flush_l2, double &ms_per_iter, std::vector<TreeNode> &nodes, EngineStats &stats,
-                         std::string &err) {
-    if (n < 1 || n > 31) {
-        err = "exact DP supports 1..31 relations";
-        return GPUQO_B200_ERR_TOO_LARGE;
-    }
-    std::lock_guard<std::mutex> lk(g_mu);
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-        return GPUQO_B200_ERR_CUDA;
-    }
-    auto &eng = g_engines[dev];
-    if (!eng) eng.reset(new Engine());
-    return eng->time_resident(blob, n, mode, ccc, warmup, iters, flush_l2, ms_per_iter, nodes, stats, err);
-}
-
 }  // namespace gqb
 
 // ===========================================================================
@@ -2347,6 +2331,7 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
     const int grp = lane / G, gl = lane % G;
     const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
     Blocks B;
+    CycleCache cc;
     for (uint32_t base = first; base < count; base += stride) {
         const uint32_t i = base + (uint32_t)grp;
         const bool has = i < count;
@@ -2411,7 +2396,7 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
                     valid = true;
                 } else if (!TREE_ONLY) {
                     uint32_t key;
-                    valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R, key);
+                    valid = mpdp_candidate(S, B, h.adj, c, bcur, L, R, key, cc);
                     p = valid ? key_index(h, key, L, S) : key;
                 }
             }
@@ -2666,7 +2651,7 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
         }
         stage_flush64(st, cnt, listA, lvl + 2);
     }
-    if (!grid_barrier(bar, epoch)) return;
+    if (!grid_barrier<false>(bar, epoch)) return;
 
     for (int k = 2; k <= maxn; k++) {
         unsigned long long *cur = (k & 1) ? listB : listA;
@@ -2686,7 +2671,7 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
             batch_groups<8, TREE_ONLY>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
         else
             batch_groups<32, TREE_ONLY>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
-        if (!grid_barrier(bar, epoch)) return;
+        if (!grid_barrier<false>(bar, epoch)) return;
         if (TREE_ONLY) continue;   // tree sets have 2(k - 1) candidates: never an overflow
         // overflow sets of level k: the counter is final after the barrier, so
         // every block takes the same branch.  A list longer than its capacity
@@ -2694,9 +2679,9 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
         const uint32_t n_ovf = (uint32_t)(__ldcg(&lk->ovf_packed) >> 40);
         if (n_ovf != 0u && n_ovf <= ovf.cap) {
             batch_ovf_chunks(qs, blobs, lk, memo, ovf, queues[warp], pairs);
-            if (!grid_barrier(bar, epoch)) return;
+            if (!grid_barrier<false>(bar, epoch)) return;
             batch_ovf_finalize(qs, blobs, lk, memo, memo_left, ovf, tid, nthreads);
-            if (!grid_barrier(bar, epoch)) return;
+            if (!grid_barrier<false>(bar, epoch)) return;
         }
     }
 
@@ -2797,6 +2782,7 @@ struct BatchEngine {
     int coop_grid_tree = -1;                     // co-resident blocks of kb_dp<true>
     BatchOvf ovf{};                              // overflow list of kb_dp
     uint64_t cap_ovf = 0;
+    void *flush = nullptr;                       // L2 flush buffer (device-resident timing only)
 
     int init(std::string &err) {
         if (stream) return 0;
@@ -3116,6 +3102,110 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
     return 0;
 }
 
+
+// One exact DP.  Tree-shaped graphs run k_dp_tree (Engine); other graphs
+// under MPDP enumeration (MPDP, and plain DPsub on valid pairs) run as a
+// one-query wave of the general persistent kernel kb_dp<false>, which has the
+// overflow phases in the same launch; the per-level launches of Engine serve
+// the rest (plain all-subsets DPsub, no cooperative launch, an overfull
+// overflow list, gpuqo_b200_persistent = 0).
+int engine_run(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, bool profile,
+               std::vector<TreeNode> &nodes, EngineStats &stats, std::string &err) {
+    if (n < 1 || n > 31) {
+        err = "exact DP supports 1..31 relations";
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return GPUQO_B200_ERR_CUDA;
+    }
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+    if (mode == kModeMpdp && h->tree_mode == 0u && n <= 30 && gpuqo_b200_persistent != 0 && !profile) {
+        auto &be = g_batch[dev];
+        if (!be) be.reset(new BatchEngine());
+        if (int rc = be->init(err)) return rc;
+        if (be->persistent_ready()) {
+            std::vector<const std::vector<uint32_t> *> wave(1, &blob);
+            std::vector<std::vector<TreeNode>> wout;
+            std::vector<int> redo;
+            EngineStats st;
+            double ms = 0.0;
+            if (int rc = be->run_wave(wave, wout, redo, st, ms, err)) return rc;
+            if (redo.empty()) {
+                nodes = std::move(wout[0]);
+                stats.connected_sets += st.connected_sets;
+                stats.filtered_subsets += st.filtered_subsets;
+                stats.evaluated_pairs += st.evaluated_pairs;
+                stats.memo_bytes = st.memo_bytes;
+                stats.device_ms += st.device_ms;
+                stats.kernel_launches += st.kernel_launches;
+                return 0;
+            }
+        }
+    }
+    auto &eng = g_engines[dev];
+    if (!eng) eng.reset(new Engine());
+    return eng->run(blob, n, mode, ccc, profile, nodes, stats, err);
+}
+
+int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, int warmup, int iters,
+                         bool flush_l2, double &ms_per_iter, std::vector<TreeNode> &nodes, EngineStats &stats,
+                         std::string &err) {
+    if (n < 1 || n > 31) {
+        err = "exact DP supports 1..31 relations";
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return GPUQO_B200_ERR_CUDA;
+    }
+    // the same routing as engine_run: graphs with cycles as one-query waves
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+    if (mode == kModeMpdp && h->tree_mode == 0u && n <= 30 && gpuqo_b200_persistent != 0 && iters > 0) {
+        auto &be = g_batch[dev];
+        if (!be) be.reset(new BatchEngine());
+        if (int rc = be->init(err)) return rc;
+        if (be->persistent_ready()) {
+            std::vector<const std::vector<uint32_t> *> wave(1, &blob);
+            const size_t flush_bytes = 256u << 20;
+            if (flush_l2 && !be->flush) CK(cudaMalloc(&be->flush, flush_bytes));
+            double total = 0.0;
+            bool ok = true;
+            for (int i = 0; ok && i < warmup + iters; i++) {
+                if (flush_l2) CK(cudaMemsetAsync(be->flush, i & 0xFF, flush_bytes, be->stream));
+                std::vector<std::vector<TreeNode>> wout;
+                std::vector<int> redo;
+                EngineStats st;
+                double ms = 0.0;
+                if (int rc = be->run_wave(wave, wout, redo, st, ms, err)) return rc;
+                ok = redo.empty();
+                if (i >= warmup) total += ms;
+                if (ok && i == warmup + iters - 1) {
+                    nodes = std::move(wout[0]);
+                    stats.connected_sets += st.connected_sets;
+                    stats.filtered_subsets += st.filtered_subsets;
+                    stats.evaluated_pairs += st.evaluated_pairs;
+                    stats.memo_bytes = st.memo_bytes;
+                    stats.kernel_launches += st.kernel_launches;
+                }
+            }
+            if (ok) {
+                ms_per_iter = total / iters;
+                stats.device_ms += ms_per_iter;
+                return 0;
+            }
+        }
+    }
+    auto &eng = g_engines[dev];
+    if (!eng) eng.reset(new Engine());
+    return eng->time_resident(blob, n, mode, ccc, warmup, iters, flush_l2, ms_per_iter, nodes, stats, err);
+}
 
 // ---------------------------------------------------------------------------
 // Autotuner.  On tree-shaped blobs of growing size (the host passes synthetic

@@ -58,17 +58,26 @@ def test_persistent_sizes_in_a_row():
         assert same_tree(_run(q, True).tree, want[q.name])
 
 
-NOT_TREES = [query.cycle(12, 801), query.clique(7, 802),
+NOT_TREES = [query.cycle(12, 801), query.cycle(22, 803), query.clique(7, 802),
+             query.random_graph(14, 804, extra_edge_p=0.3, rich=True),
              # a class of three or more members joins every pair of them
              query.multi_member_classes(6, 606), query.multi_member_classes(12, 612)]
 
 
 @pytest.mark.parametrize("q", NOT_TREES, ids=[q.name for q in NOT_TREES])
-def test_not_tree_keeps_level_launches(q):
-    r = _run(q, True)
-    assert r.stats["kernel_launches"] > 1
+def test_not_tree_single_launch(q):
+    """Graphs with cycles run as a one-query wave of the general persistent
+    kernel (kb_dp, overflow phases in the same launch); with
+    gpuqo_b200_persistent = 0 as per-level launches; both give the oracle's
+    plan."""
+    a = _run(q, True)
+    b = _run(q, False)
+    assert a.stats["kernel_launches"] == 1
+    assert b.stats["kernel_launches"] > 1
+    assert a.stats["evaluated_pairs"] == b.stats["evaluated_pairs"]
     want, _ = harness.run_port(q, 5)
-    assert same_tree(r.tree, want)
+    assert same_tree(a.tree, want)
+    assert same_tree(b.tree, want)
 
 
 @pytest.mark.parametrize("warmup,iters", [(0, 1), (2, 3)])
