@@ -418,14 +418,15 @@ def main():
     e2e_value = whole_job_ms_per_query(e2e_ms, args.steps, world)
     # bytes crossing the bus per step: the planner-info blob in (header 339
     # words, 2 words per class, its selectivities, 9 words per class member,
-    # the 3 n^2 tree tables of a tree-shaped graph; staged in 512-word
+    # the per-relation class masks, the 3 n^2 tree tables of a tree-shaped
+    # graph; staged in 512-word
     # buckets); out, one copy of the engine's control block: 33 level counters
     # (24 B), the pair counter, the barrier words, the tree size, 64 plan nodes (28 B)
     q0 = qs[0]
     n_ec = len(q0.eq_classes)
     n_sels = sum(len(e.sels) for e in q0.eq_classes)
     n_fks = sum(len(e.members) for e in q0.eq_classes)
-    words = 339 + 2 * n_ec + n_sels + 9 * n_fks + 3 * N_RELS * N_RELS
+    words = 339 + 2 * n_ec + n_sels + 9 * n_fks + N_RELS * ((n_ec + 31) // 32) + 3 * N_RELS * N_RELS
     h2d = 4 * ((words + 511) // 512 * 512)
     d2h = 33 * 24 + 8 + 16 + 4 + 4 + 64 * 28
 

@@ -172,6 +172,10 @@ __device__ __forceinline__ Htsz exec_choose_hash_table_size(float ntuples, int t
     return res;
 }
 
+// classes of a join found through DevInfoView::rel_ecs up to this many words
+// of 32 classes (1024 classes); beyond, every class is scanned
+constexpr int kMaxEcWords = 32;
+
 // 1 / v for v = +-2^m, exactly (sign and exponent bits); the bucket counts
 // of the cost model are products of powers of two, or INT_MIN after the x86
 // conversion of 2^31 and above.  Equal to the IEEE quotient, which is exact.
@@ -392,13 +396,34 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
     bool inner_unique = false, any_index = false;
     float bucketsize = 1.0f, mcvfreq = 1.0f;
     const int n_ec = h.n_ec;
-    // MASKED: only the classes in ec_mask can match (classes on the split
-    // edge of a tree-shaped query); visited in increasing class order
-    uint32_t mrem = ec_mask;
-    for (int i = 0; MASKED ? (mrem != 0u) : (i < n_ec); i++) {
-        if (MASKED) {
-            i = __ffs(mrem) - 1;
+    // Only classes with a member on each side can match, visited in
+    // increasing class order (the reference's order): MASKED, the classes in
+    // ec_mask (the split edge of a tree-shaped query); otherwise the classes
+    // of L's relations and of R's relations intersected word by word
+    // (rel_ecs), or every class when there are more than kMaxEcWords words.
+    const int ecw = MASKED ? 1 : ec_words(n_ec);
+    const bool by_mask = MASKED || ecw <= kMaxEcWords;
+    uint32_t match[kMaxEcWords];
+    if (MASKED) {
+        match[0] = ec_mask;
+    } else if (by_mask) {
+        for (int w = 0; w < ecw; w++) {
+            uint32_t cl = 0u, cr = 0u;
+            for (uint32_t x = L; x; x &= x - 1u) cl |= d.rel_ecs[lowest_idx(x) * ecw + w];
+            for (uint32_t x = R; x; x &= x - 1u) cr |= d.rel_ecs[lowest_idx(x) * ecw + w];
+            match[w] = cl & cr;
+        }
+    }
+    int w = 0;
+    uint32_t mrem = by_mask ? match[0] : 0u;
+    for (int i = 0;; i++) {
+        if (by_mask) {
+            while (mrem == 0u && ++w < ecw) mrem = match[w];
+            if (mrem == 0u) break;
+            i = (w << 5) + __ffs(mrem) - 1;
             mrem &= mrem - 1u;
+        } else if (i >= n_ec) {
+            break;
         }
         uint32_t ec = d.ec_relids[i];
         uint32_t ml = ec & L, mr = ec & R;
@@ -448,11 +473,16 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
     }
     if (any_index && !((h.composite_mask >> lowest_idx(R)) & 1u)) {
         extra.indexed_join_quals = true;
-        uint32_t mrem2 = ec_mask;
-        for (int i = 0; MASKED ? (mrem2 != 0u) : (i < n_ec); i++) {
-            if (MASKED) {
-                i = __ffs(mrem2) - 1;
+        int w2 = 0;
+        uint32_t mrem2 = by_mask ? match[0] : 0u;
+        for (int i = 0;; i++) {
+            if (by_mask) {
+                while (mrem2 == 0u && ++w2 < ecw) mrem2 = match[w2];
+                if (mrem2 == 0u) break;
+                i = (w2 << 5) + __ffs(mrem2) - 1;
                 mrem2 &= mrem2 - 1u;
+            } else if (i >= n_ec) {
+                break;
             }
             uint32_t ec = d.ec_relids[i];
             uint32_t ml = ec & L, mr = ec & R;

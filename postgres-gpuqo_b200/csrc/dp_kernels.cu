@@ -1912,7 +1912,7 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         n_fks += s;
     }
     if (n_sels >= 65536 || n_fks >= 65536) return GPUQO_B200_ERR_ARGS;
-    words = blob_words_for(n_ec, n_sels, n_fks);
+    words = blob_words_for(n, n_ec, n_sels, n_fks);
     if (words > kNoAllocMaxBlobWords) return GPUQO_B200_ERR_ARGS;
     for (uint32_t i = 0; i < words; i++) blob[i] = 0u;
     DevHeader *h = reinterpret_cast<DevHeader *>(blob);
@@ -1983,6 +1983,7 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         off_sels += s * (s - 1) / 2;
         off_fks += s;
     }
+    fill_rel_ecs(v, n);
     return 0;
 }
 

@@ -124,6 +124,9 @@ struct DevInfoView {
     const float *sels;
     const uint32_t *fks;
     const DevVar *vars;
+    // rel_ecs[v * ecw + w]: bit b set when class 32 w + b has relation v as a
+    // member (ecw = (n_ec + 31) / 32 words per relation)
+    const uint32_t *rel_ecs;
 };
 
 GQB_HD inline DevInfoView make_view(const void *blob) {
@@ -139,11 +142,29 @@ GQB_HD inline DevInfoView make_view(const void *blob) {
     v.fks = p;
     p += v.h->n_fks;
     v.vars = reinterpret_cast<const DevVar *>(p);
+    p += v.h->n_fks * (sizeof(DevVar) / 4);
+    v.rel_ecs = p;
     return v;
 }
 
-GQB_HD inline uint32_t blob_words_for(int n_ec, int n_sels, int n_fks) {
-    return (uint32_t)(sizeof(DevHeader) / 4 + 2 * n_ec + n_sels + n_fks + n_fks * (sizeof(DevVar) / 4));
+GQB_HD inline int ec_words(int n_ec) { return (n_ec + 31) / 32; }
+
+GQB_HD inline uint32_t blob_words_for(int n, int n_ec, int n_sels, int n_fks) {
+    return (uint32_t)(sizeof(DevHeader) / 4 + 2 * n_ec + n_sels + n_fks + n_fks * (sizeof(DevVar) / 4) +
+                      n * ec_words(n_ec));
+}
+
+// fills DevInfoView::rel_ecs from the class member masks (compact bits)
+GQB_HD inline void fill_rel_ecs(const DevInfoView &v, int n) {
+    uint32_t *out = const_cast<uint32_t *>(v.rel_ecs);
+    const int ecw = ec_words(v.h->n_ec);
+    for (int i = 0; i < n * ecw; i++) out[i] = 0u;
+    for (int e = 0; e < v.h->n_ec; e++)
+        for (uint32_t m = v.ec_relids[e]; m; m &= m - 1u) {
+            int r = 0;
+            while (!((m >> r) & 1u)) r++;
+            out[r * ecw + e / 32] |= 1u << (e % 32);
+        }
 }
 
 }  // namespace gqb

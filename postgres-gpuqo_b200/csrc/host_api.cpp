@@ -350,7 +350,7 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         }
         tree = (seen == (n == 64 ? ~0ull : (bit64(n) - 1)));
     }
-    const uint32_t base_words = blob_words_for(n_ec, n_sels, n_fks);
+    const uint32_t base_words = blob_words_for(n, n_ec, n_sels, n_fks);
     std::vector<uint32_t> blob(base_words + (tree ? tree_tab_words(n) : 0u), 0u);
     DevHeader *h = reinterpret_cast<DevHeader *>(blob.data());
     h->n = n;
@@ -471,6 +471,7 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         off_fks += s;
     }
     for (int i = 0; i < n_sels; i++) sels[i] = info.ec_sels[i];
+    fill_rel_ecs(v, n);
     if (h->ec_masked) {
         // ec_selectivity (gpuqo_row_estimation.cuh:49-88) of each two-member
         // class in both orientations: the FK selectivity of the outer member's
