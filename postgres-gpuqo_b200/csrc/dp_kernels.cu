@@ -689,12 +689,47 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         it.v = 0;
         it.e = 0u;
         int a = 0, b = 0;
+        // G == 32 (one set per warp): the edges of S indexed cooperatively.
+        // Lane t takes the t-th relation of S and its higher-numbered
+        // neighbours in S; the inclusive prefix of their counts numbers the
+        // edges in edge_next's order (lower end, then higher end), so a
+        // candidate finds its edge by a binary search over the lanes instead
+        // of walking the edges before it.
+        int vt = 0;
+        uint32_t fwd = 0u, scan = 0u;
+        if (G == 32) {
+            const int kk = __popc(S);
+            if (lane < kk) {
+                vt = (int)__fns(S, 0u, lane + 1);
+                fwd = h.adj[vt] & S & ~((2u << vt) - 1u);
+            }
+            scan = (uint32_t)__popc(fwd);
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t o = __shfl_up_sync(kFull, scan, off);
+                if (lane >= off) scan += o;
+            }
+        }
         LaneBest best;
         best.init();
         for (uint32_t j = 0; j < per_lane; j++) {
             const uint32_t c = (uint32_t)gl + j * G;
             const bool active = has && c < P;
-            if (active) {
+            if (G == 32) {
+                // smallest lane t with scan_t > e (every lane takes part in the shuffles)
+                const uint32_t e = c >> 1;
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const uint32_t sv = __shfl_sync(kFull, scan, lo + step - 1);
+                    if (sv <= e) lo += step;
+                }
+                const int t = lo > 31 ? 31 : lo;
+                const uint32_t before = __shfl_sync(kFull, scan, t) - (uint32_t)__popc(__shfl_sync(kFull, fwd, t));
+                const uint32_t ft = __shfl_sync(kFull, fwd, t);
+                a = __shfl_sync(kFull, vt, t);
+                if (active) b = (int)__fns(ft, 0u, (int)(e - before) + 1);
+            } else if (active) {
                 const uint32_t target = c >> 1;
                 while (it.e <= target) edge_next(h.adj, S, it, a, b);
             }
