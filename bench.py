@@ -444,7 +444,8 @@ def main():
             "impl": "b200",
             "config": {"workload": WORKLOAD, "seeds": SEEDS, "queries_per_step_per_gpu": 1,
                        "l2": "flushed before every step (256 MB write)", "parallelism": f"query-sharded x{world}",
-                       "autotuned": {k: tuning[k] for k in ("single_wide_sets", "batch_single_sets", "tune_ms")}},
+                       "autotuned": {k: tuning[k] for k in ("single_narrow_level_sets", "single_wide_level_sets",
+                                                            "batch_single_sets", "tune_ms")}},
             "evaluated_pairs_per_step": pairs / args.steps,
             "connected_sets_per_step": csgs / args.steps,
             "pairs_per_s": pairs / (tot_ms / 1000.0) if tot_ms > 0 else None,

@@ -299,13 +299,16 @@ typedef struct GpuqoB200ServerStats {
 /*
  * Autotuner (no reference counterpart).  Kernel variants and the hand-off
  * between batch waves and single launches are chosen by connected-set count;
- * gpuqo_b200_autotune measures both crossovers on the current device (about a
- * second, synthetic star queries of 14 to 24 relations) and installs them for
+ * gpuqo_b200_autotune measures the three crossovers on the current device (about
+ * a second, synthetic star queries of 14 to 24 relations) and installs them for
  * later calls.  Plans never depend on these choices.  Until it runs,
  * gpuqo_b200_get_tuning reports the built-in defaults (tuned = 0).
  */
 typedef struct GpuqoB200Tuning {
-    double single_wide_sets;   /* tree queries above this many connected sets run the 4-blocks-per-SM kernel */
+    double single_narrow_level_sets; /* tree queries with up to this many connected sets per relation
+                                        (their total over n) run the 2-blocks-per-SM kernel */
+    double single_wide_level_sets;   /* tree queries with more connected sets per relation than this run
+                                        the 4-blocks-per-SM kernel; the 3-blocks one in between */
     double batch_single_sets;  /* batches run tree queries above this many connected sets as single launches */
     double tune_ms;            /* wall time of the last gpuqo_b200_autotune, 0 if it never ran */
     int tuned;

@@ -60,11 +60,14 @@ uint64_t batch_query_bytes(int n);
 // Device-memory estimate (bytes) of one exact DP over n relations.
 uint64_t engine_bytes_needed(int n);
 
-// Measures, on the given tree-shaped blobs (growing sizes), the connected-set
-// counts from which the 4-blocks-per-SM tree kernel and single launches (over
-// batch waves) win, and installs them for the current device.
-int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_wide_sets,
-                    double &batch_single_sets, std::string &err);
-void engine_get_tuning(double &single_wide_sets, double &batch_single_sets, bool &tuned);
+// Measures, on the given tree-shaped blobs (growing sizes), the counts of
+// connected sets per level up to which the 2-blocks-per-SM tree kernel wins
+// and from which the 4-blocks-per-SM tree kernel wins, the total count from
+// which single launches win over batch waves, and installs them for the
+// current device.
+int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_narrow_level_sets,
+                    double &single_wide_level_sets, double &batch_single_sets, std::string &err);
+void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets,
+                       bool &tuned);
 
 }  // namespace gqb

@@ -1043,10 +1043,13 @@ __device__ __forceinline__ void extract_plan(const float4 *memo, const uint32_t 
     *n_out = n;
 }
 
-// MINB: blocks per SM the register budget is set for (3: 80 registers, the
-// shorter latency chain for small queries; 4: 64 registers, more warps to
-// hide latency on large levels); chosen per query from its connected-set
-// count (Tuning::single_wide_sets)
+// MINB: blocks per SM the register budget is set for (2: up to 128
+// registers, the cost model without spills and half the barrier arrivals,
+// for small and mid-size queries whose levels are latency-bound; 3: 80
+// registers; 4: 64 registers, more warps to hide latency on large levels);
+// chosen per query from its connected sets per level, the total over the
+// relation count (Tuning::single_narrow_level_sets,
+// Tuning::single_wide_level_sets)
 template <int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__restrict__ blob, uint32_t blob_words,
                                                        const uint32_t *__restrict__ binom_g, float4 *__restrict__ memo,
@@ -1316,7 +1319,10 @@ struct GraphKey {
 // Parameters the autotuner (engine_autotune) measures; these defaults apply
 // until it runs.  Neither changes a plan, only which kernel variant runs.
 struct Tuning {
-    double single_wide_sets = 1e30;            // tree queries above this many connected sets run k_dp_tree<4>
+    // tree queries with up to this many connected sets per level run
+    // k_dp_tree<2>, those with more than single_wide_level_sets k_dp_tree<4>
+    double single_narrow_level_sets = 10240.0;
+    double single_wide_level_sets = 1e30;
     double batch_single_sets = double(1u << 20);   // a batch hands larger tree queries to k_dp_tree
     bool tuned = false;
 };
@@ -1358,7 +1364,7 @@ public:
     int n_kernels = 0;                 // kernels per DP run
     unsigned *h_bar = nullptr;         // pinned copy of the barrier words
     std::map<size_t, int> coop_blocks; // (dynamic shared bytes, variant) -> co-resident blocks of k_dp_tree (0: none)
-    int force_minb = 0;                // autotuner: run this k_dp_tree variant (3 or 4); 0 = by the tuning record
+    int force_minb = 0;                // autotuner: run this k_dp_tree variant (2, 3 or 4); 0 = by the tuning record
     bool coop_off = false;             // cooperative launch refused on this device
     std::map<GraphKey, int> graph_kernels;
     float *flush = nullptr;            // L2 flush buffer (timing only)
@@ -1538,11 +1544,14 @@ public:
         const size_t smem = (size_t)(((words + 3u) & ~3u) + 33 * 33 + 3 + kWarpsPerBlock * 64) * 4u;
         if (coop_off) return 0;
         int minb = force_minb;
-        if (minb == 0)
-            minb = tree_connected_sets(reinterpret_cast<const DevHeader *>(h_blob)) > g_tuning[device].single_wide_sets
-                       ? 4
-                       : 3;
-        const void *fn = minb == 4 ? (const void *)k_dp_tree<4> : (const void *)k_dp_tree<3>;
+        if (minb == 0) {
+            const double per_level = tree_connected_sets(reinterpret_cast<const DevHeader *>(h_blob)) / n;
+            const Tuning &tu = g_tuning[device];
+            minb = per_level <= tu.single_narrow_level_sets ? 2 : (per_level > tu.single_wide_level_sets ? 4 : 3);
+        }
+        const void *fn = minb == 4   ? (const void *)k_dp_tree<4>
+                         : minb == 2 ? (const void *)k_dp_tree<2>
+                                     : (const void *)k_dp_tree<3>;
         const size_t key = smem * 8u + (size_t)minb;
         auto cb = coop_blocks.find(key);
         if (cb == coop_blocks.end()) {
@@ -3245,11 +3254,15 @@ int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, 
 
 // ---------------------------------------------------------------------------
 // Autotuner.  On tree-shaped blobs of growing size (the host passes synthetic
-// stars) it times k_dp_tree<3> and k_dp_tree<4> device-resident, and one
-// batch wave holding about 2^24 connected sets against single launches, then
-// installs in the device's tuning record the two crossovers: from which
-// connected-set count the 4-blocks variant wins at that size and every larger
-// one, and from which count a single launch beats its share of a wave.
+// stars) it times k_dp_tree<2>, <3> and <4> device-resident, and one batch
+// wave holding about 2^24 connected sets against single launches, then
+// installs in the device's tuning record the three crossovers: up to which
+// count of connected sets per level the 2-blocks variant beats the 3-blocks
+// one at that size and every smaller one, from which count per level the
+// 4-blocks variant wins at that size and every larger one (per level: the
+// variants trade latency against throughput within a level, and the count per
+// level carries over from stars to deeper trees, where the total does not),
+// and from which total count a single launch beats its share of a wave.
 // ---------------------------------------------------------------------------
 static double crossover(const std::vector<double> &sets, const std::vector<bool> &wins) {
     size_t i = wins.size();
@@ -3259,8 +3272,17 @@ static double crossover(const std::vector<double> &sets, const std::vector<bool>
     return std::sqrt(sets[i - 1] * sets[i]);
 }
 
-int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_wide_sets,
-                    double &batch_single_sets, std::string &err) {
+// the same from below: the largest count up to which `wins` holds at every size
+static double crossover_below(const std::vector<double> &sets, const std::vector<bool> &wins) {
+    size_t i = 0;
+    while (i < wins.size() && wins[i]) i++;
+    if (i == 0) return 0.0;                // loses at the smallest size
+    if (i == wins.size()) return 1e30;     // wins at every size
+    return std::sqrt(sets[i - 1] * sets[i]);
+}
+
+int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_narrow_level_sets,
+                    double &single_wide_level_sets, double &batch_single_sets, std::string &err) {
     std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
@@ -3272,14 +3294,14 @@ int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &sin
     auto &be = g_batch[dev];
     if (!be) be.reset(new BatchEngine());
     if (int rc = be->init(err)) return rc;
-    std::vector<double> sets;
-    std::vector<bool> wide_wins, single_wins;
+    std::vector<double> sets, level_sets;
+    std::vector<bool> narrow_wins, wide_wins, single_wins;
     for (const auto &blob : blobs) {
         const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
         if (!h->tree_mode) continue;
-        double t[2] = {0.0, 0.0};
-        for (int v = 0; v < 2; v++) {
-            eng->force_minb = 3 + v;
+        double t[3] = {0.0, 0.0, 0.0};   // k_dp_tree<2>, <3>, <4>
+        for (int v = 0; v < 3; v++) {
+            eng->force_minb = 2 + v;
             std::vector<TreeNode> nodes;
             EngineStats st;
             const int rc = eng->time_resident(blob, h->n, kModeMpdp, true, 1, 3, false, t[v], nodes, st, err);
@@ -3297,24 +3319,29 @@ int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &sin
             if (int rc = be->run_wave(wave, wout, redo, st, wms, err)) return rc;
         }
         sets.push_back(cs);
-        wide_wins.push_back(t[1] < t[0]);
-        single_wins.push_back(std::min(t[0], t[1]) < wms / m);
+        level_sets.push_back(cs / h->n);
+        narrow_wins.push_back(t[0] < t[1]);
+        wide_wins.push_back(t[2] < t[1]);
+        single_wins.push_back(std::min(t[0], std::min(t[1], t[2])) < wms / m);
     }
-    single_wide_sets = crossover(sets, wide_wins);
+    single_narrow_level_sets = crossover_below(level_sets, narrow_wins);
+    single_wide_level_sets = crossover(level_sets, wide_wins);
     batch_single_sets = crossover(sets, single_wins);
     Tuning &tu = g_tuning[dev];
-    tu.single_wide_sets = single_wide_sets;
+    tu.single_narrow_level_sets = single_narrow_level_sets;
+    tu.single_wide_level_sets = single_wide_level_sets;
     tu.batch_single_sets = batch_single_sets;
     tu.tuned = true;
     return 0;
 }
 
-void engine_get_tuning(double &single_wide_sets, double &batch_single_sets, bool &tuned) {
+void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets, bool &tuned) {
     std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
     cudaGetDevice(&dev);
     const Tuning &tu = g_tuning[dev];
-    single_wide_sets = tu.single_wide_sets;
+    single_narrow_level_sets = tu.single_narrow_level_sets;
+    single_wide_level_sets = tu.single_wide_level_sets;
     batch_single_sets = tu.batch_single_sets;
     tuned = tu.tuned;
 }

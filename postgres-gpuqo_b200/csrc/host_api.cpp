@@ -714,9 +714,9 @@ extern "C" int gpuqo_b200_autotune(GpuqoB200Tuning *out) {
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<std::vector<uint32_t>> blobs;
     for (int n : {14, 16, 18, 19, 20, 21, 22, 23, 24}) blobs.push_back(build_blob(synthetic_star(n, 7u + n)));
-    double wide = 0.0, single = 0.0;
+    double narrow = 0.0, wide = 0.0, single = 0.0;
     std::string err;
-    if (int rc = engine_autotune(blobs, wide, single, err)) {
+    if (int rc = engine_autotune(blobs, narrow, wide, single, err)) {
         set_error(rc, err);
         return rc;
     }
@@ -727,7 +727,7 @@ extern "C" int gpuqo_b200_autotune(GpuqoB200Tuning *out) {
 extern "C" int gpuqo_b200_get_tuning(GpuqoB200Tuning *out) {
     if (!out) return GPUQO_B200_ERR_ARGS;
     bool tuned = false;
-    engine_get_tuning(out->single_wide_sets, out->batch_single_sets, tuned);
+    engine_get_tuning(out->single_narrow_level_sets, out->single_wide_level_sets, out->batch_single_sets, tuned);
     out->tuned = tuned ? 1 : 0;
     out->tune_ms = tuned ? g_tune_ms : 0.0;
     return GPUQO_B200_OK;

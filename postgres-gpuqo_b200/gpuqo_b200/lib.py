@@ -167,7 +167,8 @@ def get_stats() -> Dict:
 
 
 class Tuning(C.Structure):
-    _fields_ = [("single_wide_sets", C.c_double), ("batch_single_sets", C.c_double), ("tune_ms", C.c_double),
+    _fields_ = [("single_narrow_level_sets", C.c_double), ("single_wide_level_sets", C.c_double),
+                ("batch_single_sets", C.c_double), ("tune_ms", C.c_double),
                 ("tuned", C.c_int)]
 
     def to_dict(self) -> Dict:

@@ -23,7 +23,7 @@ def test_autotune_installs_crossovers_without_changing_plans():
     before = _plans()
     t = lib.autotune()
     assert t["tuned"] == 1 and t["tune_ms"] > 0.0
-    for k in ("single_wide_sets", "batch_single_sets"):
+    for k in ("single_narrow_level_sets", "single_wide_level_sets", "batch_single_sets"):
         assert t[k] >= 0.0
     assert lib.get_tuning() == t
     after = _plans()
