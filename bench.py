@@ -323,6 +323,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (4096-query) section")
     ap.add_argument("--no-served", action="store_true", help="skip the served IDP2 section")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in kernel-variant crossovers (for runs under a profiler, which distorts "
+                         "the tuner's timings)")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
 
@@ -364,7 +367,8 @@ def main():
 
     from gpuqo_b200 import lib
     lib.load()
-    tuning = lib.autotune()   # kernel-variant and batch hand-off crossovers of this device (about a second)
+    # kernel-variant and batch hand-off crossovers of this device (about a second)
+    tuning = lib.get_tuning() if args.no_autotune else lib.autotune()
     qs = [query.snowflake(N_RELS, s) for s in rank_seeds(rank)]
 
     def barrier():
