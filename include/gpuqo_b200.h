@@ -316,6 +316,12 @@ typedef struct GpuqoB200Tuning {
 
 int gpuqo_b200_autotune(GpuqoB200Tuning *out);
 int gpuqo_b200_get_tuning(GpuqoB200Tuning *out);
+/* Installs the three crossovers of *in for the current device without
+ * measuring (for a process that restores the result of an earlier
+ * gpuqo_b200_autotune on the same kind of device, or pins a kernel variant
+ * for profiling); tune_ms is ignored, tuned is stored as given.  Negative or
+ * NaN crossovers: GPUQO_B200_ERR_ARGS. */
+int gpuqo_b200_set_tuning(const GpuqoB200Tuning *in);
 
 int gpuqo_b200_server_start(int max_inflight, int wave_memory_mb);
 int gpuqo_b200_server_submit(int gpuqo_algorithm, GpuqoPlannerInfoC *info, uint64_t *ticket);

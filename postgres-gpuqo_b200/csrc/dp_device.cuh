@@ -97,8 +97,8 @@ struct RelVal {
 constexpr uint32_t kWidthBits = 21;
 constexpr uint32_t kWidthMask = (1u << kWidthBits) - 1u;
 
-__device__ __forceinline__ RelVal load_rel(const float4 *memo, uint32_t s, uint32_t packed) {
-    float4 v = __ldcg(memo + s);
+// a memo entry already loaded (see load_rel)
+__device__ __forceinline__ RelVal unpack_rel(const float4 v, uint32_t packed) {
     RelVal r;
     r.rows = v.x;
     r.startup = v.y;
@@ -107,6 +107,10 @@ __device__ __forceinline__ RelVal load_rel(const float4 *memo, uint32_t s, uint3
     r.width = packed ? (int)(w & kWidthMask) : (int)w;
     r.hz = packed ? (w >> kWidthBits) : 0u;
     return r;
+}
+
+__device__ __forceinline__ RelVal load_rel(const float4 *memo, uint32_t s, uint32_t packed) {
+    return unpack_rel(__ldcg(memo + s), packed);
 }
 
 // :850-862

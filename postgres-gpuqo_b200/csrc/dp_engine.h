@@ -67,6 +67,9 @@ uint64_t engine_bytes_needed(int n);
 // current device.
 int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_narrow_level_sets,
                     double &single_wide_level_sets, double &batch_single_sets, std::string &err);
+// Installs crossovers measured earlier (or the defaults) for the current device.
+void engine_set_tuning(double single_narrow_level_sets, double single_wide_level_sets, double batch_single_sets,
+                       bool tuned);
 void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets,
                        bool &tuned);
 

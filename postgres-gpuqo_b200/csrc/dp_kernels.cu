@@ -669,7 +669,10 @@ __device__ __forceinline__ void edge_next(const uint32_t *adj, uint32_t S, EdgeI
     it.e++;
 }
 
-template <int G, bool MASKED>
+// PIPE: software-pipelined candidate loop for G < 32 (the persistent
+// kernel; the per-level kernel keeps the plain loop, which spills less at its
+// 64 registers)
+template <int G, bool MASKED, bool PIPE>
 __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first_set, uint32_t stride_sets,
                                             const uint32_t *sets, uint32_t count, int k, float4 *memo,
                                             uint32_t *memo_left, unsigned long long &pairs) {
@@ -712,10 +715,100 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         }
         LaneBest best;
         best.init();
-        for (uint32_t j = 0; j < per_lane; j++) {
-            const uint32_t c = (uint32_t)gl + j * G;
-            const bool active = has && c < P;
-            if (G == 32) {
+        const uint32_t *tab = reinterpret_cast<const uint32_t *>(d.h) + h.tree_tab;
+        const int n = h.n, nn = n * n;
+        // candidate c on edge (a, b): its two sides, its index in the
+        // reference's enumeration order and the classes on the edge
+        auto decode = [&](uint32_t c, uint32_t &L, uint32_t &R, uint32_t &p, uint32_t &ecm) {
+            const int rt = __ffs(S) - 1;
+            const uint32_t *anc_r = tab + 2 * nn + rt * n;
+            const int ch = ((anc_r[b] >> a) & 1u) ? b : a;        // child end w.r.t. root rt
+            const uint32_t comp_c = S & tab[rt * n + ch];
+            const uint32_t comp_a = (ch == a) ? comp_c : (S ^ comp_c);
+            const uint32_t side = c & 1u;
+            L = side ? (S ^ comp_a) : comp_a;                      // side 0: lb = {a}
+            R = S ^ L;
+            const uint32_t post = (uint32_t)(__popc(S & tab[nn + rt * n + ch]) - __popc(S & anc_r[ch]) +
+                                             __popc(comp_c) - 1);
+            p = h.index_order ? dpsub_index(L, S) : 2u * post + side;
+            ecm = 0u;
+            if (MASKED) {
+                const int ch0 = ((tab[2 * nn + b] >> a) & 1u) ? b : a;   // child end w.r.t. relation 0
+                ecm = h.edge_ec[ch0];
+            }
+        };
+        // costs one candidate from its two memo entries and keeps the lane's
+        // first strict minimum and first NaN in enumeration order
+        auto cost = [&](uint32_t L, uint32_t R, uint32_t p, uint32_t ecm, const float4 lv, const float4 rv) {
+            const RelVal l = unpack_rel(lv, h.hz_packed), r = unpack_rel(rv, h.hz_packed);
+            const RelVal out = join_eval_t<MASKED>(d, L, l, R, r, ecm);
+            const bool nan = isnan(out.total);
+            best.n_valid++;
+            if (p < best.first_p) {
+                best.first_p = p;
+                best.first_nan = nan;
+                if (nan) {
+                    best.nan_val = out;
+                    best.nan_left = L;
+                }
+            }
+            if (!nan) {
+                const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
+                if (key < best.key) {
+                    best.key = key;
+                    best.val = out;
+                    best.left = L;
+                }
+            }
+        };
+        if (G != 32 && !PIPE) {
+            for (uint32_t j = 0; j < per_lane; j++) {
+                const uint32_t c = (uint32_t)gl + j * G;
+                if (has && c < P) {
+                    while (it.e <= (c >> 1)) edge_next(h.adj, S, it, a, b);
+                    uint32_t L, R, p, ecm;
+                    decode(c, L, R, p, ecm);
+                    cost(L, R, p, ecm, __ldcg(memo + L), __ldcg(memo + R));
+                }
+            }
+        } else if (G != 32) {
+            // Software pipeline: a lane walks its candidates in order, and the
+            // next candidate is decoded and its two memo entries requested
+            // before the current one is costed, so that the loads are in
+            // flight during the cost model (measured: 2-3 % off 25-relation
+            // snowflakes and 22-relation stars, 1 % slower on 14-relation
+            // snowflakes and chains, whose lanes hold one or two candidates).
+            uint32_t cL = 0u, cR = 0u, cp = 0u, cecm = 0u;
+            float4 clv = make_float4(0.f, 0.f, 0.f, 0.f), crv = clv;
+            bool cact = false;
+            auto fetch = [&](uint32_t j, uint32_t &L, uint32_t &R, uint32_t &pp, uint32_t &ecm, float4 &lv,
+                             float4 &rv) -> bool {
+                const uint32_t c = (uint32_t)gl + j * G;
+                if (!(has && c < P)) return false;
+                while (it.e <= (c >> 1)) edge_next(h.adj, S, it, a, b);
+                decode(c, L, R, pp, ecm);
+                lv = __ldcg(memo + L);
+                rv = __ldcg(memo + R);
+                return true;
+            };
+            if (per_lane > 0) cact = fetch(0u, cL, cR, cp, cecm, clv, crv);
+            for (uint32_t j = 0; j < per_lane; j++) {
+                uint32_t nL = 0u, nR = 0u, np = 0u, necm = 0u;
+                float4 nlv = clv, nrv = crv;
+                const bool nact = (j + 1 < per_lane) ? fetch(j + 1, nL, nR, np, necm, nlv, nrv) : false;
+                if (cact) cost(cL, cR, cp, cecm, clv, crv);
+                cL = nL;
+                cR = nR;
+                cp = np;
+                cecm = necm;
+                clv = nlv;
+                crv = nrv;
+                cact = nact;
+            }
+        } else {
+            for (uint32_t j = 0; j < per_lane; j++) {
+                const uint32_t c = (uint32_t)gl + j * G;
+                const bool active = has && c < P;
                 // smallest lane t with scan_t > e (every lane takes part in the shuffles)
                 const uint32_t e = c >> 1;
                 int lo = 0;
@@ -728,49 +821,11 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
                 const uint32_t before = __shfl_sync(kFull, scan, t) - (uint32_t)__popc(__shfl_sync(kFull, fwd, t));
                 const uint32_t ft = __shfl_sync(kFull, fwd, t);
                 a = __shfl_sync(kFull, vt, t);
-                if (active) b = (int)__fns(ft, 0u, (int)(e - before) + 1);
-            } else if (active) {
-                const uint32_t target = c >> 1;
-                while (it.e <= target) edge_next(h.adj, S, it, a, b);
-            }
-            if (active) {
-                const uint32_t *tab = reinterpret_cast<const uint32_t *>(d.h) + h.tree_tab;
-                const int n = h.n, nn = n * n;
-                const int rt = __ffs(S) - 1;
-                const uint32_t *anc_r = tab + 2 * nn + rt * n;
-                const int ch = ((anc_r[b] >> a) & 1u) ? b : a;        // child end w.r.t. root rt
-                const uint32_t comp_c = S & tab[rt * n + ch];
-                const uint32_t comp_a = (ch == a) ? comp_c : (S ^ comp_c);
-                const uint32_t side = c & 1u;
-                const uint32_t L = side ? (S ^ comp_a) : comp_a;       // side 0: lb = {a}
-                const uint32_t R = S ^ L;
-                const uint32_t post = (uint32_t)(__popc(S & tab[nn + rt * n + ch]) - __popc(S & anc_r[ch]) +
-                                                 __popc(comp_c) - 1);
-                const uint32_t p = h.index_order ? dpsub_index(L, S) : 2u * post + side;
-                uint32_t ecm = 0u;
-                if (MASKED) {
-                    const int ch0 = ((tab[2 * nn + b] >> a) & 1u) ? b : a;   // child end w.r.t. relation 0
-                    ecm = h.edge_ec[ch0];
-                }
-                RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
-                RelVal out = join_eval_t<MASKED>(d, L, l, R, r, ecm);
-                const bool nan = isnan(out.total);
-                best.n_valid++;
-                if (p < best.first_p) {
-                    best.first_p = p;
-                    best.first_nan = nan;
-                    if (nan) {
-                        best.nan_val = out;
-                        best.nan_left = L;
-                    }
-                }
-                if (!nan) {
-                    const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
-                    if (key < best.key) {
-                        best.key = key;
-                        best.val = out;
-                        best.left = L;
-                    }
+                if (active) {
+                    b = (int)__fns(ft, 0u, (int)(e - before) + 1);
+                    uint32_t L, R, p, ecm;
+                    decode(c, L, R, p, ecm);
+                    cost(L, R, p, ecm, __ldcg(memo + L), __ldcg(memo + R));
                 }
             }
         }
@@ -823,10 +878,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_eval_tree(const uint32_t *__restr
     switch (G * 2 + (masked ? 1 : 0)) {
 #define GQB_T(g)                                                                                                 \
     case 2 * g:                                                                                                  \
-        tree_groups<g, false>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo, memo_left, pairs);   \
+        tree_groups<g, false, false>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo,               \
+                                     memo_left, pairs);                                                          \
         break;                                                                                                   \
     case 2 * g + 1:                                                                                              \
-        tree_groups<g, true>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo, memo_left, pairs);    \
+        tree_groups<g, true, false>(d, gwarp * (32 / g), nwarps * (32 / g), sets, count, k, memo,                \
+                                     memo_left, pairs);                                                          \
         break;
         GQB_T(2)
         GQB_T(8)
@@ -1075,6 +1132,10 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
     const bool masked = d.h->ec_masked != 0u;
     unsigned long long pairs = 0;
     unsigned epoch = 0;   // grid barriers passed (thread 0)
+    // the pipelined candidate loop needs the registers of the 2- and 3-blocks
+    // variants; at 64 registers it spills and the 4-blocks variant keeps the
+    // plain loop
+    constexpr bool kPipe = MINB < 4;
 
     // phase 0: base relations (gpuqo_cpu_sequential.cu:80-92) and level-2 sets
     if (blockIdx.x == 0 && threadIdx.x < n) {
@@ -1095,14 +1156,14 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
         while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
         G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
         if (G == 2) {
-            if (masked) tree_groups<2, true>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
-            else tree_groups<2, false>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
+            if (masked) tree_groups<2, true, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
+            else tree_groups<2, false, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
         } else if (G == 8) {
-            if (masked) tree_groups<8, true>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
-            else tree_groups<8, false>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
+            if (masked) tree_groups<8, true, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
+            else tree_groups<8, false, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
         } else {
-            if (masked) tree_groups<32, true>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
-            else tree_groups<32, false>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
+            if (masked) tree_groups<32, true, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
+            else tree_groups<32, false, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
         }
         if (!grid_barrier<true>(bar, epoch)) return;
     }
@@ -3333,6 +3394,19 @@ int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &sin
     tu.batch_single_sets = batch_single_sets;
     tu.tuned = true;
     return 0;
+}
+
+void engine_set_tuning(double single_narrow_level_sets, double single_wide_level_sets, double batch_single_sets,
+                       bool tuned) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaGetLastError();
+    Tuning &tu = g_tuning[dev];
+    tu.single_narrow_level_sets = single_narrow_level_sets;
+    tu.single_wide_level_sets = single_wide_level_sets;
+    tu.batch_single_sets = batch_single_sets;
+    tu.tuned = tuned;
 }
 
 void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets, bool &tuned) {

@@ -724,6 +724,15 @@ extern "C" int gpuqo_b200_autotune(GpuqoB200Tuning *out) {
     return gpuqo_b200_get_tuning(out);
 }
 
+extern "C" int gpuqo_b200_set_tuning(const GpuqoB200Tuning *in) {
+    if (!in) return GPUQO_B200_ERR_ARGS;
+    for (double v : {in->single_narrow_level_sets, in->single_wide_level_sets, in->batch_single_sets})
+        if (!(v >= 0.0)) return GPUQO_B200_ERR_ARGS;   // negative or NaN
+    engine_set_tuning(in->single_narrow_level_sets, in->single_wide_level_sets, in->batch_single_sets,
+                      in->tuned != 0);
+    return GPUQO_B200_OK;
+}
+
 extern "C" int gpuqo_b200_get_tuning(GpuqoB200Tuning *out) {
     if (!out) return GPUQO_B200_ERR_ARGS;
     bool tuned = false;

@@ -31,6 +31,10 @@ def main(argv=None):
     ap.add_argument("--idp", type=int, default=0, help="gpuqo_idp_n_iters (IDP2 when > 1)")
     ap.add_argument("--persistent", type=int, default=1, help="gpuqo_b200_persistent")
     ap.add_argument("--autotune", action="store_true", help="run gpuqo_b200_autotune first")
+    ap.add_argument("--tuning", default=None, metavar="NARROW,WIDE,HANDOFF",
+                    help="install these crossovers instead (gpuqo_b200_set_tuning): connected sets per level up to "
+                         "which the 2-blocks tree kernel runs, above which the 4-blocks one runs, and the batch "
+                         "hand-off in connected sets")
     a = ap.parse_args(argv)
 
     L = lib.load()
@@ -41,6 +45,9 @@ def main(argv=None):
     capi.set_int(L, "gpuqo_b200_persistent", a.persistent)
     if a.autotune:
         print("tuning:", lib.autotune(), flush=True)
+    if a.tuning:
+        lib.set_tuning(*[float(x) for x in a.tuning.split(",")])
+        print("tuning:", lib.get_tuning(), flush=True)
     if a.batch:
         qs = (query.batch_mix(a.batch, seed=a.seed, nmin=a.nmin, nmax=a.n) if a.mix else
               [query.make(a.shape, a.n, a.seed + i) for i in range(a.batch)])

@@ -186,6 +186,16 @@ def autotune() -> Dict:
     return t.to_dict()
 
 
+def set_tuning(single_narrow_level_sets: float, single_wide_level_sets: float, batch_single_sets: float,
+               tuned: int = 1) -> None:
+    """Install crossovers without measuring (gpuqo_b200_set_tuning)."""
+    lib = load()
+    t = Tuning(single_narrow_level_sets, single_wide_level_sets, batch_single_sets, 0.0, tuned)
+    rc = lib.gpuqo_b200_set_tuning(C.byref(t))
+    if rc:
+        raise ValueError(f"gpuqo_b200_set_tuning rejected {t.to_dict()}: {rc}")
+
+
 def get_tuning() -> Dict:
     lib = load()
     t = Tuning()

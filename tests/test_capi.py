@@ -2,6 +2,9 @@
 include/gpuqo_b200.h declares, and the ctypes mirror of the reference structs
 has the reference's layout.  No compute call is made (no GPU here)."""
 import ctypes as C
+import math
+
+import pytest
 
 from gpuqo_b200 import capi, lib
 
@@ -71,3 +74,21 @@ def test_tuning_defaults_before_autotune():
     assert t["single_narrow_level_sets"] == 10240.0
     assert t["single_wide_level_sets"] >= 1e29
     assert t["batch_single_sets"] == float(1 << 20)
+
+
+def test_set_tuning_installs_and_rejects():
+    """gpuqo_b200_set_tuning installs saved crossovers without measuring
+    (get_tuning reads them back), rejects negative and NaN ones, and restoring
+    the defaults with tuned = 0 gives back the untuned state."""
+    lib.set_tuning(5000.0, 80000.0, 123456.0)
+    t = lib.get_tuning()
+    assert (t["single_narrow_level_sets"], t["single_wide_level_sets"], t["batch_single_sets"], t["tuned"]) == \
+        (5000.0, 80000.0, 123456.0, 1)
+    for bad in ((-1.0, 1.0, 1.0), (1.0, math.nan, 1.0), (1.0, 1.0, -2.0)):
+        with pytest.raises(ValueError):
+            lib.set_tuning(*bad)
+    assert lib.get_tuning() == t
+    lib.set_tuning(10240.0, 1e30, float(1 << 20), tuned=0)
+    t = lib.get_tuning()
+    assert t["tuned"] == 0 and t["tune_ms"] == 0.0 and t["single_narrow_level_sets"] == 10240.0
+
