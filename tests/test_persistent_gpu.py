@@ -91,3 +91,34 @@ def test_time_resident_uses_persistent(warmup, iters):
     assert st["kernel_launches"] == 1
     assert st["eval_kernel_launches"] == iters
     assert same_tree(tree, want)
+
+
+# crossovers (connected sets per level) that pin one occupancy variant of the
+# persistent tree kernel: 2, 3 or 4 blocks per SM
+VARIANTS = {"2_blocks": (1e30, 1e30), "3_blocks": (0.0, 1e30), "4_blocks": (0.0, 0.0)}
+_LEVEL_PLANS = {}
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_each_variant_matches_level_launches(variant):
+    """Pinned with gpuqo_b200_set_tuning, each occupancy variant of the
+    persistent kernel (the 2- and 3-blocks ones with the software-pipelined
+    candidate loop, the 4-blocks one with the plain loop) returns the plan of
+    the per-level path on every tree, and the oracle's on the small ones."""
+    narrow, wide = VARIANTS[variant]
+    saved = lib.get_tuning()
+    lib.set_tuning(narrow, wide, saved["batch_single_sets"], tuned=saved["tuned"])
+    try:
+        for q in TREES:
+            if q.name not in _LEVEL_PLANS:
+                _LEVEL_PLANS[q.name] = _run(q, False).tree
+            a = _run(q, True)
+            assert a.stats["kernel_launches"] == 1
+            assert same_tree(a.tree, _LEVEL_PLANS[q.name]), q.name
+            if q.n <= 14:
+                want, _ = harness.run_port(q, 5)
+                assert same_tree(a.tree, want), q.name
+    finally:
+        lib.set_tuning(saved["single_narrow_level_sets"], saved["single_wide_level_sets"],
+                       saved["batch_single_sets"], tuned=saved["tuned"])
+
