@@ -228,10 +228,14 @@ HostInfo relabel(const HostInfo &from, const std::vector<int> &from_of_to) {
     const int nt = (int)from_of_to.size();
     std::vector<int> to_of_from(64, -1);
     for (int t = 0; t < nt; t++) to_of_from[from_of_to[t]] = t;
+    // bit f + 1 (relation f) -> bit to_of_from[f] + 1; bits of relations
+    // outside from_of_to (and bit 0) are dropped
     auto remap = [&](mask64 m) {
         mask64 o = 0;
-        for (int t = 0; t < nt; t++)
-            if (m & bit64(from_of_to[t] + 1)) o |= bit64(t + 1);
+        for (m &= ~1ull; m; m &= m - 1) {
+            const int t = to_of_from[__builtin_ctzll(m) - 1];
+            if (t >= 0) o |= bit64(t + 1);
+        }
         return o;
     };
     HostInfo to;
@@ -366,7 +370,8 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     h->enable_hashjoin = info.p.enable_hashjoin ? 1 : 0;
     h->composite_mask = 0;
     h->blob_words = (uint32_t)blob.size();
-    h->max_block = (uint32_t)max_block_size(info);
+    // every biconnected block of a tree is one edge
+    h->max_block = tree ? (uint32_t)std::min(n, 2) : (uint32_t)max_block_size(info);
     long long width_sum = 0;
     bool width_ok = true;
     for (int i = 0; i < n; i++) {
@@ -391,36 +396,44 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
         h->tree_tab = base_words;
         uint32_t *tab = blob.data() + base_words;
         const int nn = n * n;
+        uint32_t adj[32];
+        for (int v = 0; v < n; v++) adj[v] = h->adj[v];
         for (int r = 0; r < n; r++) {
+            // The kernels read the rows of root r only for sets whose lowest
+            // relation is r (and row 0 for the classes on edges): a relation
+            // without a higher-numbered neighbour is never the lowest of a
+            // connected set of two or more, and its rows stay zero.
+            if (r > 0 && (adj[r] >> r) <= 1u) continue;
             // preorder from r, children in increasing index order (pushed from
             // the highest index, so the lowest is visited first); n <= 32, so
             // fixed arrays
-            int parent[32], order[32], stack[32];
-            uint32_t anc[32];
+            uint32_t par_bit[32], anc[32], sub[32], before_of[32];
+            int order[32], stack[32];
             int sp = 0, no = 0;
-            for (int v = 0; v < n; v++) parent[v] = -1;
             anc[r] = 0u;
+            par_bit[r] = 0u;
             stack[sp++] = r;
             uint32_t before = 0u;
             while (sp > 0) {
                 const int u = stack[--sp];
-                tab[nn + r * n + u] = before;
+                before_of[u] = before;
                 before |= 1u << u;
                 order[no++] = u;
-                tab[2 * nn + r * n + u] = anc[u];
-                uint32_t kids = h->adj[u];
-                if (parent[u] >= 0) kids &= ~(1u << parent[u]);
+                uint32_t kids = adj[u] & ~par_bit[u];
+                const uint32_t anc_kid = anc[u] | (1u << u);
                 while (kids) {
                     const int c = 31 - __builtin_clz(kids);
                     kids &= ~(1u << c);
-                    parent[c] = u;
-                    anc[c] = anc[u] | (1u << u);
+                    par_bit[c] = 1u << u;
+                    anc[c] = anc_kid;
                     stack[sp++] = c;
                 }
             }
-            for (int v = 0; v < n; v++) tab[r * n + v] = 1u << v;
-            for (int i = no - 1; i >= 0; i--)
-                if (parent[order[i]] >= 0) tab[r * n + parent[order[i]]] |= tab[r * n + order[i]];
+            for (int v = 0; v < n; v++) sub[v] = 1u << v;
+            for (int i = no - 1; i > 0; i--) sub[__builtin_ctz(par_bit[order[i]])] |= sub[order[i]];
+            std::memcpy(tab + r * n, sub, (size_t)n * 4u);
+            std::memcpy(tab + nn + r * n, before_of, (size_t)n * 4u);
+            std::memcpy(tab + 2 * nn + r * n, anc, (size_t)n * 4u);
         }
         // classes on edges: every 2-member class must sit on an edge
         bool masked = n_ec <= 32;
