@@ -431,7 +431,30 @@ public:
             }
             tb.composite = (e.from.size() == 1) ? from.base[e.from.lowest_pos() - 1].composite : true;
         }
-        for (size_t i = 0; i < from.ec.size(); i++) {
+        // A class with members in two entries contains a listed relation, so
+        // a sub-problem (a few relations of a large query) visits only the
+        // classes of its relations, in increasing class order like the full
+        // scan; the classes it skips are the ones the full scan drops.
+        std::vector<int> cand;
+        size_t incident = 0;
+        for (const Entry &e : list)
+            e.from.for_each([&](int b) {
+                if (b - 1 < (int)from.rel_ecs.size()) incident += from.rel_ecs[b - 1].size();
+            });
+        const bool sparse = incident < from.ec.size();
+        if (sparse) {
+            cand.reserve(incident);
+            for (const Entry &e : list)
+                e.from.for_each([&](int b) {
+                    if (b - 1 < (int)from.rel_ecs.size())
+                        cand.insert(cand.end(), from.rel_ecs[b - 1].begin(), from.rel_ecs[b - 1].end());
+                });
+            std::sort(cand.begin(), cand.end());
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        }
+        const size_t n_visit = sparse ? cand.size() : from.ec.size();
+        for (size_t v = 0; v < n_visit; v++) {
+            const size_t i = sparse ? (size_t)cand[v] : v;
             if (ec_below_two_entries(from, (int)i)) continue;
             const BB &ecf = from.ec[i];
             BB ect = rel(ecf);
