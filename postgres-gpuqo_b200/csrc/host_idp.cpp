@@ -699,14 +699,34 @@ static QT *goo(const GInfo &g, Arena &A) {
         q->width = g.base[i].width;
         rels.emplace(q->id, GooNode{q, edges_of(q->id)});
     }
-    // are_valid_pair (gpuqo_filter.cuh:84-90): connected and disjoint
-    auto valid = [](const GooNode &a, const BB &bid) { return a.edges.intersects(bid) && !a.qt->id.intersects(bid); };
-    for (auto i = rels.begin(); i != rels.end(); ++i)
-        for (auto j = i; j != rels.end(); ++j)
-            if (valid(i->second, j->first)) {
+    // are_valid_pair (gpuqo_filter.cuh:84-90): connected and disjoint.  The
+    // reference tests every pair of entries in map order; the entries valid
+    // with `a` are those holding a relation of a's edges outside a, so they
+    // are found through owner[] (relation -> its entry) and visited in the
+    // same map order, which keeps the heap's push sequence and so its ties.
+    using It = std::map<BB, GooNode>::iterator;
+    std::vector<It> owner(g.n + 1, rels.end());
+    for (It it = rels.begin(); it != rels.end(); ++it)
+        it->first.for_each([&](int b) {
+            if (b <= g.n) owner[b] = it;
+        });
+    std::vector<It> cand;
+    auto valid_entries = [&](const GooNode &a) {
+        cand.clear();
+        (a.edges - a.qt->id).for_each([&](int b) {
+            if (b <= g.n && owner[b] != rels.end()) cand.push_back(owner[b]);
+        });
+        std::sort(cand.begin(), cand.end(), [](const It &x, const It &y) { return x->first < y->first; });
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    };
+    for (It i = rels.begin(); i != rels.end(); ++i) {
+        valid_entries(i->second);
+        for (const It &j : cand)
+            if (i->first < j->first) {
                 heap.push_back(join(*i->second.qt, *j->second.qt));
                 std::push_heap(heap.begin(), heap.end(), compare);
             }
+    }
     QT *smallest = nullptr;
     do {
         if (heap.empty()) return nullptr;   // disconnected query graph
@@ -719,15 +739,19 @@ static QT *goo(const GInfo &g, Arena &A) {
             smallest = nullptr;
             continue;
         }
+        // edges_of distributes over the union of the two entries
+        GooNode sn{smallest, lp->second.edges | rp->second.edges};
         rels.erase(lp);
         rels.erase(rp);
-        GooNode sn{smallest, edges_of(smallest->id)};
-        for (auto j = rels.begin(); j != rels.end(); ++j)
-            if (valid(sn, j->first)) {
-                heap.push_back(join(*smallest, *j->second.qt));
-                std::push_heap(heap.begin(), heap.end(), compare);
-            }
-        rels.emplace(smallest->id, sn);
+        valid_entries(sn);
+        for (const It &j : cand) {
+            heap.push_back(join(*smallest, *j->second.qt));
+            std::push_heap(heap.begin(), heap.end(), compare);
+        }
+        const It ins = rels.emplace(smallest->id, sn).first;
+        smallest->id.for_each([&](int b) {
+            if (b <= g.n) owner[b] = ins;
+        });
     } while (smallest == nullptr || smallest->id.size() < g.n);
     return smallest;
 }
