@@ -153,34 +153,64 @@ struct GBase {
     bool composite;
 };
 
+// Lists of ints stored back to back (offsets + one array): list i is
+// [data + off[i], data + off[i + 1]).  Indexing gives a view with begin/end/
+// size, so callers read it like a vector of vectors without one allocation
+// per list.
+struct IntLists {
+    std::vector<int> off{0}, data;
+    struct View {
+        const int *b, *e;
+        const int *begin() const { return b; }
+        const int *end() const { return e; }
+        size_t size() const { return (size_t)(e - b); }
+    };
+    View operator[](size_t i) const { return View{data.data() + off[i], data.data() + off[i + 1]}; }
+    size_t size() const { return off.size() - 1; }
+};
+
 struct GInfo {
     int n = 0;
     HostParams p;
     std::vector<GBase> base;
     std::vector<BB> edge;
     std::vector<BB> ec;                // relids
-    std::vector<std::vector<int>> ec_members;  // relation indices (bit - 1), increasing
+    IntLists ec_members;               // relation indices (bit - 1), increasing
     std::vector<float> sels;
     std::vector<BB> fks;
     std::vector<VarInfo> vars;
     std::vector<int> ec_off_sels, ec_off_fks;
-    std::vector<std::vector<int>> rel_ecs;     // per relation: classes containing it, increasing
+    IntLists rel_ecs;                  // per relation: classes containing it, increasing
     void index() {
-        ec_members.assign(ec.size(), {});
-        ec_off_sels.assign(ec.size(), 0);
-        ec_off_fks.assign(ec.size(), 0);
-        rel_ecs.assign(n, {});
+        const size_t n_ec = ec.size();
+        ec_off_sels.assign(n_ec, 0);
+        ec_off_fks.assign(n_ec, 0);
+        ec_members.off.assign(n_ec + 1, 0);
+        rel_ecs.off.assign((size_t)n + 1, 0);
+        // counts, then offsets, then the members in class order
         int os = 0, of = 0;
-        for (size_t i = 0; i < ec.size(); i++) {
-            ec.at(i).for_each([&](int b) {
-                ec_members[i].push_back(b - 1);
-                if (b - 1 < n) rel_ecs[b - 1].push_back((int)i);
+        for (size_t i = 0; i < n_ec; i++) {
+            int s = 0;
+            ec[i].for_each([&](int b) {
+                s++;
+                if (b >= 1 && b - 1 < n) rel_ecs.off[b]++;
             });
+            ec_members.off[i + 1] = ec_members.off[i] + s;
             ec_off_sels[i] = os;
             ec_off_fks[i] = of;
-            int s = (int)ec_members[i].size();
             os += s * (s - 1) / 2;
             of += s;
+        }
+        for (int r = 0; r < n; r++) rel_ecs.off[r + 1] += rel_ecs.off[r];
+        ec_members.data.resize((size_t)ec_members.off[n_ec]);
+        rel_ecs.data.resize((size_t)rel_ecs.off[n]);
+        std::vector<int> fill(rel_ecs.off.begin(), rel_ecs.off.end() - 1);
+        for (size_t i = 0; i < n_ec; i++) {
+            int k = ec_members.off[i];
+            ec[i].for_each([&](int b) {
+                ec_members.data[k++] = b - 1;
+                if (b >= 1 && b - 1 < n) rel_ecs.data[fill[b - 1]++] = (int)i;
+            });
         }
     }
 };
@@ -453,6 +483,13 @@ public:
             cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
         }
         const size_t n_visit = sparse ? cand.size() : from.ec.size();
+        if (!sparse) {
+            to.ec.reserve(from.ec.size());
+            to.sels.reserve(from.sels.size());
+            to.fks.reserve(from.fks.size());
+            to.vars.reserve(from.vars.size());
+        }
+        std::vector<int> to_bits;
         for (size_t v = 0; v < n_visit; v++) {
             const size_t i = sparse ? (size_t)cand[v] : v;
             if (ec_below_two_entries(from, (int)i)) continue;
@@ -464,7 +501,7 @@ public:
             to.sels.resize(sel_base + s_to * (s_to - 1) / 2, 0.0f);
             to.fks.resize(fk_base + s_to, BB());
             to.vars.resize(fk_base + s_to);
-            std::vector<int> to_bits;
+            to_bits.clear();
             ect.for_each([&](int b) { to_bits.push_back(b); });
             for (int lt = 0; lt < s_to; lt++) {
                 BB id_lt = BB::bit(to_bits[lt]);
