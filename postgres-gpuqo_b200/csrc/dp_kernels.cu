@@ -1382,7 +1382,7 @@ struct GraphKey {
 struct Tuning {
     // tree queries with up to this many connected sets per level run
     // k_dp_tree<2>, those with more than single_wide_level_sets k_dp_tree<4>
-    double single_narrow_level_sets = 10240.0;
+    double single_narrow_level_sets = 16384.0;
     double single_wide_level_sets = 1e30;
     double batch_single_sets = double(1u << 20);   // a batch hands larger tree queries to k_dp_tree
     bool tuned = false;

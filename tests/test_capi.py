@@ -66,12 +66,12 @@ def test_cancel_request_returns_null_before_any_device_work():
 
 def test_tuning_defaults_before_autotune():
     """Until gpuqo_b200_autotune runs, the built-in choices apply: the
-    2-blocks-per-SM tree kernel up to 10240 connected sets per relation and
+    2-blocks-per-SM tree kernel up to 16384 connected sets per relation and
     the 3-blocks-per-SM one above, batches hand tree queries of more than
     2^20 connected sets to single launches."""
     t = lib.get_tuning()
     assert t["tuned"] == 0 and t["tune_ms"] == 0.0
-    assert t["single_narrow_level_sets"] == 10240.0
+    assert t["single_narrow_level_sets"] == 16384.0
     assert t["single_wide_level_sets"] >= 1e29
     assert t["batch_single_sets"] == float(1 << 20)
 
@@ -88,7 +88,7 @@ def test_set_tuning_installs_and_rejects():
         with pytest.raises(ValueError):
             lib.set_tuning(*bad)
     assert lib.get_tuning() == t
-    lib.set_tuning(10240.0, 1e30, float(1 << 20), tuned=0)
+    lib.set_tuning(16384.0, 1e30, float(1 << 20), tuned=0)
     t = lib.get_tuning()
-    assert t["tuned"] == 0 and t["tune_ms"] == 0.0 and t["single_narrow_level_sets"] == 10240.0
+    assert t["tuned"] == 0 and t["tune_ms"] == 0.0 and t["single_narrow_level_sets"] == 16384.0
 
