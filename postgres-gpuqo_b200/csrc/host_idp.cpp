@@ -268,6 +268,24 @@ static float fkselc_of_ec(const GInfo &g, int e, const BB &outer, const BB &inne
 static float estimate_ec_selectivity(const GInfo &g, int e, const BB &l, const BB &r) {
     const BB &ecr = g.ec[e];
     int size = (int)g.ec_members[e].size();
+    if (size == 2) {
+        // Two members m0 < m1: with one on each side the steps below reduce
+        // to bit tests (the member's position in the class is 0 or 1, the FK
+        // match is the other member, ec_index(0, 1, 2) = 0).  A member on
+        // both sides takes the general path.
+        const int m[2] = {g.ec_members[e].begin()[0], g.ec_members[e].begin()[1]};
+        const int ml = (l.test(m[0] + 1) ? 1 : 0) | (l.test(m[1] + 1) ? 2 : 0);
+        const int mr = (r.test(m[0] + 1) ? 1 : 0) | (r.test(m[1] + 1) ? 2 : 0);
+        if (!(ml & mr)) {
+            if (!ml || !mr) return 1.0f;
+            const int ia = ml == 1 ? 0 : 1, ib = 1 - ia;   // positions of the l-side and r-side members
+            const int a = m[ia], b = m[ib];
+            const int off = g.ec_off_fks[e];
+            if (g.fks[off + ia].test(b + 1)) return (float)(1.0 / (double)std::fmax(1.0f, g.base[b].tuples));
+            if (g.fks[off + ib].test(a + 1)) return (float)(1.0 / (double)std::fmax(1.0f, g.base[a].tuples));
+            return g.sels[g.ec_off_sels[e]];
+        }
+    }
     BB ml = ecr & l, mr = ecr & r;
     if (ml.empty() || mr.empty()) return 1.0f;
     float fk = fkselc_of_ec(g, e, ml, mr);
@@ -285,7 +303,8 @@ static float estimate_ec_selectivity(const GInfo &g, int e, const BB &l, const B
 static float estimate_join_selectivity(const GInfo &g, const BB &l, const BB &r) {
     const BB &small = (l.size() <= r.size()) ? l : r;
     const BB &other = (&small == &l) ? r : l;
-    std::vector<int> hit;
+    thread_local std::vector<int> hit;   // reused: planners run on several threads
+    hit.clear();
     small.for_each([&](int b) {
         if (b - 1 >= g.n) return;
         for (int e : g.rel_ecs[b - 1])
