@@ -394,12 +394,16 @@ public:
     std::vector<Entry> list;
     std::vector<int> owner;     // relation index (bit - 1) -> entry position, -1 if none
     std::vector<int> of_to;     // target index -> entry position, -1 if none
-    Remap(const std::vector<Entry> &l, int n_from) : list(l), owner(n_from, -1) {
+    std::vector<char> single;   // entry position -> holds exactly one relation
+    Remap(const std::vector<Entry> &l, int n_from) : list(l), owner(n_from, -1), single(l.size(), 0) {
         int max_to = -1;
         for (size_t k = 0; k < list.size(); k++) {
+            int cnt = 0;
             list[k].from.for_each([&](int b) {
+                cnt++;
                 if (b - 1 < n_from) owner[b - 1] = (int)k;
             });
+            single[k] = cnt == 1;
             max_to = std::max(max_to, list[k].to);
         }
         of_to.assign(max_to + 1, -1);
@@ -512,9 +516,34 @@ public:
         for (size_t v = 0; v < n_visit; v++) {
             const size_t i = sparse ? (size_t)cand[v] : v;
             if (ec_below_two_entries(from, (int)i)) continue;
+            int s_from = (int)from.ec_members[i].size();
+            if (s_from == 2) {
+                // both members in single-relation entries (distinct, as the
+                // class is not below two entries): the new class has the two
+                // targets, member 0 the one with the lower target; the steps
+                // below then read sels[0] (ec_index(0, 1, 2) = 0) and each
+                // member's own FK mask and column
+                const int mm[2] = {from.ec_members[i].begin()[0], from.ec_members[i].begin()[1]};
+                const int k0 = owner[mm[0]], k1 = owner[mm[1]];
+                if (single[k0] && single[k1]) {
+                    BB ect;
+                    ect.set(list[k0].to + 1);
+                    ect.set(list[k1].to + 1);
+                    to.sels.push_back(from.sels[from.ec_off_sels[i]]);
+                    const int first = list[k0].to < list[k1].to ? 0 : 1;   // class position of new member 0
+                    for (int lt = 0; lt < 2; lt++) {
+                        const int lf = lt == 0 ? first : 1 - first;
+                        const int rel_f = mm[lf];
+                        to.fks.push_back(from.base[rel_f].composite ? BB()
+                                                                    : rel_nocomp(from.fks[from.ec_off_fks[i] + lf], from));
+                        to.vars.push_back(from.vars[from.ec_off_fks[i] + lf]);
+                    }
+                    to.ec.push_back(ect);
+                    continue;
+                }
+            }
             const BB &ecf = from.ec[i];
             BB ect = rel(ecf);
-            int s_from = (int)from.ec_members[i].size();
             int s_to = ect.size();
             size_t sel_base = to.sels.size(), fk_base = to.fks.size();
             to.sels.resize(sel_base + s_to * (s_to - 1) / 2, 0.0f);
