@@ -669,9 +669,9 @@ __device__ __forceinline__ void edge_next(const uint32_t *adj, uint32_t S, EdgeI
     it.e++;
 }
 
-// PIPE: software-pipelined candidate loop for G < 32 (the persistent
-// kernel; the per-level kernel keeps the plain loop, which spills less at its
-// 64 registers)
+// PIPE: software-pipelined candidate loop for G < 32, in the 2- and 3-blocks
+// persistent kernels; at 64 registers (the 4-blocks persistent kernel and the
+// per-level kernel) it spills, and those keep the plain loop
 template <int G, bool MASKED, bool PIPE>
 __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first_set, uint32_t stride_sets,
                                             const uint32_t *sets, uint32_t count, int k, float4 *memo,
@@ -775,9 +775,10 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
             // Software pipeline: a lane walks its candidates in order, and the
             // next candidate is decoded and its two memo entries requested
             // before the current one is costed, so that the loads are in
-            // flight during the cost model (measured: 2-3 % off 25-relation
-            // snowflakes and 22-relation stars, 1 % slower on 14-relation
-            // snowflakes and chains, whose lanes hold one or two candidates).
+            // flight during the cost model (measured on the 2- and 3-blocks
+            // variants: 2-3 % off 25-relation snowflakes and 22-relation
+            // stars, 1 % slower on 14-relation snowflakes and chains, whose
+            // lanes hold one or two candidates).
             uint32_t cL = 0u, cR = 0u, cp = 0u, cecm = 0u;
             float4 clv = make_float4(0.f, 0.f, 0.f, 0.f), crv = clv;
             bool cact = false;
