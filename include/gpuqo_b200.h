@@ -10,6 +10,8 @@
  * Struct layouts are the reference's, byte for byte, so a backend compiled
  * against src/include/optimizer/gpuqo_planner_info.h can call this library.
  * When those headers are already included, the declarations below are skipped.
+ * tests/test_abi_reference.py compiles this header and the reference's headers
+ * side by side and compares every size, offset and enum value.
  */
 #ifndef GPUQO_B200_H
 #define GPUQO_B200_H
@@ -63,13 +65,13 @@ typedef enum GpuqoIDPType {
     GPUQO_UNION
 } GpuqoIDPType;
 
-/* gpuqo_common.h:92-120 */
+/* gpuqo_common.h:91-113 */
 typedef struct PathCost { float startup; float total; } PathCost;
 typedef struct GpuqoIndexInfo { bool available; bool unique; float rows; PathCost cost; } GpuqoIndexInfo;
 typedef struct VarStats { float stadistinct; float stanullfrac; float mcvfreq; } VarStats;
 typedef struct VarInfo { VarStats stats; GpuqoIndexInfo index; } VarInfo;
 
-/* src/include/optimizer/gpuqo_planner_info.h:158-198 */
+/* src/include/optimizer/gpuqo_planner_info.h:17-55 */
 typedef Bitmapset *EdgeMask;
 typedef Bitmapset *RelationID;
 
@@ -117,8 +119,8 @@ typedef struct QueryTreeC {
 /* ---------------------------------------------------------------------- */
 
 /*
- * Replaces: extern "C" QueryTreeC *gpuqo_run(int, GpuqoPlannerInfoC*)
- *   src/include/optimizer/gpuqo.h:139, impl src/backend/optimizer/gpuqo/
+ * Replaces: extern QueryTreeC* gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC* info)
+ *   src/include/optimizer/gpuqo.h:23, impl src/backend/optimizer/gpuqo/
  *   gpuqo_main_internal.cu:177-185; caller gpuqo_main.c:584.
  *
  * gpuqo_algorithm: GPUQO_DPSUB runs the GPU DP - MPDP (biconnected-block
