@@ -19,7 +19,15 @@ Printed (rank 0, one JSON line):
            written) over its event-timed launch duration, against the
            measured HBM copy bandwidth;
   cpu_baseline - the reference's parallel_cpu_dpsub_bicc (its own code,
-           compiled from its sources into oracle/_ref) on the host cores;
+           compiled from its sources into oracle/_ref) on the host cores,
+           median of at least 5 runs after a warm-up, with the CPU model;
+  configs  - configurations 1 and 3: plain DPsub (gpuqo_dpsub_bicc off) on
+           the 12-relation stars, the 18-relation clique and the 30-relation
+           chain and cycle, device-resident ms/query and evaluated pairs/s,
+           each plan compared bit for bit with the reference's golden plan
+           (tests/golden/cases.jsonl); beside them the reference's dpe_dpsub
+           and cpu_dpsub on the stars (host cores), and the -march=native
+           build of the reference where this CPU can run it;
   batched - 4096 queries of the mixed workload (40% star, 40% snowflake, 10%
            chain, 10% cycle; relation counts uniform in [8,28], and [8,16])
            through gpuqo_b200_run_batch against gpuqo_run one query per call,
@@ -27,7 +35,8 @@ Printed (rank 0, one JSON line):
   served - IDP2 and UnionDP (k=25) snowflake queries of 30..1000 relations
            arriving as a Poisson stream at 1x and 4x the plain capacity into
            the continuous-batching service: queries/s, p50/p99 latency,
-           against one-at-a-time gpuqo_run (FIFO under the same arrivals).
+           against one-at-a-time gpuqo_run served first-in first-out under
+           the same arrivals (a worker thread, measured).
 
 --impl reference times that reference CPU engine alone (rank 0 only).
 """
@@ -156,26 +165,130 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_sample(queries, steps=None, budget_s=20.0):
-    """The reference's parallel_cpu_dpsub_bicc on the host cores (bounded)."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_reference_sample(queries, algorithm, steps=None, budget_s=20.0, min_runs=5, max_runs=40, native=False,
+                         threads=None):
+    """The reference's own CPU engine (oracle/_ref, or its -march=native
+    build) on the host cores: one warm-up, then at least min_runs timed calls
+    (steady clock around gpuqo_run) within about budget_s; returns the median
+    and mean ms per query, the threads used and the number of runs."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import harness
-    from gpuqo_b200 import capi
-    cores = os.cpu_count() or 1
-    harness.run_ref(queries[0], capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)  # warm-up
+    cores = threads or os.cpu_count() or 1
+    harness.run_ref(queries[0], algorithm, threads=cores, native=native)   # warm-up
     times = []
     t_start = time.perf_counter()
     i = 0
     while True:
         q = queries[i % len(queries)]
-        _, dt = harness.run_ref(q, capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)
+        _, dt = harness.run_ref(q, algorithm, threads=cores, native=native)
         times.append(dt * 1000.0)
         i += 1
-        if steps is not None and i >= steps:
+        if steps is not None:
+            if i >= steps:
+                break
+        elif i >= max_runs or (i >= min_runs and time.perf_counter() - t_start > budget_s):
             break
-        if steps is None and (time.perf_counter() - t_start > budget_s or i >= 40):
-            break
-    return statistics.mean(times), cores, len(times)
+    return statistics.median(times), statistics.mean(times), cores, len(times)
+
+
+GOLDEN = os.path.join(REPO, "tests", "golden", "cases.jsonl")
+
+
+def golden_cases(tag, algorithm):
+    """The committed golden queries of one tag with the reference's plans."""
+    from gpuqo_b200.query import Query
+    out = []
+    with open(GOLDEN) as f:
+        for line in f:
+            rec = json.loads(line)
+            if rec["tag"] == tag and rec["algorithm"] == algorithm:
+                rec["query"] = Query.from_dict(rec["query"])
+                out.append(rec)
+    return out
+
+
+def configs_section(cpu=True):
+    """Configurations 1 and 3 (plain DPsub): device-resident time of each
+    golden query (L2 flushed before every replay), evaluated pairs/s, and a
+    bit-for-bit comparison with the reference's golden plan; the reference's
+    CPU engines on the configuration-1 stars beside them."""
+    from gpuqo_b200 import capi, lib
+    res = {}
+    for tag, what in (("star12", "12-relation stars (configuration 1), seeds 0-9"),
+                      ("clique18", "18-relation clique (configuration 3)"),
+                      ("chain30", "30-relation chain (configuration 3)"),
+                      ("cycle30", "30-relation cycle (configuration 3)")):
+        cases = golden_cases(tag, capi.GPUQO_CPU_DPSUB)
+        if not cases:
+            continue
+        ms_all, pairs, csgs, same, launches = [], 0, 0, True, 0
+        for c in cases:
+            rc, ms, tree, st = lib.time_resident(c["query"], capi.GPUQO_DPSUB, bicc=False, warmup=2, iters=5,
+                                                 flush_l2=True)
+            if rc or tree is None:
+                raise RuntimeError(f"gpuqo_b200_time_resident failed on {c['name']}: {rc}")
+            ms_all.append(ms)
+            pairs += st["evaluated_pairs"]
+            csgs += st["connected_sets"]
+            launches = max(launches, st["kernel_launches"])
+            same = same and capi.same_plan(tree, c["expected"])
+        tot = sum(ms_all)
+        res[tag] = {"workload": what, "queries": len(cases), "ms_per_query": tot / len(cases),
+                    "evaluated_pairs_per_query": pairs / len(cases), "connected_sets_per_query": csgs / len(cases),
+                    "pairs_per_s": pairs / (tot / 1000.0) if tot > 0 else None,
+                    "kernel_launches_per_query": launches, "identical_plans_vs_reference": same}
+    if cpu and "star12" in res:
+        qs = [c["query"] for c in golden_cases("star12", capi.GPUQO_CPU_DPSUB)]
+        cores = os.cpu_count() or 1
+        base = {}
+        for name, alg, thr in (("dpe_dpsub", capi.GPUQO_DPE_DPSUB, cores),
+                               ("cpu_dpsub", capi.GPUQO_CPU_DPSUB, 1)):
+            med, mean, used, nr = cpu_reference_sample(qs, alg, budget_s=5.0, threads=thr)
+            base[name] = {"median_ms_per_query": med, "mean_ms_per_query": mean, "threads": used, "runs": nr}
+        ok, why = native_reference_usable()
+        if ok:
+            med, mean, used, nr = cpu_reference_sample(qs, capi.GPUQO_DPE_DPSUB, budget_s=5.0, native=True)
+            base["dpe_dpsub_march_native"] = {"median_ms_per_query": med, "mean_ms_per_query": mean,
+                                              "threads": used, "runs": nr}
+        else:
+            base["dpe_dpsub_march_native"] = {"skipped": why}
+        res["star12"]["reference_cpu"] = base
+        res["star12"]["reference_cpu_note"] = ("the reference's own engines (oracle/_ref) on the same stars: "
+                                               "dpe_dpsub with gpuqo_dpe_n_threads = all host threads and "
+                                               "gpuqo_dpe_pairs_per_depbuf 65536, cpu_dpsub on one thread")
+    return res
+
+
+def native_reference_usable():
+    """The -march=native build of the reference runs only on a CPU with every
+    ISA extension of the machine that built it."""
+    lib = os.path.join(REPO, "oracle", "_ref", "libgpuqo_ref_native.so")
+    isa = os.path.join(REPO, "oracle", "_ref", "libgpuqo_ref_native.isa")
+    if not (os.path.exists(lib) and os.path.exists(isa)):
+        return False, "not built"
+    need = set(open(isa).read().split())
+    have = set()
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                have = set(line.split(":", 1)[1].split())
+                break
+    except OSError:
+        return False, "no /proc/cpuinfo"
+    missing = sorted(need - have)
+    if missing:
+        return False, "this CPU lacks " + " ".join(missing[:6])
+    return True, ""
 
 
 def _prebuilt(qs):
@@ -247,8 +360,9 @@ def batched_section(seed=7):
 def served_section(n_req=48, seed=5):
     """Served IDP2 and UnionDP (k=25) over MPDP: Poisson arrivals of snowflake
     queries with relation counts log-uniform in [30,1000] into the
-    continuous-batching service, against one-at-a-time plain gpuqo_run (FIFO
-    under the same arrivals, latencies from its measured service times)."""
+    continuous-batching service, against one-at-a-time plain gpuqo_run run
+    by a first-in first-out worker thread under the same arrivals (both arms
+    measured with the wall clock from each request's arrival)."""
     import ctypes as C
     import math
     import threading
@@ -279,10 +393,24 @@ def served_section(n_req=48, seed=5):
         for mult in (1.0, 4.0):
             rate = plain_qps * mult
             arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
-            fin, lats = 0.0, []
-            for a, sv in zip(arr, svc):
-                fin = max(a, fin) + sv
-                lats.append(fin - a)
+            # plain arm, measured: one worker thread takes the requests in
+            # arrival order and runs gpuqo_run on each (one query per call)
+            lats, plain_same = [0.0] * n_req, [True]
+            t0 = time.perf_counter()
+
+            def fifo_worker():
+                for j in range(n_req):
+                    now = time.perf_counter() - t0
+                    if arr[j] > now:
+                        time.sleep(arr[j] - now)
+                    r = L.gpuqo_run(capi.GPUQO_DPSUB, builders[j].pointer())
+                    lats[j] = time.perf_counter() - t0 - arr[j]
+                    plain_same[0] = plain_same[0] and capi.same_plan(capi.tree_to_py(r), plain[j])
+                    L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
+            w = threading.Thread(target=fifo_worker)
+            w.start()
+            w.join()
+            fifo_makespan = time.perf_counter() - t0
             srv = lib.Server(max_inflight=32, wave_memory_mb=32768)
             res = [None] * n_req
 
@@ -309,7 +437,8 @@ def served_section(n_req=48, seed=5):
                 "served_p50_ms": float(np.percentile(lat, 50)), "served_p99_ms": float(np.percentile(lat, 99)),
                 "plain_fifo_p50_ms": 1e3 * float(np.percentile(lats, 50)),
                 "plain_fifo_p99_ms": 1e3 * float(np.percentile(lats, 99)),
-                "plain_fifo_qps": n_req / max(fin, arr[-1]),
+                "plain_fifo_qps": n_req / fifo_makespan,
+                "plain_fifo_same_plans": plain_same[0],
                 "identical_plans": all(x[0] == 0 and capi.same_plan(x[1], p) for x, p in zip(res, plain)),
                 "waves": st["waves"], "batched_subproblems": st["batched_subproblems"],
                 "device_ms": st["device_ms"], "busy_ms": st["busy_ms"], "starved_ms": st["starved_ms"]})
@@ -328,6 +457,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (4096-query) section")
     ap.add_argument("--no-served", action="store_true", help="skip the served IDP2 section")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the configuration 1 and 3 section (plain DPsub on star-12, clique-18, chain-30, cycle-30)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in kernel-variant crossovers (for runs under a profiler, which distorts "
                          "the tuner's timings)")
@@ -350,12 +481,14 @@ def main():
             _, dt = harness.run_ref(qs[i % len(qs)], capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, threads=cores)
             times.append(dt * 1000.0)
         v = statistics.mean(times)
+        med = statistics.median(times)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/query", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "seeds": SEEDS, "engine": "parallel_cpu_dpsub_bicc",
                            "chunk": 256},
                 "cpu_baseline": {"value": v, "unit": "ms/query", "cores": cores, "kind": "reference",
+                                 "median": med, "cpu_model": cpu_model(),
                                  "sample": f"{args.steps} snowflake-25 queries, gpuqo_dpe_n_threads={cores}"},
                 "e2e": {"value": v, "unit": "ms/query", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -470,11 +603,20 @@ def main():
             line["batched"] = batched_section()
         if world == 1 and not args.no_served:
             line["served"] = served_section()
+        if world == 1 and not args.no_configs:
+            line["configs"] = configs_section(cpu=not args.no_cpu_baseline)
         if world == 1 and not args.no_cpu_baseline:
-            cv, cores, ns = cpu_reference_sample(qs)
-            line["cpu_baseline"] = {"value": cv, "unit": "ms/query", "cores": cores, "kind": "reference",
-                                    "sample": f"{ns} snowflake-25 queries, parallel_cpu_dpsub_bicc, "
-                                              f"{cores} threads, chunk 256"}
+            med, mean, cores, ns = cpu_reference_sample(qs, capi.GPUQO_CPU_DPSUB_BICC_PARALLEL)
+            line["cpu_baseline"] = {"value": med, "unit": "ms/query", "cores": cores, "kind": "reference",
+                                    "mean": mean, "cpu_model": cpu_model(),
+                                    "sample": f"median of {ns} snowflake-25 MPDP queries after one warm-up, "
+                                              f"parallel_cpu_dpsub_bicc, {cores} threads, chunk 256"}
+            ok, why = native_reference_usable()
+            if ok:
+                med_n, mean_n, _, nn = cpu_reference_sample(qs, capi.GPUQO_CPU_DPSUB_BICC_PARALLEL, native=True)
+                line["cpu_baseline"]["march_native"] = {"value": med_n, "mean": mean_n, "runs": nn}
+            else:
+                line["cpu_baseline"]["march_native"] = {"skipped": why}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -202,6 +202,7 @@ typedef struct GpuqoB200Stats {
     uint32_t n_subproblems;       /* exact DP runs (1, or IDP iterations) */
     uint32_t kernel_launches;     /* kernels launched by the DP runs */
     uint32_t fallback_sets;       /* tree-mode sets re-evaluated in exact order (ties, NaN) */
+    uint32_t barrier_timeouts;    /* persistent launches whose grid barrier gave up (rerun per level) */
 } GpuqoB200Stats;
 void gpuqo_b200_get_stats(GpuqoB200Stats *out);
 
@@ -214,6 +215,25 @@ extern int gpuqo_b200_profile_kernels;
  * selects the per-level launches (also used automatically when a cooperative
  * launch is not possible or its barrier times out). */
 extern int gpuqo_b200_persistent;
+
+/* Every grid-barrier wait of the persistent kernels is bounded (4 s and 2^26
+ * polls).  When one gives up, the kernel raises an error flag, every block
+ * leaves, the host reruns that DP with per-level launches (same plan) and the
+ * device's engines keep using per-level launches until
+ * gpuqo_b200_reset_persistent() clears that state (it returns how many
+ * engines it cleared).  gpuqo_b200_barrier_poll_limit, when > 0, replaces the
+ * 2^26 polls: a small value makes waits run out on purpose, to exercise that
+ * path without a fault; 0 (default) keeps the built-in limits. */
+extern int gpuqo_b200_barrier_poll_limit;
+int gpuqo_b200_reset_persistent(void);
+
+/* Device-memory budget of the exact-DP arenas in MB (0, the default: no
+ * limit but the device's).  A DP whose dense memo, level lists or batch wave
+ * would need more is refused before anything is allocated: the call returns
+ * NULL (or the status) with GPUQO_B200_ERR_NOMEM and the library's state is
+ * unchanged, so later calls that fit succeed.  A failed cudaMalloc is
+ * reported the same way. */
+extern int gpuqo_b200_device_memory_mb;
 
 /*
  * Device-resident timing of the exact DP of one query (< 32 relations, no
@@ -247,8 +267,10 @@ typedef struct GpuqoB200PlanNode {
  * when elog(ERROR) longjmps out of a cancelled query, or a process whose
  * device memory is owned by another pool.  All scratch lives in one static
  * device array of about 6.7 MB that every GPU loading this library keeps
- * until exit; queries are limited to 18 relations (larger ones return
- * GPUQO_B200_ERR_TOO_LARGE with a message).  The caller passes the planner
+ * until exit; queries are limited to 18 relations and to a device planner
+ * info of 6144 32-bit words (about 270 two-member equivalence classes, more
+ * than the 153 edges of an 18-relation clique); larger ones return
+ * GPUQO_B200_ERR_TOO_LARGE with a message naming the limit.  The caller passes the planner
  * info (host, as for gpuqo_run), a CUDA stream (cudaStream_t, NULL for the
  * default stream) and an output array of at least 2*n_rels-1 nodes; the call
  * returns after the stream work completes.  The first call on each device
@@ -328,6 +350,11 @@ int gpuqo_b200_set_tuning(const GpuqoB200Tuning *in);
 int gpuqo_b200_server_start(int max_inflight, int wave_memory_mb);
 int gpuqo_b200_server_submit(int gpuqo_algorithm, GpuqoPlannerInfoC *info, uint64_t *ticket);
 int gpuqo_b200_server_wait(uint64_t ticket, QueryTreeC **out, double *latency_ms);
+/* Cancels one request: it stops before its next exact DP (IDP iterations
+ * included) and its wait returns GPUQO_B200_ERR_CANCELLED, unless it had
+ * already finished; the other requests are unaffected.  Unknown ticket:
+ * GPUQO_B200_ERR_ARGS.  (InterruptPending still cancels every request.) */
+int gpuqo_b200_server_cancel(uint64_t ticket);
 int gpuqo_b200_server_stats(GpuqoB200ServerStats *out);
 int gpuqo_b200_server_stop(void);
 

@@ -28,9 +28,12 @@ from gpuqo_b200 import capi  # noqa: E402
 from gpuqo_b200.query import Query  # noqa: E402
 
 REF_SO = os.path.join(HERE, "_ref", "libgpuqo_ref.so")
+# the same sources built for the build machine's CPU (-march=native): a
+# separately reported CPU-baseline flavour, never the parity oracle
+REF_NATIVE_SO = os.path.join(HERE, "_ref", "libgpuqo_ref_native.so")
 PORT_SO = os.path.join(HERE, "libgpuqo_oracle.so")
 
-_ref = None
+_ref = {}
 _port = None
 
 
@@ -38,13 +41,12 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
-def load_ref():
+def load_ref(native=False):
     """The reference library, with the GUC globals it needs initialised
     (they are zero in a bare process; gpuqo_cpu_dpe.cu:33-34 and
     gpuqo_cpu_dpsub_parallel.cu:30 read them)."""
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(REF_SO, mode=C.RTLD_LOCAL)
+    if native not in _ref:
+        lib = C.CDLL(REF_NATIVE_SO if native else REF_SO, mode=C.RTLD_LOCAL)
         capi.bind_gpuqo_run(lib)
         lib.ref_free_query_tree.argtypes = [C.c_void_p]
         lib.ref_free_query_tree.restype = None
@@ -54,8 +56,8 @@ def load_ref():
         capi.set_int(lib, "gpuqo_idp_n_iters", 0)
         capi.set_int(lib, "gpuqo_idp_type", capi.GPUQO_IDP2)
         capi.set_bool(lib, "gpuqo_spanning_tree_enable", False)
-        _ref = lib
-    return _ref
+        _ref[native] = lib
+    return _ref[native]
 
 
 def load_port():
@@ -90,9 +92,9 @@ def _restore(saved):
 
 
 def run_ref(q: Query, algorithm: int, idp_n_iters: int = 0,
-            idp_type: int = capi.GPUQO_IDP2, threads: int = 0, quiet=True):
+            idp_type: int = capi.GPUQO_IDP2, threads: int = 0, quiet=True, native=False):
     """Run the reference's gpuqo_run; returns (tree, seconds)."""
-    lib = load_ref()
+    lib = load_ref(native)
     capi.set_int(lib, "gpuqo_idp_n_iters", idp_n_iters)
     capi.set_int(lib, "gpuqo_idp_type", idp_type)
     if threads:

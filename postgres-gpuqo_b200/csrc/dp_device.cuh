@@ -406,6 +406,7 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
     // of L's relations and of R's relations intersected word by word
     // (rel_ecs), or every class when there are more than kMaxEcWords words.
     const int ecw = MASKED ? 1 : ec_words(n_ec);
+    const int ecs = ec_stride(n_ec);
     const bool by_mask = MASKED || ecw <= kMaxEcWords;
     uint32_t match[kMaxEcWords];
     if (MASKED) {
@@ -413,8 +414,8 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
     } else if (by_mask) {
         for (int w = 0; w < ecw; w++) {
             uint32_t cl = 0u, cr = 0u;
-            for (uint32_t x = L; x; x &= x - 1u) cl |= d.rel_ecs[lowest_idx(x) * ecw + w];
-            for (uint32_t x = R; x; x &= x - 1u) cr |= d.rel_ecs[lowest_idx(x) * ecw + w];
+            for (uint32_t x = L; x; x &= x - 1u) cl |= d.rel_ecs[lowest_idx(x) * ecs + w];
+            for (uint32_t x = R; x; x &= x - 1u) cr |= d.rel_ecs[lowest_idx(x) * ecs + w];
             match[w] = cl & cr;
         }
     }
@@ -507,6 +508,198 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
 __device__ __forceinline__ RelVal join_eval(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
                                             const RelVal &r) {
     return join_eval_t<false>(d, L, l, R, r, 0u);
+}
+
+// ---------------------------------------------------------------------------
+// Both orientations of one split in one pass.  Plain DPsub costs every split
+// (L, R) and its mirror (R, L); the classes with a member on each side are the
+// same for both, so they are found once (rel_ecs rows, 16-byte vector loads)
+// and visited once, while every quantity of each orientation is accumulated
+// with join_eval_t's operations in join_eval_t's class order, so each result
+// equals join_eval's bit for bit.  A two-member class takes its selectivity
+// for either orientation from DevInfoView::pair_sel (the value ec_selectivity
+// selects, precomputed on the host).
+// NW: 16-byte words per rel_ecs row (1: up to 128 classes, 2: up to 256).
+// ---------------------------------------------------------------------------
+struct SideTerms {
+    Htsz hz;
+    int nbuckets;
+    float sel, bucketsize, mcvfreq;
+    bool inner_unique, any_index;
+};
+
+__device__ __forceinline__ void side_init(const DevHeader &h, const RelVal &inner, SideTerms &t) {
+    if (inner.hz) {
+        t.hz.numbuckets = 1 << ((inner.hz >> 1) & 31u);
+        t.hz.numbatches = 1 << (inner.hz >> 6);
+    } else {
+        t.hz = exec_choose_hash_table_size(inner.rows, inner.width, h.work_mem);
+    }
+    t.nbuckets = f2i_x86((float)t.hz.numbuckets * (float)t.hz.numbatches);
+    t.sel = 1.0f;
+    t.bucketsize = 1.0f;
+    t.mcvfreq = 1.0f;
+    t.inner_unique = false;
+    t.any_index = false;
+}
+
+// one inner member's variable (first: the class's lowest inner member)
+__device__ __forceinline__ void side_var(SideTerms &t, const DevVar &v, bool first, bool inner_single) {
+    if (first && inner_single) {
+        if ((v.flags & 1u) && (v.flags & 2u)) t.inner_unique = true;
+        if (v.flags & 1u) t.any_index = true;
+    }
+    const float this_bs = bucketsize_one(v, t.nbuckets);
+    if (t.bucketsize > this_bs) t.bucketsize = this_bs;
+    if (t.mcvfreq > v.mcvfreq) t.mcvfreq = v.mcvfreq;
+}
+
+// general class of any size: the inner members of one orientation
+__device__ __forceinline__ void side_members(const DevInfoView &d, int off_fks, uint32_t ec, uint32_t mi,
+                                             bool inner_single, SideTerms &t) {
+    bool first = true;
+    for (uint32_t m = mi; m; m &= m - 1u) {
+        const uint32_t in_id = lowest(m);
+        side_var(t, d.vars[off_fks + popc((in_id - 1u) & ec)], first, inner_single);
+        first = false;
+    }
+}
+
+// rows, the cost functions and the index nested loops of one orientation
+// (outer O, inner I): the tail of join_eval_t
+template <int NW>
+__device__ __forceinline__ RelVal side_finish(const DevInfoView &d, uint32_t O, const RelVal &o, uint32_t I,
+                                              const RelVal &in, const SideTerms &t, int n_quals, float per_tuple,
+                                              const uint32_t (&match)[4 * NW]) {
+    const DevHeader &h = *d.h;
+    RelVal out;
+    const float rows = t.sel * o.rows * in.rows;
+    out.rows = rows > 1.0f ? roundf(rows) : 1.0f;
+    out.width = o.width + in.width;
+    Extra extra;
+    extra.inner_unique = t.inner_unique;
+    extra.indexed_join_quals = false;
+    extra.joinrows = out.rows;
+    extra.outer_match_frac = t.inner_unique ? out.rows / (o.rows * in.rows) : 0.0f;
+    extra.match_count = in.rows;
+    float min_s, min_t, s, c;
+    cost_nestloop(h, o, in.rows, in.startup, in.total, extra, per_tuple, min_s, min_t);
+    if (h.enable_hashjoin) {
+        cost_hashjoin(h, o, in, extra, n_quals, per_tuple, t.hz, t.bucketsize, t.mcvfreq, s, c);
+        if (c < min_t) { min_s = s; min_t = c; }
+    }
+    if (t.any_index && !((h.composite_mask >> lowest_idx(I)) & 1u)) {
+        extra.indexed_join_quals = true;
+#pragma unroll
+        for (int w = 0; w < 4 * NW; w++) {
+            for (uint32_t mm = match[w]; mm; mm &= mm - 1u) {
+                const int i = (w << 5) + __ffs(mm) - 1;
+                const uint32_t ec = d.ec_relids[i];
+                const int off_fks = (int)(d.ec_off[i] & 0xFFFFu);
+                const DevVar v = d.vars[off_fks + popc((lowest(ec & I) - 1u) & ec)];
+                if (!(v.flags & 1u)) continue;
+                cost_nestloop(h, o, v.idx_rows, v.idx_startup, v.idx_total, extra, per_tuple, s, c);
+                if (c < min_t) { min_s = s; min_t = c; }
+            }
+        }
+    }
+    out.startup = min_s;
+    out.total = min_t;
+    return out;
+}
+
+template <int NW>
+__device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
+                                                   const RelVal &r, RelVal &out_lr, RelVal &out_rl) {
+    const DevHeader &h = *d.h;
+    // classes with a member in L and one in R, 32 per word, in class order
+    uint32_t match[4 * NW];
+    {
+        uint32_t cl[4 * NW], cr[4 * NW];
+#pragma unroll
+        for (int w = 0; w < 4 * NW; w++) cl[w] = cr[w] = 0u;
+        for (uint32_t x = L; x; x &= x - 1u) {
+            const uint4 *row = reinterpret_cast<const uint4 *>(d.rel_ecs + lowest_idx(x) * (4 * NW));
+#pragma unroll
+            for (int j = 0; j < NW; j++) {
+                const uint4 a = row[j];
+                cl[4 * j] |= a.x;
+                cl[4 * j + 1] |= a.y;
+                cl[4 * j + 2] |= a.z;
+                cl[4 * j + 3] |= a.w;
+            }
+        }
+        for (uint32_t x = R; x; x &= x - 1u) {
+            const uint4 *row = reinterpret_cast<const uint4 *>(d.rel_ecs + lowest_idx(x) * (4 * NW));
+#pragma unroll
+            for (int j = 0; j < NW; j++) {
+                const uint4 a = row[j];
+                cr[4 * j] |= a.x;
+                cr[4 * j + 1] |= a.y;
+                cr[4 * j + 2] |= a.z;
+                cr[4 * j + 3] |= a.w;
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < 4 * NW; w++) match[w] = cl[w] & cr[w];
+    }
+    SideTerms lr, rl;   // (outer L, inner R) and (outer R, inner L)
+    side_init(h, r, lr);
+    side_init(h, l, rl);
+    const bool r_single = (R & (R - 1u)) == 0u, l_single = (L & (L - 1u)) == 0u;
+    int n_quals = 0;
+    float per_tuple = 0.0f;
+    // the words are visited in order through a shifting window, so that the
+    // match words stay in registers
+    uint32_t win[4 * NW];
+#pragma unroll
+    for (int w = 0; w < 4 * NW; w++) win[w] = match[w];
+#pragma unroll 1
+    for (int base = 0; base < 128 * NW; base += 32) {
+        for (uint32_t mm = win[0]; mm; mm &= mm - 1u) {
+            const int i = base + __ffs(mm) - 1;
+            const uint32_t ec = d.ec_relids[i];
+            const int off_fks = (int)(d.ec_off[i] & 0xFFFFu);
+            if (popc(ec) == 2) {
+                // one member on each side; lo_left: the lower member is in L
+                const bool lo_left = (lowest(ec) & L) != 0u;
+                const float2 ps = *reinterpret_cast<const float2 *>(d.pair_sel + 2 * i);
+                lr.sel *= lo_left ? ps.x : ps.y;
+                rl.sel *= lo_left ? ps.y : ps.x;
+                per_tuple += h.cpu_operator_cost;
+                n_quals++;
+                side_var(lr, d.vars[off_fks + (lo_left ? 1 : 0)], true, r_single);
+                side_var(rl, d.vars[off_fks + (lo_left ? 0 : 1)], true, l_single);
+            } else {
+                const uint32_t ml = ec & L, mr = ec & R;
+                lr.sel *= ec_selectivity(d, i, ec, ml, mr);
+                rl.sel *= ec_selectivity(d, i, ec, mr, ml);
+                per_tuple += h.cpu_operator_cost;
+                n_quals++;
+                side_members(d, off_fks, ec, mr, r_single, lr);
+                side_members(d, off_fks, ec, ml, l_single, rl);
+            }
+        }
+#pragma unroll
+        for (int w = 0; w + 1 < 4 * NW; w++) win[w] = win[w + 1];
+        win[4 * NW - 1] = 0u;
+    }
+    out_lr = side_finish<NW>(d, L, l, R, r, lr, n_quals, per_tuple, match);
+    out_rl = side_finish<NW>(d, R, r, L, l, rl, n_quals, per_tuple, match);
+}
+
+// (L, R) and (R, L); classes beyond 256 take two join_eval calls
+__device__ __forceinline__ void join_eval_mirror(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
+                                                 const RelVal &r, RelVal &out_lr, RelVal &out_rl) {
+    const int n_ec = d.h->n_ec;
+    if (n_ec <= 128) {
+        join_eval_mirror_w<1>(d, L, l, R, r, out_lr, out_rl);
+    } else if (n_ec <= 256) {
+        join_eval_mirror_w<2>(d, L, l, R, r, out_lr, out_rl);
+    } else {
+        out_lr = join_eval(d, L, l, R, r);
+        out_rl = join_eval(d, R, r, L, l);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -32,6 +32,7 @@ struct EngineStats {
     uint32_t eval_kernel_launches = 0;
     uint32_t kernel_launches = 0;
     uint32_t fallback_sets = 0;
+    uint32_t barrier_timeouts = 0;     // persistent launches whose grid barrier gave up (rerun per level)
 };
 
 // Runs one exact DP on the calling thread's current device.  `blob` is the
@@ -70,6 +71,10 @@ int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &sin
 // Installs crossovers measured earlier (or the defaults) for the current device.
 void engine_set_tuning(double single_narrow_level_sets, double single_wide_level_sets, double batch_single_sets,
                        bool tuned);
+// Clears the latch that a grid-barrier timeout sets on the current device's
+// engines (they then use per-level launches); returns how many were cleared.
+int engine_reset_persistent();
+
 void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets,
                        bool &tuned);
 

@@ -49,6 +49,8 @@
 #include "gpuqo_b200.h"
 
 extern "C" int gpuqo_b200_persistent;
+extern "C" int gpuqo_b200_barrier_poll_limit;
+extern "C" int gpuqo_b200_device_memory_mb;
 
 namespace gqb {
 
@@ -60,6 +62,11 @@ constexpr uint32_t kOvfLimit = 32u * 64u;
 // candidates per overflow chunk
 constexpr uint32_t kChunk = 32u * 64u;
 constexpr int kQueueWords = 64 * 3;    // per-warp CCC queue: 64 x (p, L, R)
+
+// units of chunked work of a set with P candidates: plain DPsub costs a split
+// and its mirror together (eval_range_dpsub), so its P candidates are P / 2
+// units; MPDP candidates are one unit each
+__host__ __device__ __forceinline__ uint32_t ovf_work(int mode, uint32_t P) { return mode == kModeDpsub ? P / 2u : P; }
 
 struct LevelCounters {
     uint32_t n_sets;                   // connected sets found by k_filter
@@ -292,29 +299,109 @@ struct LaneBest {
     }
 };
 
-__device__ __forceinline__ void evaluate_pair(const DevInfoView &d, const float4 *memo, uint32_t p, uint32_t L,
-                                              uint32_t R, LaneBest &b) {
-    RelVal l = load_rel(memo, L, d.h->hz_packed);
-    RelVal r = load_rel(memo, R, d.h->hz_packed);
-    RelVal out = join_eval(d, L, l, R, r);
-    bool nan = isnan(out.total);
-    b.n_valid++;
-    if (p < b.first_p) {
-        b.first_p = p;
-        b.first_nan = nan;
+// one valid candidate p = (outer L, inner side) with its cost: the lane keeps
+// its first strict minimum (key (ordered cost, p)) and its first candidate
+// in enumeration order with that candidate's NaN status
+__device__ __forceinline__ void best_update(LaneBest &best, uint32_t p, uint32_t L, const RelVal &out) {
+    const bool nan = isnan(out.total);
+    best.n_valid++;
+    if (p < best.first_p) {
+        best.first_p = p;
+        best.first_nan = nan;
         if (nan) {
-            b.nan_val = out;
-            b.nan_left = L;
+            best.nan_val = out;
+            best.nan_left = L;
         }
     }
     if (!nan) {
-        unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
-        if (key < b.key) {
-            b.key = key;
-            b.val = out;
-            b.left = L;
+        const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
+        if (key < best.key) {
+            best.key = key;
+            best.val = out;
+            best.left = L;
         }
     }
+}
+
+__device__ __forceinline__ void evaluate_pair(const DevInfoView &d, const float4 *memo, uint32_t p, uint32_t L,
+                                              uint32_t R, LaneBest &b) {
+    const RelVal l = load_rel(memo, L, d.h->hz_packed);
+    const RelVal r = load_rel(memo, R, d.h->hz_packed);
+    best_update(b, p, L, join_eval(d, L, l, R, r));
+}
+
+// A valid split (L, R) of a plain-DPsub set and its mirror (R, L), costed in
+// one pass (join_eval_mirror); p and pm are their indices in the reference's
+// enumeration order.
+__device__ __forceinline__ void evaluate_mirror(const DevInfoView &d, const float4 *memo, uint32_t p, uint32_t pm,
+                                                uint32_t L, uint32_t R, LaneBest &b) {
+    const RelVal l = load_rel(memo, L, d.h->hz_packed);
+    const RelVal r = load_rel(memo, R, d.h->hz_packed);
+    RelVal out_lr, out_rl;
+    join_eval_mirror(d, L, l, R, r, out_lr, out_rl);
+    best_update(b, p, L, out_lr);
+    best_update(b, pm, R, out_rl);
+}
+
+// Plain DPsub over mirror pairs: the reference visits L = pdep(p + 1, S) for
+// p = 0 .. P - 1 (P = 2^|S| - 2, gpuqo_cpu_dpsub.cu:32-78), and candidate
+// P - 1 - p is the complement of candidate p.  Lanes take contiguous slices
+// of [lo, hi) within [0, P / 2); each h names the split L = pdep(h + 1, S)
+// and its mirror, both connected or neither, costed together and keyed by
+// their own indices h and P - 1 - h.  With ccc the valid splits go through
+// the per-warp queue and are costed 32 at a time (the reference's CCC,
+// gpuqo_dpsub.cuh:193-259, as a compaction queue).
+__device__ __forceinline__ void eval_range_dpsub(const DevInfoView &d, const uint32_t *adj, uint32_t S, uint32_t P,
+                                                 uint32_t lo, uint32_t hi, const float4 *memo, uint32_t *q,
+                                                 bool ccc, LaneBest &best) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t span = hi - lo;
+    const uint32_t per = (span + 31u) / 32u;
+    uint32_t my_lo = lo + per * lane;
+    if (my_lo > hi) my_lo = hi;
+    const uint32_t my_hi = my_lo + per < hi ? my_lo + per : hi;
+    uint32_t h = my_lo;
+    uint32_t L = h < my_hi ? pdep32(h + 1u, S) : 0u;
+    int qn = 0;   // warp-uniform queue length
+    while (__any_sync(kFull, h < my_hi)) {
+        const bool has = h < my_hi;
+        bool valid = false;
+        uint32_t cl = 0, cr = 0;
+        if (has) {
+            cl = L;
+            cr = S ^ L;
+            valid = is_connected(cl, adj) && is_connected(cr, adj);
+            L = next_subset(L, S);
+        }
+        const uint32_t ch = h;
+        if (has) h++;
+        if (!ccc) {
+            if (valid) evaluate_mirror(d, memo, ch, P - 1u - ch, cl, cr, best);
+            continue;
+        }
+        const uint32_t m = __ballot_sync(kFull, valid);
+        if (valid) {
+            const int pos = qn + __popc(m & ((1u << lane) - 1u));
+            q[pos * 3 + 0] = ch;
+            q[pos * 3 + 1] = cl;
+            q[pos * 3 + 2] = cr;
+        }
+        qn += __popc(m);
+        __syncwarp();
+        if (qn >= 32) {
+            const int pos = qn - 32 + lane;
+            const uint32_t eh = q[pos * 3 + 0], el = q[pos * 3 + 1], er = q[pos * 3 + 2];
+            __syncwarp();
+            qn -= 32;
+            evaluate_mirror(d, memo, eh, P - 1u - eh, el, er, best);
+        }
+    }
+    if (ccc && qn > 0) {
+        __syncwarp();
+        if (lane < qn) evaluate_mirror(d, memo, q[lane * 3 + 0], P - 1u - q[lane * 3 + 0], q[lane * 3 + 1],
+                                       q[lane * 3 + 2], best);
+    }
+    __syncwarp();
 }
 
 // Enumerates candidate indices [lo, hi) of set S (lanes take contiguous
@@ -465,7 +552,7 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
                                                  const uint32_t *__restrict__ count_ptr = nullptr) {
     const uint32_t count = count_ptr ? *count_ptr : lc->n_sets;
     if (count == 0u) return;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     load_blob_to_smem(blob, blob_words, sm);
     const DevInfoView d = make_view(sm);
     const uint32_t *adj = d.h->adj;
@@ -486,7 +573,7 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
         }
         if (P > kOvfLimit) {
             if (lane == 0) {
-                uint32_t nch = (P + kChunk - 1u) / kChunk;
+                uint32_t nch = (ovf_work(MODE, P) + kChunk - 1u) / kChunk;
                 unsigned long long old = atomicAdd(&lc->ovf_packed, (1ull << 40) | (unsigned long long)nch);
                 uint32_t idx = (uint32_t)(old >> 40);
                 ovf_set[idx] = S;
@@ -499,7 +586,8 @@ __global__ void __launch_bounds__(kBlock) k_eval(const uint32_t *__restrict__ bl
         }
         LaneBest best;
         best.init();
-        eval_range<MODE>(d, adj, S, B, 0u, P, memo, q, ccc != 0, best);
+        if constexpr (MODE == kModeDpsub) eval_range_dpsub(d, adj, S, P, 0u, P / 2u, memo, q, ccc != 0, best);
+        else eval_range<MODE>(d, adj, S, B, 0u, P, memo, q, ccc != 0, best);
         unsigned long long mk, fk;
         WarpWinner w = warp_winner(best, mk, fk);
         if (w.is_writer) {
@@ -604,7 +692,7 @@ __global__ void __launch_bounds__(kBlock) k_eval_mpdp(const uint32_t *__restrict
                                                       unsigned long long *__restrict__ ovf_first,
                                                       GlobalCounters *__restrict__ glob, uint32_t target_lanes,
                                                       int max_group) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     load_blob_to_smem(blob, blob_words, sm);
     const DevInfoView d = make_view(sm);
     const uint32_t *adj = d.h->adj;
@@ -862,7 +950,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_eval_tree(const uint32_t *__restr
                                                       uint32_t *__restrict__ memo_left,
                                                       GlobalCounters *__restrict__ glob, uint32_t target_lanes,
                                                       int max_group) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     load_blob_to_smem(blob, blob_words, sm);
     const DevInfoView d = make_view(sm);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -911,6 +999,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_eval_tree(const uint32_t *__restr
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;   // 4 s of global time
 constexpr unsigned kBarrierSpinLimit = 1u << 26;                  // hard cap on polls as well (~30 s)
 
+// poll limit of one barrier wait: the launch argument when non-zero (the
+// gpuqo_b200_barrier_poll_limit setting, which makes waits run out on purpose
+// so that the timeout path can be exercised), else kBarrierSpinLimit
+__device__ __forceinline__ unsigned barrier_polls(unsigned poll_limit) {
+    return poll_limit != 0u ? poll_limit : kBarrierSpinLimit;
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -930,9 +1025,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // same SM.  The verdict is the same for every thread of the block (thread 0
 // decides); blocks may disagree only after a timeout, and then every later
 // barrier sees the error flag and returns false at once, so all blocks leave.
-// epoch: the caller's count of barriers passed (thread 0).
+// epoch: the caller's count of barriers passed (thread 0); max_polls: polls
+// before the wait gives up (barrier_polls).
 template <bool ACQUIRE_POLL>
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &epoch) {
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &epoch, unsigned max_polls) {
     __shared__ unsigned s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -953,7 +1049,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &epoch) {
                 if (!ACQUIRE_POLL) __threadfence();
                 break;
             }
-            if (++spins > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
+            if (++spins >= max_polls || global_ns() - t0 > kBarrierTimeoutNs) {
                 atomicExch(bar + 2, 1u);
                 break;
             }
@@ -1115,9 +1211,10 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
                                                        uint32_t *__restrict__ setsB, LevelCounters *__restrict__ lvl,
                                                        GlobalCounters *__restrict__ glob, TreeNode *__restrict__ tree,
                                                        int *__restrict__ tree_n, unsigned *__restrict__ bar,
-                                                       uint32_t target_lanes) {
-    extern __shared__ uint32_t sm[];
+                                                       uint32_t target_lanes, unsigned poll_limit) {
+    extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t bw = (blob_words + 3u) & ~3u;
+    const unsigned max_polls = barrier_polls(poll_limit);
     uint32_t *binom = sm + bw;
     uint32_t *stage = binom + 33 * 33 + 3;   // 16-byte aligned (bw, 1092 words)
     for (uint32_t i = threadIdx.x; i < blob_words; i += blockDim.x) sm[i] = blob[i];
@@ -1145,7 +1242,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
         memo_left[1u << i] = 0u;
     }
     if (n >= 2) level_sets_phase(adj, binom, st, n, 2, nullptr, (uint32_t)n, setsA, lvl + 2);
-    if (!grid_barrier<true>(bar, epoch)) return;
+    if (!grid_barrier<true>(bar, epoch, max_polls)) return;
     for (int k = 2; k <= n; k++) {
         uint32_t *cur = (k & 1) ? setsB : setsA;
         uint32_t *nxt = (k & 1) ? setsA : setsB;
@@ -1166,7 +1263,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
             if (masked) tree_groups<32, true, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
             else tree_groups<32, false, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
         }
-        if (!grid_barrier<true>(bar, epoch)) return;
+        if (!grid_barrier<true>(bar, epoch, max_polls)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t full = (n == 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
@@ -1192,7 +1289,7 @@ __global__ void __launch_bounds__(kBlock) k_ovf_chunks(const uint32_t *__restric
     const uint32_t n_ovf = (uint32_t)(packed >> 40);
     const uint32_t n_chunks = (uint32_t)(packed & 0xFFFFFFFFFFull);
     if (n_ovf == 0) return;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     load_blob_to_smem(blob, blob_words, sm);
     const DevInfoView d = make_view(sm);
     const uint32_t *adj = d.h->adj;
@@ -1219,11 +1316,13 @@ __global__ void __launch_bounds__(kBlock) k_ovf_chunks(const uint32_t *__restric
         const uint32_t P = ovf_P[idx];
         if (MODE == kModeMpdp && idx != cur_idx) find_blocks(S, adj, B);
         cur_idx = idx;
+        const uint32_t W = ovf_work(MODE, P);
         uint32_t lo = (c - ovf_off[idx]) * kChunk;
-        uint32_t hi = lo + kChunk < P ? lo + kChunk : P;
+        uint32_t hi = lo + kChunk < W ? lo + kChunk : W;
         LaneBest best;
         best.init();
-        eval_range<MODE>(d, adj, S, B, lo, hi, memo, q, ccc != 0, best);
+        if constexpr (MODE == kModeDpsub) eval_range_dpsub(d, adj, S, P, lo, hi, memo, q, ccc != 0, best);
+        else eval_range<MODE>(d, adj, S, B, lo, hi, memo, q, ccc != 0, best);
         unsigned long long mk, fk;
         warp_winner(best, mk, fk);
         if (lane == 0) {
@@ -1245,7 +1344,7 @@ __global__ void __launch_bounds__(kBlock) k_ovf_finalize(const uint32_t *__restr
                                                          const unsigned long long *__restrict__ ovf_first) {
     const uint32_t n_ovf = (uint32_t)(lc->ovf_packed >> 40);
     if (n_ovf == 0) return;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     load_blob_to_smem(blob, blob_words, sm);
     const DevInfoView d = make_view(sm);
     const uint32_t *adj = d.h->adj;
@@ -1359,14 +1458,31 @@ uint64_t engine_bytes_needed(int n) {
     return memo + lv + (1u << 20);
 }
 
+// a failed allocation is GPUQO_B200_ERR_NOMEM (it leaves no sticky error:
+// the next call may succeed), any other failure GPUQO_B200_ERR_CUDA
 #define CK(call)                                                                          \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
         if (e_ != cudaSuccess) {                                                          \
             err = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+            if (e_ == cudaErrorMemoryAllocation) {                                        \
+                cudaGetLastError();                                                       \
+                return GPUQO_B200_ERR_NOMEM;                                              \
+            }                                                                             \
             return GPUQO_B200_ERR_CUDA;                                                   \
         }                                                                                 \
     } while (0)
+
+// gpuqo_b200_device_memory_mb: when > 0, a DP whose arena would need more
+// device memory than this is refused with GPUQO_B200_ERR_NOMEM before any
+// allocation (the engines keep what they hold, so later calls are unaffected)
+static int over_budget(uint64_t bytes, const char *what, std::string &err) {
+    const int mb = gpuqo_b200_device_memory_mb;
+    if (mb <= 0 || bytes <= ((uint64_t)mb << 20)) return 0;
+    err = std::string(what) + " needs " + std::to_string(bytes >> 20) + " MB of device memory; " +
+          "gpuqo_b200_device_memory_mb allows " + std::to_string(mb);
+    return GPUQO_B200_ERR_NOMEM;
+}
 
 struct GraphKey {
     int n, mode, ccc, profile;
@@ -1428,6 +1544,7 @@ public:
     std::map<size_t, int> coop_blocks; // (dynamic shared bytes, variant) -> co-resident blocks of k_dp_tree (0: none)
     int force_minb = 0;                // autotuner: run this k_dp_tree variant (2, 3 or 4); 0 = by the tuning record
     bool coop_off = false;             // cooperative launch refused on this device
+    bool barrier_timed_out = false;    // a grid barrier of k_dp_tree gave up: per-level launches until reset
     std::map<GraphKey, int> graph_kernels;
     float *flush = nullptr;            // L2 flush buffer (timing only)
 
@@ -1479,6 +1596,7 @@ public:
             blob_cap_words = cap;
         }
         if (n <= cap_n) return 0;
+        if (int rc = over_budget(engine_bytes_needed(n), "the exact DP's dense memo and level lists", err)) return rc;
         drop_graphs();
         cudaFree(a.memo);
         cudaFree(a.memo_left);
@@ -1636,8 +1754,9 @@ public:
         // of 20- to 25-relation trees by about 8 %; a quarter or an eighth is
         // slower again)
         uint32_t target_lanes = (uint32_t)grid * (uint32_t)kBlock / 2u;
+        unsigned poll_limit = (unsigned)std::max(0, gpuqo_b200_barrier_poll_limit);
         void *args[] = {&a.blob, &bwords, &a.binom, &a.memo, &a.memo_left, &a.sets, &a.sets2,
-                        &a.lvl, &a.glob, &a.tree, &a.tree_n, &a.bar, &target_lanes};
+                        &a.lvl, &a.glob, &a.tree, &a.tree_n, &a.bar, &target_lanes, &poll_limit};
         cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, smem, stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -1650,11 +1769,17 @@ public:
     }
 
     // brings the control words back (one copy) and reports whether the last
-    // persistent run's grid barrier timed out
-    int barrier_failed(bool &failed, std::string &err) {
+    // persistent run's grid barrier timed out; a timeout latches the engine
+    // onto the per-level launches (gpuqo_b200_reset_persistent clears it), so
+    // later calls do not wait for another timeout first
+    int barrier_failed(bool &failed, EngineStats &st, std::string &err) {
         if (int rc = download(err)) return rc;
         CK(cudaStreamSynchronize(stream));
         failed = h_bar[2] != 0u;
+        if (failed) {
+            barrier_timed_out = true;
+            st.barrier_timeouts++;
+        }
         return 0;
     }
 
@@ -1757,7 +1882,8 @@ public:
 
     bool persistent_ok(const std::vector<uint32_t> &blob, DpMode mode) const {
         const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
-        return gpuqo_b200_persistent != 0 && !coop_off && mode == kModeMpdp && h->tree_mode != 0u;
+        return gpuqo_b200_persistent != 0 && !coop_off && !barrier_timed_out && mode == kModeMpdp &&
+               h->tree_mode != 0u;
     }
 
     // stage the blob without building a graph (persistent path)
@@ -1782,7 +1908,7 @@ public:
             CK(cudaEventRecord(ev1, stream));
             bool failed = true;
             if (launched) {
-                if (int rc = barrier_failed(failed, err)) return rc;
+                if (int rc = barrier_failed(failed, st, err)) return rc;
             }
             if (launched && !failed) {
                 if (int rc = finish(n, false, nodes, st, err, true)) return rc;
@@ -1825,7 +1951,7 @@ public:
                 bool launched = false, failed = false;
                 if (int rc = launch_persistent(n, pw, launched, err)) return rc;
                 if (launched)
-                    if (int rc = barrier_failed(failed, err)) return rc;
+                    if (int rc = barrier_failed(failed, st, err)) return rc;
                 usable = launched && !failed;
             }
             double total = 0.0;
@@ -1842,7 +1968,7 @@ public:
                 st.eval_kernel_ms += ms;
                 st.eval_kernel_launches += 1;
                 if (launched)
-                    if (int rc = barrier_failed(failed, err)) return rc;
+                    if (int rc = barrier_failed(failed, st, err)) return rc;
                 usable = launched && !failed;
             }
             if (usable && iters > 0) {
@@ -1980,11 +2106,15 @@ static inline int na_ecidx(int l, int r, int size) {
 
 // GpuqoPlannerInfoC -> BFS-relabelled device blob in a caller buffer (the
 // same relabelling as bfs_order/relabel/build_blob, in fixed-size storage).
+// On failure prints the cause and returns its status code.
 static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &words, int *from_of_to) {
     const int n = c->n_rels;
     uint64_t edge[kNoAllocMaxRels];
     for (int i = 0; i < n; i++) {
-        if (na_bms(c->base_rels[i].id) != (1ull << (i + 1))) return GPUQO_B200_ERR_ARGS;
+        if (na_bms(c->base_rels[i].id) != (1ull << (i + 1))) {
+            fprintf(stderr, "gpuqo_b200_run_noalloc: base relation %d does not carry relid bit %d\n", i, i + 1);
+            return GPUQO_B200_ERR_ARGS;
+        }
         edge[i] = na_bms(c->edge_table[i]);
     }
     // BFS order (gpuqo_bfs_indexing.cu:14-55)
@@ -2003,7 +2133,10 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         }
         seen |= edge[b];
     }
-    if (nt != n) return GPUQO_B200_ERR_ARGS;   // disconnected graph
+    if (nt != n) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: the query graph is disconnected\n");
+        return GPUQO_B200_ERR_ARGS;
+    }
     auto remap = [&](uint64_t m) {
         uint64_t o = 0;
         for (int t = 0; t < n; t++)
@@ -2017,9 +2150,13 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         n_sels += s * (s - 1) / 2;
         n_fks += s;
     }
-    if (n_sels >= 65536 || n_fks >= 65536) return GPUQO_B200_ERR_ARGS;
     words = blob_words_for(n, n_ec, n_sels, n_fks);
-    if (words > kNoAllocMaxBlobWords) return GPUQO_B200_ERR_ARGS;
+    if (n_sels >= 65536 || n_fks >= 65536 || words > kNoAllocMaxBlobWords) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: the planner info needs %u words (%d equivalence classes, %d "
+                        "selectivities, %d members); this entry point holds at most %u\n",
+                words, n_ec, n_sels, n_fks, kNoAllocMaxBlobWords);
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
     for (uint32_t i = 0; i < words; i++) blob[i] = 0u;
     DevHeader *h = reinterpret_cast<DevHeader *>(blob);
     h->n = n;
@@ -2090,6 +2227,7 @@ static int noalloc_blob(const GpuqoPlannerInfoC *c, uint32_t *blob, uint32_t &wo
         off_fks += s;
     }
     fill_rel_ecs(v, n);
+    fill_pair_sel(v);
     return 0;
 }
 
@@ -2133,11 +2271,10 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
     uint32_t blob[kNoAllocMaxBlobWords];
     uint32_t words = 0;
     int from_of_to[kNoAllocMaxRels];
-    if (int rc = noalloc_blob(info, blob, words, from_of_to)) {
-        fprintf(stderr, "gpuqo_b200_run_noalloc: planner info not supported (disconnected graph, relid layout "
-                        "or more than %u blob words)\n", kNoAllocMaxBlobWords);
-        return rc;
-    }
+    if (int rc = noalloc_blob(info, blob, words, from_of_to)) return rc;
+    // an error left pending by unrelated earlier work would otherwise be
+    // reported as this call's own
+    cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GPUQO_B200_ERR_CUDA;
     if (int rc = noalloc_setup(dev)) return rc;
@@ -2162,13 +2299,21 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
     const int ccc = gpuqo_dpsub_ccc_enable ? 1 : 0;
     const size_t smem = (size_t)(((words + 3u) & ~3u) + kWarpsPerBlock * kQueueWords) * 4u;
 
+    // every enqueue is checked where it is made, so a failure names its step
+    auto failed = [&](cudaError_t e, const char *what) {
+        if (e == cudaSuccess) return false;
+        fprintf(stderr, "gpuqo_b200_run_noalloc: %s: %s\n", what, cudaGetErrorString(e));
+        return true;
+    };
     // counters start at zero on every call; the memo needs no clearing (only
     // entries written earlier in the same call are read)
-    cudaMemcpyAsync(d_blob, blob, words * 4, cudaMemcpyHostToDevice, stream);
-    cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
-    cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
-    cudaMemsetAsync(tree_n, 0, sizeof(int), stream);
+    if (failed(cudaMemcpyAsync(d_blob, blob, words * 4, cudaMemcpyHostToDevice, stream), "planner info upload") ||
+        failed(cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream), "counter reset") ||
+        failed(cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream), "counter reset") ||
+        failed(cudaMemsetAsync(tree_n, 0, sizeof(int), stream), "counter reset"))
+        return GPUQO_B200_ERR_CUDA;
     k_init_base<<<1, 32, 0, stream>>>(d_blob, memo, memo_left);
+    if (failed(cudaGetLastError(), "base relations launch")) return GPUQO_B200_ERR_CUDA;
     for (int k = 2; k <= n; k++) {
         uint64_t total = binom64(n, k);
         uint64_t threads = std::min<uint64_t>((uint64_t)sm_count * 8 * kBlock, (total + 3) / 4);
@@ -2198,18 +2343,17 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
                                                                               ovf_set, ovf_key, ovf_first);
             }
         }
+        if (failed(cudaGetLastError(), "level launch")) return GPUQO_B200_ERR_CUDA;
     }
     k_extract<<<1, 32, 0, stream>>>(memo, memo_left, (1u << n) - 1u, d_blob, tree, tree_n);
+    if (failed(cudaGetLastError(), "plan extraction launch")) return GPUQO_B200_ERR_CUDA;
     TreeNode host_nodes[64];
     int host_n = 0;
-    cudaMemcpyAsync(host_nodes, tree, 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(&host_n, tree_n, sizeof(int), cudaMemcpyDeviceToHost, stream);
-    cudaError_t e = cudaStreamSynchronize(stream);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        fprintf(stderr, "gpuqo_b200_run_noalloc: %s\n", cudaGetErrorString(e));
+    if (failed(cudaMemcpyAsync(host_nodes, tree, 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream),
+               "plan download") ||
+        failed(cudaMemcpyAsync(&host_n, tree_n, sizeof(int), cudaMemcpyDeviceToHost, stream), "plan download") ||
+        failed(cudaStreamSynchronize(stream), "stream synchronisation"))
         return GPUQO_B200_ERR_CUDA;
-    }
     if (host_n != 2 * n - 1) {
         fprintf(stderr, "gpuqo_b200_run_noalloc: plan extraction produced %d nodes\n", host_n);
         return GPUQO_B200_ERR_CUDA;
@@ -2405,27 +2549,6 @@ __device__ __forceinline__ void tree_cand(const DevHeader &h, uint32_t S, int a,
     if (masked) {
         const int ch0 = ((__ldg(tab + 2 * nn + b) >> a) & 1u) ? b : a;
         ecm = h.edge_ec[ch0];
-    }
-}
-
-__device__ __forceinline__ void best_update(LaneBest &best, uint32_t p, uint32_t L, const RelVal &out) {
-    const bool nan = isnan(out.total);
-    best.n_valid++;
-    if (p < best.first_p) {
-        best.first_p = p;
-        best.first_nan = nan;
-        if (nan) {
-            best.nan_val = out;
-            best.nan_left = L;
-        }
-    }
-    if (!nan) {
-        const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
-        if (key < best.key) {
-            best.key = key;
-            best.val = out;
-            best.left = L;
-        }
     }
 }
 
@@ -2718,7 +2841,8 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
                                                    LevelCounters *__restrict__ lvl, GlobalCounters *__restrict__ glob,
                                                    TreeNode *__restrict__ tree, int *__restrict__ tree_n,
                                                    unsigned *__restrict__ bar, uint32_t target_lanes,
-                                                   BatchOvf ovf) {
+                                                   BatchOvf ovf, unsigned poll_limit) {
+    const unsigned max_polls = barrier_polls(poll_limit);
     __shared__ unsigned long long stage[kWarpsPerBlock][64];
     __shared__ uint32_t queues[kWarpsPerBlock][kQueueWords];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -2758,7 +2882,7 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
         }
         stage_flush64(st, cnt, listA, lvl + 2);
     }
-    if (!grid_barrier<false>(bar, epoch)) return;
+    if (!grid_barrier<false>(bar, epoch, max_polls)) return;
 
     for (int k = 2; k <= maxn; k++) {
         unsigned long long *cur = (k & 1) ? listB : listA;
@@ -2778,7 +2902,7 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
             batch_groups<8, TREE_ONLY>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
         else
             batch_groups<32, TREE_ONLY>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
-        if (!grid_barrier<false>(bar, epoch)) return;
+        if (!grid_barrier<false>(bar, epoch, max_polls)) return;
         if (TREE_ONLY) continue;   // tree sets have 2(k - 1) candidates: never an overflow
         // overflow sets of level k: the counter is final after the barrier, so
         // every block takes the same branch.  A list longer than its capacity
@@ -2786,9 +2910,9 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
         const uint32_t n_ovf = (uint32_t)(__ldcg(&lk->ovf_packed) >> 40);
         if (n_ovf != 0u && n_ovf <= ovf.cap) {
             batch_ovf_chunks(qs, blobs, lk, memo, ovf, queues[warp], pairs);
-            if (!grid_barrier<false>(bar, epoch)) return;
+            if (!grid_barrier<false>(bar, epoch, max_polls)) return;
             batch_ovf_finalize(qs, blobs, lk, memo, memo_left, ovf, tid, nthreads);
-            if (!grid_barrier<false>(bar, epoch)) return;
+            if (!grid_barrier<false>(bar, epoch, max_polls)) return;
         }
     }
 
@@ -2887,6 +3011,7 @@ struct BatchEngine {
     unsigned *bar = nullptr, *h_bar = nullptr;   // grid barrier words of kb_dp (device, pinned copy)
     int coop_grid = -1;                          // co-resident blocks of kb_dp<false> (0: no cooperative launch)
     int coop_grid_tree = -1;                     // co-resident blocks of kb_dp<true>
+    bool barrier_timed_out = false;              // a grid barrier of kb_dp gave up: per-level launches until reset
     BatchOvf ovf{};                              // overflow list of kb_dp
     uint64_t cap_ovf = 0;
     void *flush = nullptr;                       // L2 flush buffer (device-resident timing only)
@@ -2940,14 +3065,15 @@ struct BatchEngine {
     // is tree-shaped); false when it could not start
     bool enqueue_persistent(int nq, int maxn, uint64_t seen_words, bool tree_only) {
         const int grid = tree_only ? coop_grid_tree : coop_grid;
-        if (grid <= 0 || gpuqo_b200_persistent == 0) return false;
+        if (grid <= 0 || gpuqo_b200_persistent == 0 || barrier_timed_out) return false;
         cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
         cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
         if (!tree_only) cudaMemsetAsync(seen, 0, seen_words * 4, stream);
         cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), stream);
         uint32_t target_lanes = (uint32_t)grid * kBlock;
+        unsigned poll_limit = (unsigned)std::max(0, gpuqo_b200_barrier_poll_limit);
         void *args[] = {&qs, &nq, &maxn, &blobs, &memo, &memo_left, &seen, &listA, &listB,
-                        &lvl, &glob, &tree, &tree_n, &bar, &target_lanes, &ovf};
+                        &lvl, &glob, &tree, &tree_n, &bar, &target_lanes, &ovf, &poll_limit};
         const void *fn = tree_only ? (const void *)kb_dp<true> : (const void *)kb_dp<false>;
         if (cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, stream) != cudaSuccess) {
             cudaGetLastError();
@@ -2978,7 +3104,9 @@ struct BatchEngine {
         return 0;
     }
 
-    bool persistent_ready() const { return coop_grid > 0 && coop_grid_tree > 0 && gpuqo_b200_persistent != 0; }
+    bool persistent_ready() const {
+        return coop_grid > 0 && coop_grid_tree > 0 && gpuqo_b200_persistent != 0 && !barrier_timed_out;
+    }
 
     // One wave: all queries' memos fit.  wb: per query planner-info blob.
     // Queries that this wave could not finish (sets beyond the group limit
@@ -3045,6 +3173,9 @@ struct BatchEngine {
         }
         items = std::max(items, base);
         ovf_need = std::min(ovf_need, kBatchOvfCap);
+        if (int rc = over_budget(slots * (sizeof(float4) + 4) + words * 4 + seen_words * 4 + items * 16 + ovf_need * 32,
+                                 "the batch wave's arena", err))
+            return rc;
         uint64_t c1 = cap_slots, c2 = cap_slots, c3 = cap_words, c4 = cap_seen, c5 = cap_items, c6 = cap_items;
         if (int rc = grow(memo, c1, slots, err)) return rc;
         if (int rc = grow(memo_left, c2, slots, err)) return rc;
@@ -3093,6 +3224,8 @@ struct BatchEngine {
             CK(cudaGetLastError());
             if (h_bar[2] != 0u) {   // barrier timed out: rerun with per-level launches
                 persistent = false;
+                barrier_timed_out = true;   // and use them until gpuqo_b200_reset_persistent
+                st.barrier_timeouts++;
                 CK(cudaEventRecord(ev0, stream));
             }
         }
@@ -3249,6 +3382,7 @@ int engine_run(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, 
                 stats.memo_bytes = st.memo_bytes;
                 stats.device_ms += st.device_ms;
                 stats.kernel_launches += st.kernel_launches;
+                stats.barrier_timeouts += st.barrier_timeouts;
                 return 0;
             }
         }
@@ -3301,6 +3435,7 @@ int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, 
                     stats.memo_bytes = st.memo_bytes;
                     stats.kernel_launches += st.kernel_launches;
                 }
+                stats.barrier_timeouts += st.barrier_timeouts;
             }
             if (ok) {
                 ms_per_iter = total / iters;
@@ -3408,6 +3543,27 @@ void engine_set_tuning(double single_narrow_level_sets, double single_wide_level
     tu.single_wide_level_sets = single_wide_level_sets;
     tu.batch_single_sets = batch_single_sets;
     tu.tuned = tuned;
+}
+
+int engine_reset_persistent() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int cleared = 0;
+    auto e = g_engines.find(dev);
+    if (e != g_engines.end() && e->second && e->second->barrier_timed_out) {
+        e->second->barrier_timed_out = false;
+        cleared++;
+    }
+    auto b = g_batch.find(dev);
+    if (b != g_batch.end() && b->second && b->second->barrier_timed_out) {
+        b->second->barrier_timed_out = false;
+        cleared++;
+    }
+    return cleared;
 }
 
 void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets, bool &tuned) {

@@ -105,6 +105,10 @@ struct DevHeader {
     // gpuqo_row_estimation.cuh:49-88 returns a FK selectivity or the class's
     // stored selectivity, no arithmetic, so the host fills the table exactly
     float edge_sel[2][kMaxRels];
+    // every class has exactly two members (DevInfoView::pair_sel then holds
+    // the selectivity of every class in both orientations)
+    uint32_t all_pairs;
+    uint32_t pad_[3];
 };
 
 // Tree tables (tree_mode), appended after the class arrays: for every root r
@@ -124,10 +128,24 @@ struct DevInfoView {
     const float *sels;
     const uint32_t *fks;
     const DevVar *vars;
-    // rel_ecs[v * ecw + w]: bit b set when class 32 w + b has relation v as a
-    // member (ecw = (n_ec + 31) / 32 words per relation)
+    // rel_ecs[v * ec_stride(n_ec) + w]: bit b set when class 32 w + b has
+    // relation v as a member (ec_words(n_ec) words per relation, each row
+    // padded to a multiple of 4 words and 16-byte aligned for vector loads)
     const uint32_t *rel_ecs;
+    // pair_sel[2 i + o]: ec_selectivity of two-member class i (members x < y)
+    // with x on the outer side (o = 0) or y there (o = 1); NaN for classes of
+    // another size, which take the general path
+    const float *pair_sel;
 };
+
+GQB_HD inline int ec_words(int n_ec) { return (n_ec + 31) / 32; }
+GQB_HD inline int ec_stride(int n_ec) { return (ec_words(n_ec) + 3) & ~3; }
+
+// words from the blob start to the 16-byte aligned rel_ecs rows
+GQB_HD inline uint32_t rel_ecs_offset(int n_ec, int n_sels, int n_fks) {
+    const uint32_t w = (uint32_t)(sizeof(DevHeader) / 4 + 2 * n_ec + n_sels + n_fks + n_fks * (sizeof(DevVar) / 4));
+    return (w + 3u) & ~3u;
+}
 
 GQB_HD inline DevInfoView make_view(const void *blob) {
     DevInfoView v;
@@ -142,29 +160,62 @@ GQB_HD inline DevInfoView make_view(const void *blob) {
     v.fks = p;
     p += v.h->n_fks;
     v.vars = reinterpret_cast<const DevVar *>(p);
-    p += v.h->n_fks * (sizeof(DevVar) / 4);
-    v.rel_ecs = p;
+    v.rel_ecs = reinterpret_cast<const uint32_t *>(v.h) + rel_ecs_offset(v.h->n_ec, v.h->n_sels, v.h->n_fks);
+    v.pair_sel = reinterpret_cast<const float *>(v.rel_ecs + v.h->n * ec_stride(v.h->n_ec));
     return v;
 }
 
-GQB_HD inline int ec_words(int n_ec) { return (n_ec + 31) / 32; }
-
 GQB_HD inline uint32_t blob_words_for(int n, int n_ec, int n_sels, int n_fks) {
-    return (uint32_t)(sizeof(DevHeader) / 4 + 2 * n_ec + n_sels + n_fks + n_fks * (sizeof(DevVar) / 4) +
-                      n * ec_words(n_ec));
+    return rel_ecs_offset(n_ec, n_sels, n_fks) + (uint32_t)(n * ec_stride(n_ec) + 2 * n_ec);
 }
 
 // fills DevInfoView::rel_ecs from the class member masks (compact bits)
 GQB_HD inline void fill_rel_ecs(const DevInfoView &v, int n) {
     uint32_t *out = const_cast<uint32_t *>(v.rel_ecs);
-    const int ecw = ec_words(v.h->n_ec);
-    for (int i = 0; i < n * ecw; i++) out[i] = 0u;
+    const int ecs = ec_stride(v.h->n_ec);
+    for (int i = 0; i < n * ecs; i++) out[i] = 0u;
     for (int e = 0; e < v.h->n_ec; e++)
         for (uint32_t m = v.ec_relids[e]; m; m &= m - 1u) {
             int r = 0;
             while (!((m >> r) & 1u)) r++;
-            out[r * ecw + e / 32] |= 1u << (e % 32);
+            out[r * ecs + e / 32] |= 1u << (e % 32);
         }
+}
+
+// fills DevInfoView::pair_sel and DevHeader::all_pairs from the class arrays
+// and DevHeader::fksel (after those are written): ec_selectivity
+// (gpuqo_row_estimation.cuh:49-88) of a two-member class {x < y} is the FK
+// selectivity of the outer member's key into the inner one, else of the
+// inner member's key into the outer one, else the class's stored
+// selectivity; it selects a value and does no arithmetic, so the table holds
+// exactly what the per-pair evaluation would compute.
+GQB_HD inline void fill_pair_sel(const DevInfoView &v) {
+    DevHeader *h = const_cast<DevHeader *>(v.h);
+    float *ps = const_cast<float *>(v.pair_sel);
+    uint32_t all = 1u;
+    for (int i = 0; i < h->n_ec; i++) {
+        const uint32_t rr = v.ec_relids[i];
+        uint32_t m = rr;
+        int cnt = 0, x = -1, y = -1;
+        for (int r = 0; m; r++, m >>= 1)
+            if (m & 1u) {
+                if (cnt == 0) x = r;
+                y = r;
+                cnt++;
+            }
+        if (cnt != 2) {
+            all = 0u;
+            ps[2 * i] = ps[2 * i + 1] = __builtin_nanf("");
+            continue;
+        }
+        const int off_f = (int)(v.ec_off[i] & 0xFFFFu), off_s = (int)(v.ec_off[i] >> 16);
+        const bool fk_xy = (v.fks[off_f + 0] >> y) & 1u;   // member x's key matches y
+        const bool fk_yx = (v.fks[off_f + 1] >> x) & 1u;   // member y's key matches x
+        const float sel = v.sels[off_s];
+        ps[2 * i] = fk_xy ? h->fksel[y] : (fk_yx ? h->fksel[x] : sel);
+        ps[2 * i + 1] = fk_yx ? h->fksel[x] : (fk_xy ? h->fksel[y] : sel);
+    }
+    h->all_pairs = (h->n_ec > 0) ? all : 0u;
 }
 
 }  // namespace gqb

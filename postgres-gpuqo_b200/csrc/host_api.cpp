@@ -80,6 +80,8 @@ int gpuqo_dplin_threshold_idp = 100;
 int gpuqo_b200_profile_kernels = 0;
 int gpuqo_b200_batch_memory_mb = 32768;
 int gpuqo_b200_persistent = 1;
+int gpuqo_b200_barrier_poll_limit = 0;
+int gpuqo_b200_device_memory_mb = 0;
 }
 
 namespace gqb {
@@ -104,6 +106,7 @@ void stats_add(const EngineStats &s) {
     t_stats.eval_kernel_launches += s.eval_kernel_launches;
     t_stats.kernel_launches += s.kernel_launches;
     t_stats.fallback_sets += s.fallback_sets;
+    t_stats.barrier_timeouts += s.barrier_timeouts;
     t_stats.n_subproblems += 1;
 }
 
@@ -485,6 +488,7 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     }
     for (int i = 0; i < n_sels; i++) sels[i] = info.ec_sels[i];
     fill_rel_ecs(v, n);
+    fill_pair_sel(v);
     if (h->ec_masked) {
         // ec_selectivity (gpuqo_row_estimation.cuh:49-88) of each two-member
         // class in both orientations: the FK selectivity of the outer member's
@@ -618,6 +622,12 @@ QueryTreeC *run_one(int algorithm, GpuqoPlannerInfoC *info_c) {
         return NULL;
     }
     std::vector<int> order = bfs_order(info);
+    if ((int)order.size() != info.n) {
+        // the reference plans connected query graphs only (a join tree of a
+        // BFS order that misses relations would lose them)
+        set_error(GPUQO_B200_ERR_ARGS, "query graph is not connected");
+        return NULL;
+    }
     HostInfo remapped = relabel(info, order);
     std::vector<TreeNode> nodes;
     int rc = exact_dp(remapped, mode_for(algorithm), nodes, err);
@@ -667,6 +677,10 @@ extern "C" int gpuqo_b200_time_resident(int gpuqo_algorithm_arg, GpuqoPlannerInf
         return t_last_error;
     }
     std::vector<int> order = bfs_order(info);
+    if ((int)order.size() != info.n) {
+        set_error(GPUQO_B200_ERR_ARGS, "query graph is not connected");
+        return t_last_error;
+    }
     HostInfo remapped = relabel(info, order);
     std::vector<uint32_t> blob = build_blob(remapped);
     DpMode mode = mode_for(gpuqo_algorithm_arg);
@@ -736,6 +750,8 @@ extern "C" int gpuqo_b200_autotune(GpuqoB200Tuning *out) {
     g_tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return gpuqo_b200_get_tuning(out);
 }
+
+extern "C" int gpuqo_b200_reset_persistent(void) { return engine_reset_persistent(); }
 
 extern "C" int gpuqo_b200_set_tuning(const GpuqoB200Tuning *in) {
     if (!in) return GPUQO_B200_ERR_ARGS;

@@ -18,6 +18,7 @@
 // are identical.  The heaps and priority queues are the same libstdc++
 // algorithms fed in the same order, so their tie behaviour is the reference's.
 #include <algorithm>
+#include <atomic>
 #include <csignal>
 #include <array>
 #include <cmath>
@@ -699,6 +700,10 @@ struct Ctx {
     int err = 0;
     std::string msg;
     SubSolver solve;        // exact DP of one remapped sub-problem
+    std::atomic<bool> cancel{false};   // this request's own cancel (planner_cancel)
+
+    // InterruptPending (the backend's cancel) or this request's cancel
+    bool cancelled() const { return InterruptPending || cancel.load(std::memory_order_relaxed); }
 };
 
 static QT *nodes_to_qt(const std::vector<TreeNode> &nodes, int idx, Arena &A) {
@@ -722,7 +727,7 @@ static QT *solve_sub(const GInfo &info, const std::vector<Entry> &list, Ctx &C) 
     // a cancel request ends the IDP loop before its next DP; the drivers
     // unwind normally and the entry point returns NULL with
     // GPUQO_B200_ERR_CANCELLED (the caller's CHECK_FOR_INTERRUPTS then acts)
-    if (InterruptPending) {
+    if (C.cancelled()) {
         C.err = GPUQO_B200_ERR_CANCELLED;
         C.msg = "cancelled between IDP iterations";
         return nullptr;
@@ -1055,6 +1060,10 @@ struct Planner {
                 return GPUQO_B200_ERR_UNSUPPORTED;
             }
         } else if (g.n <= 31) {
+            if (C.cancelled()) {
+                C.msg = "cancelled before the exact DP";
+                return GPUQO_B200_ERR_CANCELLED;
+            }
             HostInfo h;
             if (int rc = to_host_info(rg, h, C.msg)) return rc;
             std::vector<TreeNode> nodes;
@@ -1083,6 +1092,10 @@ PlannerHandle *planner_new(int algorithm, const GpuqoPlannerInfoC *info_c, int i
     p->idp_n_iters = idp_n_iters;
     p->idp_type = idp_type;
     return reinterpret_cast<PlannerHandle *>(p);
+}
+
+void planner_cancel(PlannerHandle *h) {
+    reinterpret_cast<Planner *>(h)->C.cancel.store(true, std::memory_order_relaxed);
 }
 
 int planner_run(PlannerHandle *h, std::string &err) {

@@ -21,6 +21,9 @@ struct PlannerHandle;
 PlannerHandle *planner_new(int algorithm, const GpuqoPlannerInfoC *info, int idp_n_iters, int idp_type,
                            SubSolver solver, std::string &err);
 int planner_run(PlannerHandle *p, std::string &err);
+// Asks a planner to stop: it returns GPUQO_B200_ERR_CANCELLED before its next
+// exact DP (thread-safe; a planner that has finished keeps its result).
+void planner_cancel(PlannerHandle *p);
 QueryTreeC *planner_result(PlannerHandle *p);   // palloc'd, caller's numbering
 void planner_free(PlannerHandle *p);
 

@@ -226,6 +226,20 @@ public:
         return 0;
     }
 
+    // the request stops before its next exact DP (planner_cancel) and its
+    // wait returns GPUQO_B200_ERR_CANCELLED, unless it has already finished;
+    // the other requests, and the waves it shared with them, are unaffected
+    int cancel(uint64_t ticket, std::string &err) {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = reqs.find(ticket);
+        if (it == reqs.end()) {
+            err = "unknown ticket";
+            return GPUQO_B200_ERR_ARGS;
+        }
+        planner_cancel(it->second->planner);
+        return 0;
+    }
+
     int wait(uint64_t ticket, QueryTreeC **out, double *latency_ms, std::string &err) {
         Request *r;
         {
@@ -239,13 +253,20 @@ public:
             cv_req.wait(lk, [&] { return r->done; });
         }
         r->th.join();
-        int rc = r->rc;
-        if (out) *out = rc ? nullptr : planner_result(r->planner);
-        if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
-        if (rc) err = r->err;
-        planner_free(r->planner);
-        std::lock_guard<std::mutex> lk(mu);
-        reqs.erase(ticket);
+        // take the request out of the table before its planner is freed, so
+        // that a concurrent cancel finds no planner to touch
+        std::unique_ptr<Request> own;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            auto it = reqs.find(ticket);
+            own = std::move(it->second);
+            reqs.erase(it);
+        }
+        int rc = own->rc;
+        if (out) *out = rc ? nullptr : planner_result(own->planner);
+        if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(own->t_done - own->t_submit).count();
+        if (rc) err = own->err;
+        planner_free(own->planner);
         return rc;
     }
 
@@ -305,6 +326,14 @@ extern "C" int gpuqo_b200_server_wait(uint64_t ticket, QueryTreeC **out, double 
     if (!g_server) return GPUQO_B200_ERR_ARGS;
     std::string err;
     int rc = g_server->wait(ticket, out, latency_ms, err);
+    if (rc) set_error(rc, err);
+    return rc;
+}
+
+extern "C" int gpuqo_b200_server_cancel(uint64_t ticket) {
+    if (!g_server) return GPUQO_B200_ERR_ARGS;
+    std::string err;
+    int rc = g_server->cancel(ticket, err);
     if (rc) set_error(rc, err);
     return rc;
 }

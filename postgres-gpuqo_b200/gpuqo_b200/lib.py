@@ -26,7 +26,8 @@ class Stats(C.Structure):
                 ("filtered_subsets", C.c_uint64), ("memo_bytes", C.c_uint64),
                 ("device_ms", C.c_double), ("eval_kernel_ms", C.c_double),
                 ("eval_kernel_launches", C.c_uint32), ("n_subproblems", C.c_uint32),
-                ("kernel_launches", C.c_uint32), ("fallback_sets", C.c_uint32)]
+                ("kernel_launches", C.c_uint32), ("fallback_sets", C.c_uint32),
+                ("barrier_timeouts", C.c_uint32)]
 
     def to_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -67,6 +68,10 @@ def load():
         lib.gpuqo_b200_server_stats.restype = C.c_int
         lib.gpuqo_b200_server_stop.argtypes = []
         lib.gpuqo_b200_server_stop.restype = C.c_int
+        lib.gpuqo_b200_server_cancel.argtypes = [C.c_uint64]
+        lib.gpuqo_b200_server_cancel.restype = C.c_int
+        lib.gpuqo_b200_reset_persistent.argtypes = []
+        lib.gpuqo_b200_reset_persistent.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -248,6 +253,10 @@ class Server:
         if out:
             self.lib.gpuqo_b200_free_query_tree(C.cast(out, C.c_void_p))
         return rc, tree, lat.value
+
+    def cancel(self, ticket: int) -> int:
+        """Cancel one request (gpuqo_b200_server_cancel); returns the status."""
+        return self.lib.gpuqo_b200_server_cancel(ticket)
 
     def stats(self) -> Dict:
         st = ServerStats()

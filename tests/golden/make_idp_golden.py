@@ -7,8 +7,9 @@ gpuqo_run returned (oracle/_ref/libgpuqo_ref.so, built from the reference's
 sources by ``make -C oracle ref``).  The reference provides UnionDP only
 below 64 relations (gpuqo_dpdp_union.cu instantiates it for Bitmapset32/64).
 
-Usage: python tests/golden/make_idp_golden.py
+Usage: python tests/golden/make_idp_golden.py [--tags idp2_large --append]
 """
+import argparse
 import json
 import os
 import sys
@@ -35,6 +36,10 @@ def cases():
                    (query.snowflake(50, 14, rich=True), 12), (query.star(30, 15), 12), (query.chain(40, 16), 10),
                    (query.cycle(35, 17), 10), (query.random_graph(40, 18, extra_edge_p=0.05), 12)]:
         out.append(("union", q, k, UNION))
+    # the served workload's sizes (snowflakes of 30..1000 relations, k = 25):
+    # the reference runs them on its dynamic bitsets
+    for (q, k) in [(query.snowflake(300, 20), 25), (query.snowflake(1000, 21), 25)]:
+        out.append(("idp2_large", q, k, IDP2))
     return out
 
 
@@ -45,10 +50,17 @@ def tree_json(t):
 
 
 def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--tags", default="", help="comma-separated tags to generate (default: all)")
+    ap.add_argument("--append", action="store_true", help="append to the fixture file instead of rewriting it")
+    args = ap.parse_args()
+    tags = set(t for t in args.tags.split(",") if t)
     if not harness.ref_available():
         sys.exit("oracle/_ref/libgpuqo_ref.so missing: run `make -C oracle ref` first")
-    with open(os.path.join(HERE, "idp_cases.jsonl"), "w") as f:
+    with open(os.path.join(HERE, "idp_cases.jsonl"), "a" if args.append else "w") as f:
         for tag, q, k, typ in cases():
+            if tags and tag not in tags:
+                continue
             t0 = time.time()
             tree, _ = harness.run_ref(q, 5, idp_n_iters=k, idp_type=typ)
             rec = {"tag": tag, "name": q.name, "algorithm": 5, "idp_n_iters": k, "idp_type": typ,

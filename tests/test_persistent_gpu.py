@@ -5,6 +5,8 @@ gpuqo_b200_persistent selects the path (default 1).  Both paths must return
 bit-identical plans; the persistent one must report a single kernel launch,
 and queries that are not tree-shaped must keep the per-level path.
 """
+import ctypes as C
+
 import pytest
 
 from conftest import same_tree
@@ -122,3 +124,56 @@ def test_each_variant_matches_level_launches(variant):
         lib.set_tuning(saved["single_narrow_level_sets"], saved["single_wide_level_sets"],
                        saved["batch_single_sets"], tuned=saved["tuned"])
 
+
+
+def _reset_latch():
+    L = lib.load()
+    L.gpuqo_b200_reset_persistent.restype = C.c_int
+    return L.gpuqo_b200_reset_persistent()
+
+
+def test_barrier_timeout_reruns_per_level_and_latches():
+    """A grid-barrier wait that runs out (gpuqo_b200_barrier_poll_limit = 1:
+    a block gives up after one poll unless every block has already arrived)
+    raises the kernel's error flag; the host reruns the DP with per-level
+    launches, returns the per-level plan, and keeps the engine on per-level
+    launches until gpuqo_b200_reset_persistent()."""
+    L = lib.load()
+    q = query.snowflake(20, 3)
+    want = _run(q, False).tree
+    assert same_tree(want, harness.run_port(q, 5)[0])
+    try:
+        capi.set_int(L, "gpuqo_b200_barrier_poll_limit", 1)
+        first = _run(q, True)
+        assert first.stats["barrier_timeouts"] == 1
+        assert same_tree(first.tree, want)
+        # latched: no second persistent attempt, per-level launches straight away
+        again = _run(q, True)
+        assert again.stats["barrier_timeouts"] == 0
+        assert again.stats["kernel_launches"] > 1
+        assert same_tree(again.tree, want)
+    finally:
+        capi.set_int(L, "gpuqo_b200_barrier_poll_limit", 0)
+    assert _reset_latch() >= 1
+    back = _run(q, True)
+    assert back.stats["kernel_launches"] == 1 and back.stats["barrier_timeouts"] == 0
+    assert same_tree(back.tree, want)
+
+
+def test_batch_wave_barrier_timeout_reruns_per_level():
+    """The same for a batch wave (kb_dp): the timed-out wave is rerun with
+    per-level launches and every plan equals gpuqo_run's."""
+    L = lib.load()
+    qs = [query.snowflake(n, 800 + n) for n in (8, 10, 12, 14)] + [query.cycle(n, 850 + n) for n in (7, 11)]
+    want = [_run(q, False).tree for q in qs]
+    try:
+        capi.set_int(L, "gpuqo_b200_barrier_poll_limit", 1)
+        trees, rc = lib.run_batch(qs, capi.GPUQO_DPSUB, bicc=True)
+        assert rc == 0 and lib.get_stats()["barrier_timeouts"] >= 1
+        assert all(same_tree(a, b) for a, b in zip(trees, want))
+    finally:
+        capi.set_int(L, "gpuqo_b200_barrier_poll_limit", 0)
+    _reset_latch()
+    trees, rc = lib.run_batch(qs, capi.GPUQO_DPSUB, bicc=True)
+    assert rc == 0 and lib.get_stats()["barrier_timeouts"] == 0
+    assert all(same_tree(a, b) for a, b in zip(trees, want))
