@@ -92,11 +92,13 @@ def _restore(saved):
 
 
 def run_ref(q: Query, algorithm: int, idp_n_iters: int = 0,
-            idp_type: int = capi.GPUQO_IDP2, threads: int = 0, quiet=True, native=False):
-    """Run the reference's gpuqo_run; returns (tree, seconds)."""
+            idp_type: int = capi.GPUQO_IDP2, threads: int = 0, quiet=True, native=False, spanning=False):
+    """Run the reference's gpuqo_run; returns (tree, seconds).  spanning sets
+    gpuqo_spanning_tree_enable for the call."""
     lib = load_ref(native)
     capi.set_int(lib, "gpuqo_idp_n_iters", idp_n_iters)
     capi.set_int(lib, "gpuqo_idp_type", idp_type)
+    capi.set_bool(lib, "gpuqo_spanning_tree_enable", spanning)
     if threads:
         capi.set_int(lib, "gpuqo_dpe_n_threads", threads)
     b = capi.PlannerInfoBuilder(q)

@@ -608,13 +608,20 @@ __device__ __forceinline__ RelVal side_finish(const DevInfoView &d, uint32_t O, 
     return out;
 }
 
-template <int NW>
+// MASKED (tree-shaped query graph, DevHeader::ec_masked): every class is a
+// two-member class on an edge, and the classes of the split edge are ec_mask
+template <int NW, bool MASKED>
 __device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
-                                                   const RelVal &r, RelVal &out_lr, RelVal &out_rl) {
+                                                   const RelVal &r, uint32_t ec_mask, RelVal &out_lr,
+                                                   RelVal &out_rl) {
     const DevHeader &h = *d.h;
     // classes with a member in L and one in R, 32 per word, in class order
     uint32_t match[4 * NW];
-    {
+    if (MASKED) {
+        match[0] = ec_mask;
+#pragma unroll
+        for (int w = 1; w < 4 * NW; w++) match[w] = 0u;
+    } else {
         uint32_t cl[4 * NW], cr[4 * NW];
 #pragma unroll
         for (int w = 0; w < 4 * NW; w++) cl[w] = cr[w] = 0u;
@@ -655,12 +662,12 @@ __device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_
 #pragma unroll
     for (int w = 0; w < 4 * NW; w++) win[w] = match[w];
 #pragma unroll 1
-    for (int base = 0; base < 128 * NW; base += 32) {
+    for (int base = 0; base < (MASKED ? 32 : 128 * NW); base += 32) {
         for (uint32_t mm = win[0]; mm; mm &= mm - 1u) {
             const int i = base + __ffs(mm) - 1;
             const uint32_t ec = d.ec_relids[i];
             const int off_fks = (int)(d.ec_off[i] & 0xFFFFu);
-            if (popc(ec) == 2) {
+            if (MASKED || popc(ec) == 2) {
                 // one member on each side; lo_left: the lower member is in L
                 const bool lo_left = (lowest(ec) & L) != 0u;
                 const float2 ps = *reinterpret_cast<const float2 *>(d.pair_sel + 2 * i);
@@ -688,14 +695,30 @@ __device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_
     out_rl = side_finish<NW>(d, R, r, L, l, rl, n_quals, per_tuple, match);
 }
 
+// (L, R) and (R, L) of a split edge of a tree-shaped query graph (the tree
+// kernels' edge decode): MASKED reads only the edge's classes (ec_mask)
+template <bool MASKED>
+__device__ __forceinline__ void join_eval_mirror_tree(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
+                                                      const RelVal &r, uint32_t ec_mask, RelVal &out_lr,
+                                                      RelVal &out_rl) {
+    if (MASKED) {
+        join_eval_mirror_w<1, true>(d, L, l, R, r, ec_mask, out_lr, out_rl);
+    } else {
+        // classes off the tree's edges: one orientation after the other (the
+        // fused general pass needs more registers than the tree kernels have)
+        out_lr = join_eval(d, L, l, R, r);
+        out_rl = join_eval(d, R, r, L, l);
+    }
+}
+
 // (L, R) and (R, L); classes beyond 256 take two join_eval calls
 __device__ __forceinline__ void join_eval_mirror(const DevInfoView &d, uint32_t L, const RelVal &l, uint32_t R,
                                                  const RelVal &r, RelVal &out_lr, RelVal &out_rl) {
     const int n_ec = d.h->n_ec;
     if (n_ec <= 128) {
-        join_eval_mirror_w<1>(d, L, l, R, r, out_lr, out_rl);
+        join_eval_mirror_w<1, false>(d, L, l, R, r, 0u, out_lr, out_rl);
     } else if (n_ec <= 256) {
-        join_eval_mirror_w<2>(d, L, l, R, r, out_lr, out_rl);
+        join_eval_mirror_w<2, false>(d, L, l, R, r, 0u, out_lr, out_rl);
     } else {
         out_lr = join_eval(d, L, l, R, r);
         out_rl = join_eval(d, R, r, L, l);

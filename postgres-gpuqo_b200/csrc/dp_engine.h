@@ -12,6 +12,7 @@ namespace gqb {
 enum DpMode : int {
     kModeDpsub = 0,   // all-subsets enumeration (gpuqo_algorithm=dpsub, bicc off)
     kModeMpdp = 1,    // biconnected-block enumeration (bicc on)
+    kModeDpsize = 2,  // DPsize (gpuqo_algorithm=dpsize): cpu_dpsize's level-list order and ties
 };
 
 // One node of the extracted plan, compact masks (bit i = relation i).

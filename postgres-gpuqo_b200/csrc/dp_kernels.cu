@@ -42,6 +42,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "dp_device.cuh"
@@ -98,6 +99,13 @@ struct DevArena {
     TreeNode *tree = nullptr;          // [64]
     int *tree_n = nullptr;
     unsigned *bar = nullptr;           // grid barrier of the persistent kernel: arrivals, generation, error
+    // DPsize only (allocated on its first use)
+    uint32_t *pos = nullptr;           // [2^n] place of a set in its level list
+    uint32_t *bmask = nullptr;         // [maxC] per set of the previous level: places of its discoveries
+    uint32_t *bstart = nullptr;        // [maxC] exclusive prefix of the mask popcounts
+    uint32_t *tile_sum = nullptr;      // [maxC / kScanTile + 2]
+    unsigned long long *disc = nullptr;   // [maxC] discovery key of each set of the level
+    uint32_t *level1 = nullptr;        // [32] the level-1 list (place of each relation)
 };
 
 // ---------------------------------------------------------------------------
@@ -757,9 +765,17 @@ __device__ __forceinline__ void edge_next(const uint32_t *adj, uint32_t S, EdgeI
     it.e++;
 }
 
-// PIPE: software-pipelined candidate loop for G < 32, in the 2- and 3-blocks
-// persistent kernels; at 64 registers (the 4-blocks persistent kernel and the
-// per-level kernel) it spills, and those keep the plain loop
+// Edge-wise evaluation: the candidates of S come in mirror pairs, c = 2e and
+// c = 2e + 1 being the two orientations of split edge e (side 0 puts the
+// component of a on the outer side).  A lane takes whole edges: it decodes
+// the edge once, loads the two memo entries once and costs both orientations
+// in one fused pass (join_eval_mirror_tree: shared class visit, two
+// independent cost chains), keyed by the reference's indices of both
+// candidates.  Lanes of a group take edges e = gl, gl + G, ...
+// PIPE: software-pipelined edge loop for G < 32, in the 2- and 3-blocks
+// persistent kernels (the next edge's memo entries are requested before the
+// current edge is costed); at 64 registers (the 4-blocks persistent kernel and
+// the per-level kernel) it spills, and those keep the plain loop.
 template <int G, bool MASKED, bool PIPE>
 __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first_set, uint32_t stride_sets,
                                             const uint32_t *sets, uint32_t count, int k, float4 *memo,
@@ -768,8 +784,10 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
     const int lane = threadIdx.x & 31;
     const int grp = lane / G, gl = lane % G;
     const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
-    const uint32_t P = 2u * (uint32_t)(k - 1);
-    const uint32_t per_lane = (P + G - 1u) / G;
+    const uint32_t E = (uint32_t)(k - 1);                 // split edges of a k-set
+    const uint32_t per_lane = (E + G - 1u) / G;
+    // plain-DPsub index of the mirror: pext(S - L, S) - 1 = 2^k - 3 - p
+    const uint32_t mirror_base = (k >= 32 ? 0xFFFFFFFFu : ((1u << k) - 1u)) - 2u;
     for (uint32_t base = first_set; base < count; base += stride_sets) {
         const uint32_t i = base + (uint32_t)grp;
         const bool has = i < count;
@@ -783,9 +801,9 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         // G == 32 (one set per warp): the edges of S indexed cooperatively.
         // Lane t takes the t-th relation of S and its higher-numbered
         // neighbours in S; the inclusive prefix of their counts numbers the
-        // edges in edge_next's order (lower end, then higher end), so a
-        // candidate finds its edge by a binary search over the lanes instead
-        // of walking the edges before it.
+        // edges in edge_next's order (lower end, then higher end), so an
+        // edge is found by a binary search over the lanes instead of walking
+        // the edges before it.
         int vt = 0;
         uint32_t fwd = 0u, scan = 0u;
         if (G == 32) {
@@ -805,90 +823,71 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         best.init();
         const uint32_t *tab = reinterpret_cast<const uint32_t *>(d.h) + h.tree_tab;
         const int n = h.n, nn = n * n;
-        // candidate c on edge (a, b): its two sides, its index in the
-        // reference's enumeration order and the classes on the edge
-        auto decode = [&](uint32_t c, uint32_t &L, uint32_t &R, uint32_t &p, uint32_t &ecm) {
+        // split edge (a, b): the side holding a (outer in orientation 0), the
+        // reference's indices of both orientations and the classes on the edge
+        auto decode = [&](uint32_t &L0, uint32_t &p0, uint32_t &p1, uint32_t &ecm) {
             const int rt = __ffs(S) - 1;
             const uint32_t *anc_r = tab + 2 * nn + rt * n;
             const int ch = ((anc_r[b] >> a) & 1u) ? b : a;        // child end w.r.t. root rt
             const uint32_t comp_c = S & tab[rt * n + ch];
-            const uint32_t comp_a = (ch == a) ? comp_c : (S ^ comp_c);
-            const uint32_t side = c & 1u;
-            L = side ? (S ^ comp_a) : comp_a;                      // side 0: lb = {a}
-            R = S ^ L;
+            L0 = (ch == a) ? comp_c : (S ^ comp_c);
             const uint32_t post = (uint32_t)(__popc(S & tab[nn + rt * n + ch]) - __popc(S & anc_r[ch]) +
                                              __popc(comp_c) - 1);
-            p = h.index_order ? dpsub_index(L, S) : 2u * post + side;
+            if (h.index_order) {
+                p0 = dpsub_index(L0, S);
+                p1 = mirror_base - p0;
+            } else {
+                p0 = 2u * post;
+                p1 = p0 + 1u;
+            }
             ecm = 0u;
             if (MASKED) {
                 const int ch0 = ((tab[2 * nn + b] >> a) & 1u) ? b : a;   // child end w.r.t. relation 0
                 ecm = h.edge_ec[ch0];
             }
         };
-        // costs one candidate from its two memo entries and keeps the lane's
-        // first strict minimum and first NaN in enumeration order
-        auto cost = [&](uint32_t L, uint32_t R, uint32_t p, uint32_t ecm, const float4 lv, const float4 rv) {
+        // costs both orientations of one edge from its two memo entries
+        auto cost2 = [&](uint32_t L0, uint32_t p0, uint32_t p1, uint32_t ecm, const float4 lv, const float4 rv) {
+            const uint32_t R0 = S ^ L0;
             const RelVal l = unpack_rel(lv, h.hz_packed), r = unpack_rel(rv, h.hz_packed);
-            const RelVal out = join_eval_t<MASKED>(d, L, l, R, r, ecm);
-            const bool nan = isnan(out.total);
-            best.n_valid++;
-            if (p < best.first_p) {
-                best.first_p = p;
-                best.first_nan = nan;
-                if (nan) {
-                    best.nan_val = out;
-                    best.nan_left = L;
-                }
-            }
-            if (!nan) {
-                const unsigned long long key = ((unsigned long long)ord_float(out.total) << 32) | p;
-                if (key < best.key) {
-                    best.key = key;
-                    best.val = out;
-                    best.left = L;
-                }
-            }
+            RelVal o0, o1;
+            join_eval_mirror_tree<MASKED>(d, L0, l, R0, r, ecm, o0, o1);
+            best_update(best, p0, L0, o0);
+            best_update(best, p1, R0, o1);
         };
         if (G != 32 && !PIPE) {
             for (uint32_t j = 0; j < per_lane; j++) {
-                const uint32_t c = (uint32_t)gl + j * G;
-                if (has && c < P) {
-                    while (it.e <= (c >> 1)) edge_next(h.adj, S, it, a, b);
-                    uint32_t L, R, p, ecm;
-                    decode(c, L, R, p, ecm);
-                    cost(L, R, p, ecm, __ldcg(memo + L), __ldcg(memo + R));
+                const uint32_t e = (uint32_t)gl + j * G;
+                if (has && e < E) {
+                    while (it.e <= e) edge_next(h.adj, S, it, a, b);
+                    uint32_t L0, p0, p1, ecm;
+                    decode(L0, p0, p1, ecm);
+                    cost2(L0, p0, p1, ecm, __ldcg(memo + L0), __ldcg(memo + (S ^ L0)));
                 }
             }
         } else if (G != 32) {
-            // Software pipeline: a lane walks its candidates in order, and the
-            // next candidate is decoded and its two memo entries requested
-            // before the current one is costed, so that the loads are in
-            // flight during the cost model (measured on the 2- and 3-blocks
-            // variants: 2-3 % off 25-relation snowflakes and 22-relation
-            // stars, 1 % slower on 14-relation snowflakes and chains, whose
-            // lanes hold one or two candidates).
-            uint32_t cL = 0u, cR = 0u, cp = 0u, cecm = 0u;
+            uint32_t cL = 0u, cp0 = 0u, cp1 = 0u, cecm = 0u;
             float4 clv = make_float4(0.f, 0.f, 0.f, 0.f), crv = clv;
             bool cact = false;
-            auto fetch = [&](uint32_t j, uint32_t &L, uint32_t &R, uint32_t &pp, uint32_t &ecm, float4 &lv,
+            auto fetch = [&](uint32_t j, uint32_t &L0, uint32_t &p0, uint32_t &p1, uint32_t &ecm, float4 &lv,
                              float4 &rv) -> bool {
-                const uint32_t c = (uint32_t)gl + j * G;
-                if (!(has && c < P)) return false;
-                while (it.e <= (c >> 1)) edge_next(h.adj, S, it, a, b);
-                decode(c, L, R, pp, ecm);
-                lv = __ldcg(memo + L);
-                rv = __ldcg(memo + R);
+                const uint32_t e = (uint32_t)gl + j * G;
+                if (!(has && e < E)) return false;
+                while (it.e <= e) edge_next(h.adj, S, it, a, b);
+                decode(L0, p0, p1, ecm);
+                lv = __ldcg(memo + L0);
+                rv = __ldcg(memo + (S ^ L0));
                 return true;
             };
-            if (per_lane > 0) cact = fetch(0u, cL, cR, cp, cecm, clv, crv);
+            if (per_lane > 0) cact = fetch(0u, cL, cp0, cp1, cecm, clv, crv);
             for (uint32_t j = 0; j < per_lane; j++) {
-                uint32_t nL = 0u, nR = 0u, np = 0u, necm = 0u;
+                uint32_t nL = 0u, np0 = 0u, np1 = 0u, necm = 0u;
                 float4 nlv = clv, nrv = crv;
-                const bool nact = (j + 1 < per_lane) ? fetch(j + 1, nL, nR, np, necm, nlv, nrv) : false;
-                if (cact) cost(cL, cR, cp, cecm, clv, crv);
+                const bool nact = (j + 1 < per_lane) ? fetch(j + 1, nL, np0, np1, necm, nlv, nrv) : false;
+                if (cact) cost2(cL, cp0, cp1, cecm, clv, crv);
                 cL = nL;
-                cR = nR;
-                cp = np;
+                cp0 = np0;
+                cp1 = np1;
                 cecm = necm;
                 clv = nlv;
                 crv = nrv;
@@ -896,10 +895,9 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
             }
         } else {
             for (uint32_t j = 0; j < per_lane; j++) {
-                const uint32_t c = (uint32_t)gl + j * G;
-                const bool active = has && c < P;
+                const uint32_t e = (uint32_t)gl + j * G;
+                const bool active = has && e < E;
                 // smallest lane t with scan_t > e (every lane takes part in the shuffles)
-                const uint32_t e = c >> 1;
                 int lo = 0;
 #pragma unroll
                 for (int step = 16; step >= 1; step >>= 1) {
@@ -912,9 +910,9 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
                 a = __shfl_sync(kFull, vt, t);
                 if (active) {
                     b = (int)__fns(ft, 0u, (int)(e - before) + 1);
-                    uint32_t L, R, p, ecm;
-                    decode(c, L, R, p, ecm);
-                    cost(L, R, p, ecm, __ldcg(memo + L), __ldcg(memo + R));
+                    uint32_t L0, p0, p1, ecm;
+                    decode(L0, p0, p1, ecm);
+                    cost2(L0, p0, p1, ecm, __ldcg(memo + L0), __ldcg(memo + (S ^ L0)));
                 }
             }
         }
@@ -1248,8 +1246,9 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
         uint32_t *nxt = (k & 1) ? setsA : setsB;
         const uint32_t count = __ldcg(&lvl[k].n_sets);
         if (k < n) level_sets_phase(adj, binom, st, n, k + 1, cur, count, nxt, lvl + k + 1);
+        // lanes take whole split edges (tree_groups): k - 1 per set
         int max_group = 1;
-        while (max_group < 32 && max_group < 2 * (k - 1)) max_group <<= 1;
+        while (max_group < 32 && max_group < k - 1) max_group <<= 1;
         int G = 2;
         while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
         G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
@@ -1371,6 +1370,216 @@ __global__ void __launch_bounds__(kBlock) k_ovf_finalize(const uint32_t *__restr
         RelVal out = join_eval(d, L, l, R, r);
         memo_write(*d.h, memo, memo_left, S, out, L);
     }
+}
+
+// ---------------------------------------------------------------------------
+// DPsize (gpuqo_cpu_dpsize.cu:28-96 with gpuqo_cpu_sequential.cu:28-58): for
+// join size k = 2..n, left size m = k-1 down to 1, every relation set L of the
+// level-m list and R of the level-(k-m) list, in list order, a disjoint and
+// connected pair (L, R) is costed as L joining R; the set L + R keeps its
+// first strict minimum (a NaN cost first found is kept), and is appended to
+// the level-k list when it is first produced.  The level-1 list is the
+// iteration order of the reference's unordered_map memo after the base
+// relations are inserted (dpsize_level1_places); later lists are in
+// discovery order.
+//
+// Here every connected k-set S is costed on its own (one warp, the valid
+// splits of S from the biconnected-block enumeration), with each split keyed
+// by its place in that loop: G = off[|L|] + pos[L], off[m] = the sizes of
+// levels m+1 .. k-1 (larger left sides first), pos[] the position of a set in
+// its level list.  The lexicographic minimum of (cost, G) is the reference's
+// first strict minimum.  S is first produced by its split of smallest
+// (G, pos[R]); that split always has |L| = k-1 (every connected set has a
+// relation whose removal leaves it connected), so S's discovery key is
+// (pos[L*], pos[v*]) with v* the relation outside L*.  The level-k list order
+// follows from the keys without a sort: the sets discovered from one L* are
+// L* + v for different relations v, so one 32-bit mask per level-(k-1) set
+// collects the pos[v] of its discoveries, an exclusive scan of the mask
+// popcounts gives each L*'s first place, and a set's place is that plus the
+// number of lower bits in its L*'s mask.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_dpsize_eval(const uint32_t *__restrict__ blob, uint32_t blob_words,
+                                                        int k, const uint32_t *__restrict__ sets,
+                                                        const LevelCounters *__restrict__ lvl,
+                                                        float4 *__restrict__ memo, uint32_t *__restrict__ memo_left,
+                                                        const uint32_t *__restrict__ pos,
+                                                        unsigned long long *__restrict__ disc,
+                                                        uint32_t *__restrict__ bmask,
+                                                        GlobalCounters *__restrict__ glob) {
+    const uint32_t count = __ldcg(&lvl[k].n_sets);
+    if (count == 0u) return;
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t off[33];
+    load_blob_to_smem(blob, blob_words, sm);
+    const DevInfoView d = make_view(sm);
+    const uint32_t *adj = d.h->adj;
+    if (threadIdx.x == 0) {
+        // off[m] = sizes of the levels m+1 .. k-1; level 1 holds the n relations
+        uint32_t acc = 0u;
+        for (int m = k - 1; m >= 1; m--) {
+            off[m] = acc;
+            acc += (m == 1) ? (uint32_t)d.h->n : __ldcg(&lvl[m].n_sets);
+        }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
+    unsigned long long pairs = 0;
+    Blocks B;
+    CycleCache cc;
+    for (uint32_t i = blockIdx.x * kWarpsPerBlock + warp; i < count; i += nwarps) {
+        const uint32_t S = __ldcg(sets + i);
+        find_blocks(S, adj, B);
+        const uint32_t P = B.etotal;
+        LaneBest best;
+        best.init();
+        unsigned long long dmin = ~0ull;
+        int b = 0;
+        for (uint32_t c = (uint32_t)lane; c < P; c += 32u) {
+            uint32_t L, R, key;
+            if (!mpdp_candidate(S, B, adj, c, b, L, R, key, cc)) continue;
+            const uint32_t g = off[__popc(L)] + __ldcg(pos + L);
+            const unsigned long long dk = ((unsigned long long)g << 32) | __ldcg(pos + R);
+            if (dk < dmin) dmin = dk;
+            const RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
+            best_update(best, g, L, join_eval(d, L, l, R, r));
+        }
+        unsigned long long mk, fk;
+        const WarpWinner w = warp_winner(best, mk, fk);
+        if (w.is_writer) {
+            if (w.use_nan) memo_write(*d.h, memo, memo_left, S, best.nan_val, best.nan_left);
+            else memo_write(*d.h, memo, memo_left, S, best.val, best.left);
+        }
+        const uint32_t dh = __reduce_min_sync(kFull, (uint32_t)(dmin >> 32));
+        const uint32_t dl = __reduce_min_sync(kFull, (uint32_t)(dmin >> 32) == dh ? (uint32_t)dmin : kFull);
+        if (lane == 0) {
+            disc[i] = ((unsigned long long)dh << 32) | dl;
+            atomicOr(bmask + dh, 1u << dl);
+        }
+        pairs += best.n_valid;
+    }
+    pairs = __reduce_add_sync(kFull, (uint32_t)pairs);
+    if (lane == 0 && pairs) atomicAdd(&glob->evaluated_pairs, pairs);
+}
+
+constexpr uint32_t kScanTile = kBlock * 4;   // mask words per block of the place scan
+
+// block b: the popcount total of bmask[b * kScanTile ..) (entries < level k-1's size)
+__global__ void __launch_bounds__(kBlock) k_dpsize_scan_tiles(const uint32_t *__restrict__ bmask,
+                                                              const LevelCounters *__restrict__ lvl, int km1, int n,
+                                                              uint32_t *__restrict__ tile_sum) {
+    const uint32_t cnt = km1 == 1 ? (uint32_t)n : __ldcg(&lvl[km1].n_sets);
+    const uint32_t base = blockIdx.x * kScanTile;
+    if (base >= cnt) return;
+    uint32_t v = 0u;
+    for (uint32_t j = threadIdx.x; j < kScanTile; j += kBlock)
+        if (base + j < cnt) v += (uint32_t)__popc(__ldcg(bmask + base + j));
+    v = __reduce_add_sync(kFull, v);
+    __shared__ uint32_t ws[kWarpsPerBlock];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0u;
+        for (int w = 0; w < kWarpsPerBlock; w++) t += ws[w];
+        tile_sum[blockIdx.x] = t;
+    }
+}
+
+// one block: exclusive scan of the tile totals, in place
+__global__ void __launch_bounds__(kBlock) k_dpsize_scan_top(uint32_t *__restrict__ tile_sum,
+                                                            const LevelCounters *__restrict__ lvl, int km1, int n) {
+    const uint32_t cnt = km1 == 1 ? (uint32_t)n : __ldcg(&lvl[km1].n_sets);
+    const uint32_t tiles = (cnt + kScanTile - 1u) / kScanTile;
+    __shared__ uint32_t carry;
+    __shared__ uint32_t ws[kWarpsPerBlock];
+    if (threadIdx.x == 0) carry = 0u;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < tiles; base += kBlock) {
+        const uint32_t idx = base + threadIdx.x;
+        const uint32_t v = idx < tiles ? tile_sum[idx] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) ws[warp] = incl;
+        __syncthreads();
+        uint32_t wpre = 0u, total = 0u;
+        for (int w = 0; w < kWarpsPerBlock; w++) {
+            if (w < warp) wpre += ws[w];
+            total += ws[w];
+        }
+        if (idx < tiles) tile_sum[idx] = carry + wpre + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+// block b: bstart[j] = exclusive prefix of the mask popcounts for the masks j
+// of tile b (the tile's offset from k_dpsize_scan_top plus the popcounts of
+// the tile's earlier masks); each thread takes 4 consecutive masks
+__global__ void __launch_bounds__(kBlock) k_dpsize_scan_fill(const uint32_t *__restrict__ bmask,
+                                                             const LevelCounters *__restrict__ lvl, int km1, int n,
+                                                             const uint32_t *__restrict__ tile_sum,
+                                                             uint32_t *__restrict__ bstart) {
+    const uint32_t cnt = km1 == 1 ? (uint32_t)n : __ldcg(&lvl[km1].n_sets);
+    const uint32_t base = blockIdx.x * kScanTile;
+    if (base >= cnt) return;
+    const uint32_t j0 = base + threadIdx.x * 4u;
+    uint32_t c[4], tot = 0u;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        c[q] = (j0 + q < cnt) ? (uint32_t)__popc(__ldcg(bmask + j0 + q)) : 0u;
+        tot += c[q];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __shared__ uint32_t ws[kWarpsPerBlock];
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    uint32_t run = __ldcg(tile_sum + blockIdx.x) + incl - tot;
+    for (int w = 0; w < warp; w++) run += ws[w];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (j0 + q < cnt) bstart[j0 + q] = run;
+        run += c[q];
+    }
+}
+
+// every set of level k: its place in the level-k list
+__global__ void __launch_bounds__(kBlock) k_dpsize_place(const uint32_t *__restrict__ sets,
+                                                         const LevelCounters *__restrict__ lvl, int k,
+                                                         const unsigned long long *__restrict__ disc,
+                                                         const uint32_t *__restrict__ bmask,
+                                                         const uint32_t *__restrict__ bstart,
+                                                         uint32_t *__restrict__ pos) {
+    const uint32_t count = __ldcg(&lvl[k].n_sets);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const unsigned long long dk = __ldcg(disc + i);
+        const uint32_t bl = (uint32_t)(dk >> 32), v = (uint32_t)dk;
+        pos[__ldcg(sets + i)] = __ldcg(bstart + bl) + (uint32_t)__popc(__ldcg(bmask + bl) & ((1u << v) - 1u));
+    }
+}
+
+// the masks of the level-(k-1) sets, cleared once every place is read
+__global__ void __launch_bounds__(kBlock) k_dpsize_clear(uint32_t *__restrict__ bmask,
+                                                         const LevelCounters *__restrict__ lvl, int km1, int n) {
+    const uint32_t cnt = km1 == 1 ? (uint32_t)n : __ldcg(&lvl[km1].n_sets);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) bmask[j] = 0u;
+}
+
+// the level-1 list: pos[1 << i] = place of relation i
+__global__ void k_dpsize_init(uint32_t *__restrict__ pos, const uint32_t *__restrict__ level1, int n) {
+    const int i = threadIdx.x;
+    if (i < n) pos[1u << i] = level1[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -1508,6 +1717,20 @@ static std::map<int, Tuning> g_tuning;          // per device, guarded by g_mu
 
 static double tree_connected_sets(const DevHeader *h);
 
+// cpu_dpsize's level-1 list (gpuqo_cpu_dpsize.cu:43-48 after
+// gpuqo_cpu_sequential.cu:73-84): the iteration order of its unordered_map
+// memo once base relation i (key 2^(i+1), whose hash is the key itself) has
+// been inserted for i = 0 .. n-1.  The same standard-library container,
+// filled the same way, gives the same order; place[i] = position of relation i.
+static std::vector<uint32_t> dpsize_level1_places(int n) {
+    std::unordered_map<uint32_t, int> m;
+    for (int i = 0; i < n; i++) m.insert(std::make_pair(1u << (i + 1), i));
+    std::vector<uint32_t> place((size_t)n, 0u);
+    uint32_t p = 0;
+    for (const auto &kv : m) place[(size_t)kv.second] = p++;
+    return place;
+}
+
 // Per-run control words of the single-query engine, contiguous so that one
 // memset clears the counters and one copy brings everything back.
 struct EngineCtl {
@@ -1530,6 +1753,7 @@ public:
     uint64_t cap_sets = 0;
     uint32_t blob_cap_words = 0;
     uint32_t *h_blob = nullptr;        // pinned staging
+    uint32_t h_level1[32];             // staging of the DPsize level-1 list (copied before each launch)
     EngineCtl *d_ctl = nullptr;        // device control words (a.lvl, a.glob, a.bar, a.tree_n, a.tree point here)
     EngineCtl *h_ctl = nullptr;        // pinned copy
     TreeNode *h_tree = nullptr;        // views into h_ctl
@@ -1627,12 +1851,87 @@ public:
         return 0;
     }
 
+    int dpsize_cap_n = -1;             // DPsize buffers sized for this many relations
+
+    int ensure_dpsize(int n, std::string &err) {
+        if (n <= dpsize_cap_n) return 0;
+        const uint64_t ms = max_level_sets(n);
+        const uint64_t tiles = ms / kScanTile + 2;
+        if (int rc = over_budget(engine_bytes_needed(n) + (1ull << n) * 4 + ms * 16 + tiles * 4,
+                                 "DPsize's dense memo, level lists and place arrays", err))
+            return rc;
+        drop_graphs();
+        cudaFree(a.pos);
+        cudaFree(a.bmask);
+        cudaFree(a.bstart);
+        cudaFree(a.tile_sum);
+        cudaFree(a.disc);
+        a.pos = a.bmask = a.bstart = a.tile_sum = nullptr;
+        a.disc = nullptr;
+        dpsize_cap_n = -1;
+        CK(cudaMalloc(&a.pos, (1ull << n) * sizeof(uint32_t)));
+        CK(cudaMalloc(&a.bmask, ms * sizeof(uint32_t)));
+        CK(cudaMalloc(&a.bstart, ms * sizeof(uint32_t)));
+        CK(cudaMalloc(&a.tile_sum, tiles * sizeof(uint32_t)));
+        CK(cudaMalloc(&a.disc, ms * sizeof(unsigned long long)));
+        if (!a.level1) CK(cudaMalloc(&a.level1, 32 * sizeof(uint32_t)));
+        dpsize_cap_n = n;
+        return 0;
+    }
+
+    // DPsize of n relations on `stream` (see k_dpsize_eval)
+    int enqueue_dpsize(int n, uint32_t blob_words, std::string &err) {
+        const size_t smem = eval_smem(blob_words);
+        CK(cudaMemsetAsync(d_ctl, 0, kCtlClearBytes, stream));
+        CK(cudaMemsetAsync(a.seen, 0, std::max<uint64_t>((1ull << n) / 8, 4), stream));
+        CK(cudaMemsetAsync(a.bmask, 0, max_level_sets(n) * sizeof(uint32_t), stream));
+        n_kernels = 0;
+        k_init_base<<<1, 32, 0, stream>>>(a.blob, a.memo, a.memo_left);
+        k_dpsize_init<<<1, 32, 0, stream>>>(a.pos, a.level1, n);
+        n_kernels += 2;
+        for (int k = 2; k <= n; k++) {
+            const uint64_t total = binom64(n, k);
+            uint64_t threads = std::min<uint64_t>((uint64_t)sm_count * 8 * kBlock, (total + 3) / 4);
+            threads = std::max<uint64_t>(threads, 32);
+            const uint32_t per_thread = (uint32_t)((total + threads - 1) / threads);
+            const uint32_t fblocks =
+                (uint32_t)((total + (uint64_t)per_thread * kBlock - 1) / ((uint64_t)per_thread * kBlock));
+            uint32_t *cur_sets = (k & 1) ? a.sets2 : a.sets;
+            const uint32_t *prev_sets = (k & 1) ? a.sets : a.sets2;
+            k_level_sets<<<fblocks, kBlock, 0, stream>>>(a.blob, a.binom, n, k, total, per_thread, prev_sets,
+                                                         a.lvl + (k - 1), a.seen, cur_sets, a.lvl + k);
+            const int eblocks =
+                (int)std::min<uint64_t>((uint64_t)sm_count * 4, (total + kWarpsPerBlock - 1) / kWarpsPerBlock);
+            CK(cudaEventRecordWithFlags(kev[2 * k], stream, cudaEventRecordExternal));
+            k_dpsize_eval<<<eblocks, kBlock, smem, stream>>>(a.blob, blob_words, k, cur_sets, a.lvl, a.memo,
+                                                             a.memo_left, a.pos, a.disc, a.bmask, a.glob);
+            CK(cudaEventRecordWithFlags(kev[2 * k + 1], stream, cudaEventRecordExternal));
+            // places of the level-k sets from the masks of the level-(k-1) sets
+            const uint64_t prev_total = binom64(n, k - 1);
+            const uint32_t tiles = (uint32_t)((prev_total + kScanTile - 1) / kScanTile);
+            k_dpsize_scan_tiles<<<tiles, kBlock, 0, stream>>>(a.bmask, a.lvl, k - 1, n, a.tile_sum);
+            k_dpsize_scan_top<<<1, kBlock, 0, stream>>>(a.tile_sum, a.lvl, k - 1, n);
+            k_dpsize_scan_fill<<<tiles, kBlock, 0, stream>>>(a.bmask, a.lvl, k - 1, n, a.tile_sum, a.bstart);
+            const uint32_t pblocks = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8, (total + kBlock - 1) / kBlock);
+            k_dpsize_place<<<pblocks, kBlock, 0, stream>>>(cur_sets, a.lvl, k, a.disc, a.bmask, a.bstart, a.pos);
+            const uint32_t cblocks =
+                (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8, (prev_total + kBlock - 1) / kBlock);
+            k_dpsize_clear<<<cblocks, kBlock, 0, stream>>>(a.bmask, a.lvl, k - 1, n);
+            n_kernels += 7;
+        }
+        const uint32_t full = (n == 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
+        k_extract<<<1, 32, 0, stream>>>(a.memo, a.memo_left, full, a.blob, a.tree, a.tree_n);
+        n_kernels++;
+        return 0;
+    }
+
     size_t eval_smem(uint32_t blob_words) const {
         return (size_t)(((blob_words + 3u) & ~3u) + kWarpsPerBlock * kQueueWords) * 4u;
     }
 
     // Enqueues the whole DP for n relations on `stream`.
     int enqueue(int n, DpMode mode, bool ccc, bool profile, uint32_t blob_words, std::string &err) {
+        if (mode == kModeDpsize) return enqueue_dpsize(n, blob_words, err);
         const size_t smem = eval_smem(blob_words);
         const uint32_t max_block = reinterpret_cast<const DevHeader *>(h_blob)->max_block;
         const bool tree_mode = reinterpret_cast<const DevHeader *>(h_blob)->tree_mode != 0u;
@@ -1668,8 +1967,11 @@ public:
                 const uint32_t target_lanes = (uint32_t)sm_count * 24u * 32u;
                 int mblocks = (int)std::min<uint64_t>((uint64_t)sm_count * 4, (total * 32 + kBlock - 1) / kBlock);
                 if (tree_mode) {
+                    // the tree kernel's lanes take split edges: k - 1 per set
+                    int max_edge_group = 1;
+                    while (max_edge_group < 32 && max_edge_group < k - 1) max_edge_group <<= 1;
                     k_eval_tree<<<mblocks, kBlock, smem, stream>>>(a.blob, blob_words, k, cur_sets, lc, a.memo,
-                                                                   a.memo_left, a.glob, target_lanes, max_group);
+                                                                   a.memo_left, a.glob, target_lanes, max_edge_group);
                 } else {
                     k_eval_mpdp<<<mblocks, kBlock, smem, stream>>>(a.blob, blob_words, cur_sets, lc, a.memo,
                                                                    a.memo_left, a.ovf_set, a.ovf_P, a.ovf_off,
@@ -1791,10 +2093,17 @@ public:
         // graph serves every query of the same size class
         words = ((uint32_t)blob.size() + 511u) & ~511u;
         if (int rc = ensure(n, words, err)) return rc;
+        if (mode == kModeDpsize) {
+            if (int rc = ensure_dpsize(n, err)) return rc;
+            const std::vector<uint32_t> l1 = dpsize_level1_places(n);
+            std::memcpy(h_level1, l1.data(), l1.size() * 4);
+            CK(cudaMemcpyAsync(a.level1, h_level1, l1.size() * 4, cudaMemcpyHostToDevice, stream));
+        }
         std::memset(h_blob, 0, words * 4);
         std::memcpy(h_blob, blob.data(), blob.size() * 4);
         const size_t smem = eval_smem(words);
         if (smem > 48 * 1024) {
+            CK(cudaFuncSetAttribute(k_dpsize_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             CK(cudaFuncSetAttribute(k_eval<kModeDpsub>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             CK(cudaFuncSetAttribute(k_eval<kModeMpdp>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             CK(cudaFuncSetAttribute(k_ovf_chunks<kModeDpsub>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -2250,6 +2559,11 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
         fprintf(stderr, "gpuqo_b200_run_noalloc: output holds %d nodes, %d needed\n", max_nodes, 2 * n - 1);
         return GPUQO_B200_ERR_ARGS;
     }
+    if (gpuqo_spanning_tree_enable) {
+        fprintf(stderr, "gpuqo_b200_run_noalloc: plans the query graph as given; gpuqo_spanning_tree_enable is "
+                        "served by gpuqo_run\n");
+        return GPUQO_B200_ERR_UNSUPPORTED;
+    }
     DpMode mode;
     switch (gpuqo_algorithm_arg) {
     case GPUQO_CPU_DPSUB_BICC:
@@ -2265,7 +2579,8 @@ extern "C" int gpuqo_b200_run_noalloc(int gpuqo_algorithm_arg, const GpuqoPlanne
         mode = gpuqo_dpsub_bicc_enable ? kModeMpdp : kModeDpsub;
         break;
     default:
-        fprintf(stderr, "gpuqo_b200_run_noalloc: algorithm %d is outside this library\n", gpuqo_algorithm_arg);
+        fprintf(stderr, "gpuqo_b200_run_noalloc: algorithm %d is not served by this entry point (DPsub and MPDP "
+                        "only)\n", gpuqo_algorithm_arg);
         return GPUQO_B200_ERR_UNSUPPORTED;
     }
     uint32_t blob[kNoAllocMaxBlobWords];

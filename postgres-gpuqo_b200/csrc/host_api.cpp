@@ -541,6 +541,10 @@ void apply_dpsub_csg(std::vector<uint32_t> &blob, DpMode &mode) {
 
 DpMode mode_for(int algorithm) {
     switch (algorithm) {
+    case GPUQO_DPSIZE:
+    case GPUQO_CPU_DPSIZE:
+    case GPUQO_DPE_DPSIZE:
+        return kModeDpsize;
     case GPUQO_CPU_DPSUB_BICC:
     case GPUQO_CPU_DPSUB_BICC_PARALLEL:
         return kModeMpdp;
@@ -555,6 +559,9 @@ DpMode mode_for(int algorithm) {
 
 bool algorithm_supported(int algorithm) {
     switch (algorithm) {
+    case GPUQO_DPSIZE:
+    case GPUQO_CPU_DPSIZE:
+    case GPUQO_DPE_DPSIZE:
     case GPUQO_DPSUB:
     case GPUQO_CPU_DPSUB:
     case GPUQO_CPU_DPSUB_PARALLEL:
@@ -614,7 +621,7 @@ QueryTreeC *run_one(int algorithm, GpuqoPlannerInfoC *info_c) {
     }
     const int n = info_c->n_rels;
     const bool idp = gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < n;
-    if (idp || n >= 64) return run_idp(algorithm, info_c);
+    if (idp || n >= 64 || gpuqo_spanning_tree_enable) return run_planned(algorithm, info_c);
 
     HostInfo info;
     if (!convert_info(info_c, info, err)) {
@@ -669,6 +676,11 @@ extern "C" int gpuqo_b200_time_resident(int gpuqo_algorithm_arg, GpuqoPlannerInf
     if (!algorithm_supported(gpuqo_algorithm_arg) || !info_c || info_c->n_rels < 1 || info_c->n_rels > 31 ||
         warmup < 0 || iters < 1 || !ms_per_iter) {
         set_error(GPUQO_B200_ERR_ARGS, "gpuqo_b200_time_resident: bad arguments");
+        return t_last_error;
+    }
+    if (gpuqo_spanning_tree_enable) {
+        set_error(GPUQO_B200_ERR_UNSUPPORTED, "gpuqo_b200_time_resident times the query graph as given "
+                                              "(gpuqo_spanning_tree_enable is set)");
         return t_last_error;
     }
     HostInfo info;
@@ -796,7 +808,8 @@ extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *
     auto prepare = [&](int i) {
         GpuqoPlannerInfoC *c = infos[i];
         const bool idp = c && gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < c->n_rels;
-        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp) return;
+        // the planner path (run_one) applies gpuqo_spanning_tree_enable
+        if (!c || c->n_rels < 1 || c->n_rels > 30 || idp || gpuqo_spanning_tree_enable) return;
         DpMode m = mode;
         HostInfo info;
         std::string err;

@@ -18,6 +18,7 @@
 // are identical.  The heaps and priority queues are the same libstdc++
 // algorithms fed in the same order, so their tie behaviour is the reference's.
 #include <algorithm>
+#include <limits>
 #include <atomic>
 #include <csignal>
 #include <array>
@@ -38,6 +39,7 @@
 
 extern "C" int gpuqo_idp_n_iters;
 extern "C" int gpuqo_idp_type;
+extern "C" bool gpuqo_spanning_tree_enable;
 extern "C" volatile sig_atomic_t InterruptPending;
 extern "C" void *palloc(size_t size);
 extern "C" void *palloc0(size_t size);
@@ -323,6 +325,60 @@ static float estimate_join_rows(const GInfo &g, const QT &l, const QT &r) {
     float sel = estimate_join_selectivity(g, l.id, r.id);
     float rows = sel * l.rows * r.rows;
     return rows > 1 ? std::round(rows) : 1;
+}
+
+// ---------------------------------------------------------------------------
+// gpuqo_spanning_tree_enable (minimumSpanningTree, gpuqo_spanning_tree.cu:19-72,
+// applied by __gpuqo_run before the BFS relabelling for every algorithm,
+// gpuqo_main_internal.cu:94-100): the join graph is replaced by a spanning
+// tree grown from relation 0, each step adding the edge from the tree to a
+// new relation whose two base relations give the fewest estimated join rows
+// (the first strict minimum, tree relations and their neighbours both in
+// increasing order).  The equivalence classes stay as they are, so joins are
+// still costed with every class; only the csg-cmp pairs follow the tree.
+// A step that finds no edge with fewer rows than FLT_MAX (every estimate
+// infinite or NaN; the reference leaves that case undefined) takes the first
+// edge it visited.
+// ---------------------------------------------------------------------------
+static void spanning_tree(GInfo &g) {
+    const int n = g.n;
+    std::vector<BB> out(n);
+    std::vector<char> in_tree(n, 0);
+    BB S = BB::bit(1);
+    in_tree[0] = 1;
+    for (int added = 1; added < n; added++) {
+        float best = std::numeric_limits<float>::max();
+        int ai = -1, ao = -1, fi = -1, fo = -1;
+        for (int i = 0; i < n; i++) {
+            if (!in_tree[i]) continue;
+            (g.edge[i] - S).for_each([&](int b) {
+                const int j = b - 1;
+                if (j < 0 || j >= n) return;
+                if (fi < 0) {
+                    fi = i;
+                    fo = j;
+                }
+                const float sel = estimate_join_selectivity(g, BB::bit(i + 1), BB::bit(j + 1));
+                const float r = sel * g.base[i].rows * g.base[j].rows;
+                const float rows = r > 1 ? std::round(r) : 1;
+                if (rows < best) {
+                    best = rows;
+                    ai = i;
+                    ao = j;
+                }
+            });
+        }
+        if (ao < 0) {
+            if (fo < 0) break;   // disconnected: refused by the caller's BFS check
+            ai = fi;
+            ao = fo;
+        }
+        S.set(ao + 1);
+        in_tree[ao] = 1;
+        out[ai].set(ao + 1);
+        out[ao].set(ai + 1);
+    }
+    g.edge = std::move(out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1040,9 +1096,11 @@ struct Planner {
     Ctx C;
     GInfo g;
     int idp_n_iters = 0, idp_type = GPUQO_IDP2;
+    bool spanning = false;   // gpuqo_spanning_tree_enable at creation
     QT *result = nullptr;
 
     int run() {
+        if (spanning) spanning_tree(g);
         std::vector<Entry> bl = bfs_list(g);
         if ((int)bl.size() != g.n) {
             C.msg = "query graph is not connected";
@@ -1091,6 +1149,7 @@ PlannerHandle *planner_new(int algorithm, const GpuqoPlannerInfoC *info_c, int i
     p->C.solve = std::move(solver);
     p->idp_n_iters = idp_n_iters;
     p->idp_type = idp_type;
+    p->spanning = gpuqo_spanning_tree_enable;
     return reinterpret_cast<PlannerHandle *>(p);
 }
 
@@ -1109,16 +1168,16 @@ QueryTreeC *planner_result(PlannerHandle *h) { return qt_to_c(reinterpret_cast<P
 
 void planner_free(PlannerHandle *h) { delete reinterpret_cast<Planner *>(h); }
 
-QueryTreeC *run_idp(int algorithm, GpuqoPlannerInfoC *info_c) {
+QueryTreeC *run_planned(int algorithm, GpuqoPlannerInfoC *info_c) {
     std::string err;
     const int n = info_c->n_rels;
     const bool idp = gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < n;
-    if (!idp) {
+    if (!idp && n > 31) {
         set_error(GPUQO_B200_ERR_UNSUPPORTED,
                   std::to_string(n) + " relations need IDP (set gpuqo_idp_n_iters between 2 and n-1)");
         return nullptr;
     }
-    if (gpuqo_idp_type != GPUQO_IDP2 && gpuqo_idp_type != GPUQO_UNION) {
+    if (idp && gpuqo_idp_type != GPUQO_IDP2 && gpuqo_idp_type != GPUQO_UNION) {
         set_error(GPUQO_B200_ERR_UNSUPPORTED, "gpuqo_idp_type: only IDP2 and UNION are provided");
         return nullptr;
     }

@@ -27,9 +27,11 @@ void planner_cancel(PlannerHandle *p);
 QueryTreeC *planner_result(PlannerHandle *p);   // palloc'd, caller's numbering
 void planner_free(PlannerHandle *p);
 
-// Entry used by gpuqo_run when 1 < gpuqo_idp_n_iters < n_rels, or when the
-// query has 64 or more relations.
-QueryTreeC *run_idp(int algorithm, GpuqoPlannerInfoC *info);
+// Entry used by gpuqo_run when 1 < gpuqo_idp_n_iters < n_rels, when the
+// query has 64 or more relations, or when gpuqo_spanning_tree_enable is set:
+// the planner on dynamic bitsets (spanning tree, BFS relabel, IDP2 / UnionDP
+// or one exact DP of at most 31 relations).
+QueryTreeC *run_planned(int algorithm, GpuqoPlannerInfoC *info);
 
 void set_error(int code, const std::string &msg);
 

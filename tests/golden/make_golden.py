@@ -8,9 +8,17 @@ gpuqo module compiled from its sources by ``make -C oracle ref``.
 Algorithm codes follow src/include/optimizer/gpuqo_common.h:13-29:
 3 = GPUQO_CPU_DPSUB (plain DPsub), 5 = GPUQO_CPU_DPSUB_BICC (MPDP).
 
+``spanning_cases.jsonl`` (``--spanning``) holds queries planned with
+gpuqo_spanning_tree_enable set: the reference replaces the join graph by its
+minimum spanning tree before any algorithm runs (exact DP or IDP).
+``dpsize_cases.jsonl`` (``--dpsize``) holds the plans of the reference's
+cpu_dpsize (algorithm code 2), the tie order the library's DPsize follows.
+
 Usage (needs the reference library; run where the reference sources are):
     python tests/golden/make_golden.py            # small + full-size cases
     python tests/golden/make_golden.py --quick    # skip the minutes-long ones
+    python tests/golden/make_golden.py --spanning # the spanning-tree fixtures
+    python tests/golden/make_golden.py --dpsize   # the DPsize fixtures
 """
 import argparse
 import json
@@ -33,7 +41,7 @@ def cases(quick):
     for s in range(10):
         out.append(("star12", query.star(12, s), DPSUB))
     # configuration 2: 25-relation snowflake, MPDP
-    for s in range(3):
+    for s in range(4):
         out.append(("snowflake25", query.snowflake(25, s), BICC))
     # configuration 3 at reduced sizes
     for s in range(3):
@@ -60,10 +68,48 @@ def cases(quick):
     if not quick:
         # configuration 3 at full size (minutes of reference CPU time each)
         out.append(("clique14_bicc", query.clique(14, 0), BICC))
+        out.append(("clique18", query.clique(18, 0), DPSUB))
         out.append(("chain30", query.chain(30, 0), DPSUB))
         out.append(("cycle30", query.cycle(30, 0), DPSUB))
         out.append(("chain30_bicc", query.chain(30, 0), BICC))
         out.append(("cycle30_bicc", query.cycle(30, 0), BICC))
+    return out
+
+
+def spanning_cases():
+    """(tag, query, algorithm, idp_n_iters, idp_type) with the spanning tree on."""
+    out = []
+    for s in range(4):
+        out.append(("sp_random", query.random_graph(9 + s, 9100 + s, extra_edge_p=0.35, rich=True), DPSUB, 0, 1))
+        out.append(("sp_random_bicc", query.random_graph(11 + s, 9200 + s, extra_edge_p=0.35, rich=True), BICC, 0, 1))
+        out.append(("sp_multi", query.multi_member_classes(9 + s, 9300 + s), BICC, 0, 1))
+    out.append(("sp_cycle", query.cycle(14, 9400), BICC, 0, 1))
+    out.append(("sp_clique", query.clique(9, 9401), DPSUB, 0, 1))
+    out.append(("sp_clique_bicc", query.clique(10, 9402, rich=True), BICC, 0, 1))
+    out.append(("sp_equal", query.random_graph(10, 9403, extra_edge_p=0.4, equal=True), BICC, 0, 1))
+    # IDP2 over the spanning tree, 64-bit and dynamic relation sets
+    out.append(("sp_idp2", query.random_graph(40, 9500, extra_edge_p=0.06), BICC, 12, 1))
+    out.append(("sp_idp2_dyn", query.random_graph(80, 9501, extra_edge_p=0.03), BICC, 12, 1))
+    out.append(("sp_union", query.random_graph(36, 9502, extra_edge_p=0.06), BICC, 10, 2))
+    return out
+
+
+def dpsize_cases():
+    """(tag, query, algorithm, idp_n_iters, idp_type) for cpu_dpsize (code 2)."""
+    DPSIZE = 2
+    out = []
+    for s in range(3):
+        out.append(("dz_star12", query.star(12, s), DPSIZE, 0, 1))
+        out.append(("dz_snowflake16", query.snowflake(16, 9600 + s), DPSIZE, 0, 1))
+        out.append(("dz_random", query.random_graph(11 + s, 9610 + s, extra_edge_p=0.3, rich=True), DPSIZE, 0, 1))
+        out.append(("dz_equal", query.random_graph(10 + s, 9620 + s, extra_edge_p=0.3, equal=True), DPSIZE, 0, 1))
+        out.append(("dz_multi", query.multi_member_classes(9 + s, 9630 + s), DPSIZE, 0, 1))
+    out.append(("dz_chain18", query.chain(18, 9640), DPSIZE, 0, 1))
+    out.append(("dz_cycle14", query.cycle(14, 9641), DPSIZE, 0, 1))
+    out.append(("dz_clique9", query.clique(9, 9642), DPSIZE, 0, 1))
+    out.append(("dz_single", query.chain(1, 0), DPSIZE, 0, 1))
+    out.append(("dz_pair", query.chain(2, 1), DPSIZE, 0, 1))
+    out.append(("dz_idp2", query.snowflake(40, 9650), DPSIZE, 10, 1))
     return out
 
 
@@ -77,9 +123,24 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--out", default=os.path.join(HERE, "cases.jsonl"))
+    ap.add_argument("--spanning", action="store_true", help="write spanning_cases.jsonl instead")
+    ap.add_argument("--dpsize", action="store_true", help="write dpsize_cases.jsonl (cpu_dpsize) instead")
     args = ap.parse_args()
     if not harness.ref_available():
         sys.exit("oracle/_ref/libgpuqo_ref.so missing: run `make -C oracle ref` first")
+    if args.spanning or args.dpsize:
+        fname, gen = ("spanning_cases.jsonl", spanning_cases) if args.spanning else ("dpsize_cases.jsonl", dpsize_cases)
+        with open(os.path.join(HERE, fname), "w") as f:
+            for tag, q, alg, k, typ in gen():
+                t0 = time.time()
+                tree, _ = harness.run_ref(q, alg, idp_n_iters=k, idp_type=typ, spanning=args.spanning)
+                rec = {"tag": tag, "name": q.name, "algorithm": alg, "idp_n_iters": k, "idp_type": typ,
+                       "query": q.to_dict(), "expected": tree_json(tree)}
+                f.write(json.dumps(rec, separators=(",", ":")) + "\n")
+                f.flush()
+                print(f"{tag:16s} {q.name:24s} alg={alg} k={k} {time.time() - t0:7.2f}s root_total={tree[3]!r}",
+                      flush=True)
+        return
     with open(args.out, "w") as f:
         for tag, q, alg in cases(args.quick):
             t0 = time.time()
