@@ -296,6 +296,23 @@ int gpuqo_b200_run_batch(int gpuqo_algorithm, GpuqoPlannerInfoC **infos,
                          int n_queries, QueryTreeC **out);
 
 /*
+ * Devices of the batch entry and of the planner service (no reference
+ * counterpart): 1 (the default) uses the calling thread's current device;
+ * N > 1 the N devices from the current one on, wrapping around the visible
+ * ones; 0 every visible device.  Queries are independent, so a batch is
+ * split by estimated work (gpuqo_b200_plan_shards) and each device runs its
+ * share with its own engines on its own host thread; the service gives each
+ * request to the device with the fewest requests in flight.  No data crosses
+ * between devices.  Plans do not depend on the setting.
+ */
+extern int gpuqo_b200_devices;
+
+/* The split used by the batch: item i of weight work[i] goes to device
+ * device_of_item[i] in [0, n_devices), longest first onto the least-loaded
+ * device (lower index first on ties).  A pure host function. */
+int gpuqo_b200_plan_shards(const double *work, int n_items, int n_devices, int *device_of_item);
+
+/*
  * Continuous-batching planner service (standalone planning processes; inside
  * a Postgres backend use gpuqo_run).  Requests are planned concurrently, at
  * most max_inflight at a time (later ones wait for a slot); every exact DP a

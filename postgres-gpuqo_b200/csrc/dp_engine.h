@@ -57,6 +57,13 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
                      std::vector<std::vector<TreeNode>> &out, EngineStats &stats, std::vector<double> &wave_ms,
                      std::string &err);
 bool batch_eligible(const std::vector<uint32_t> &blob);
+// Relative work of one exact DP (connected sets times candidates per set, from
+// the exact count on tree-shaped graphs, an upper bound otherwise): the
+// weight by which a batch is spread over devices.
+double engine_work_estimate(const std::vector<uint32_t> &blob);
+// Host-side helpers of the multi-device batch and service (host_api.cpp).
+void plan_shards(const double *work, int n, int n_dev, int *dev_of);
+int batch_devices(std::vector<int> &devs, std::string &err);
 uint64_t batch_query_bytes(int n);
 
 // Device-memory estimate (bytes) of one exact DP over n relations.

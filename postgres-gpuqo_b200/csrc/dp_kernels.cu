@@ -1713,7 +1713,8 @@ struct Tuning {
     double batch_single_sets = double(1u << 20);   // a batch hands larger tree queries to k_dp_tree
     bool tuned = false;
 };
-static std::map<int, Tuning> g_tuning;          // per device, guarded by g_mu
+constexpr int kMaxDevices = 64;
+static Tuning g_tuning[kMaxDevices];            // per device, guarded by g_dev_mu
 
 static double tree_connected_sets(const DevHeader *h);
 
@@ -2311,8 +2312,27 @@ public:
     }
 };
 
-static std::mutex g_mu;
-static std::map<int, std::unique_ptr<Engine>> g_engines;
+// One engine of each kind per device, each device's engines and tuning
+// record guarded by that device's mutex, so that host threads driving
+// different devices (the batch and the server spread over several) do not
+// wait for one another.
+static std::mutex g_dev_mu[kMaxDevices];
+static std::unique_ptr<Engine> g_engines[kMaxDevices];
+
+// the calling thread's current device (a valid index of the engine tables)
+static int current_device(int &dev, std::string &err) {
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return GPUQO_B200_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        err = "device index " + std::to_string(dev) + " beyond the library's " + std::to_string(kMaxDevices);
+        return GPUQO_B200_ERR_CUDA;
+    }
+    return 0;
+}
 
 }  // namespace gqb
 
@@ -3303,6 +3323,13 @@ static bool batch_prefers_single(const std::vector<uint32_t> &blob, int device) 
            tree_connected_sets(h) > g_tuning[device].batch_single_sets;
 }
 
+double engine_work_estimate(const std::vector<uint32_t> &blob) {
+    const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
+    const double n = (double)h->n;
+    if (h->tree_mode) return tree_connected_sets(h) * 2.0 * std::max(n - 1.0, 1.0);
+    return std::ldexp(1.0, h->n) * n;
+}
+
 uint64_t batch_query_bytes(int n) {
     const uint64_t slots = 1ull << n;
     return slots * (sizeof(float4) + 4) + slots / 8 + 2 * max_level_sets(n) * 8 + 64 * sizeof(TreeNode) + 4096;
@@ -3586,17 +3613,14 @@ struct BatchEngine {
     }
 };
 
-static std::map<int, std::unique_ptr<BatchEngine>> g_batch;
+static std::unique_ptr<BatchEngine> g_batch[kMaxDevices];
 
 int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, uint64_t wave_bytes,
                      std::vector<std::vector<TreeNode>> &out, EngineStats &st, std::vector<double> &wave_ms,
                      std::string &err) {
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        err = "cudaGetDevice failed";
-        return GPUQO_B200_ERR_CUDA;
-    }
+    if (int rc = current_device(dev, err)) return rc;
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     auto &be = g_batch[dev];
     if (!be) be.reset(new BatchEngine());
     if (int rc = be->init(err)) return rc;
@@ -3670,13 +3694,9 @@ int engine_run(const std::vector<uint32_t> &blob, int n, DpMode mode, bool ccc, 
         err = "exact DP supports 1..31 relations";
         return GPUQO_B200_ERR_TOO_LARGE;
     }
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-        return GPUQO_B200_ERR_CUDA;
-    }
+    if (int rc = current_device(dev, err)) return rc;
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
     if (mode == kModeMpdp && h->tree_mode == 0u && n <= 30 && gpuqo_b200_persistent != 0 && !profile) {
         auto &be = g_batch[dev];
@@ -3714,13 +3734,9 @@ int engine_time_resident(const std::vector<uint32_t> &blob, int n, DpMode mode, 
         err = "exact DP supports 1..31 relations";
         return GPUQO_B200_ERR_TOO_LARGE;
     }
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-        return GPUQO_B200_ERR_CUDA;
-    }
+    if (int rc = current_device(dev, err)) return rc;
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     // the same routing as engine_run: graphs with cycles as one-query waves
     const DevHeader *h = reinterpret_cast<const DevHeader *>(blob.data());
     if (mode == kModeMpdp && h->tree_mode == 0u && n <= 30 && gpuqo_b200_persistent != 0 && iters > 0) {
@@ -3795,12 +3811,9 @@ static double crossover_below(const std::vector<double> &sets, const std::vector
 
 int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &single_narrow_level_sets,
                     double &single_wide_level_sets, double &batch_single_sets, std::string &err) {
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        err = "cudaGetDevice failed";
-        return GPUQO_B200_ERR_CUDA;
-    }
+    if (int rc = current_device(dev, err)) return rc;
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     auto &eng = g_engines[dev];
     if (!eng) eng.reset(new Engine());
     auto &be = g_batch[dev];
@@ -3849,10 +3862,10 @@ int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &sin
 
 void engine_set_tuning(double single_narrow_level_sets, double single_wide_level_sets, double batch_single_sets,
                        bool tuned) {
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    cudaGetDevice(&dev);
-    cudaGetLastError();
+    std::string err;
+    if (current_device(dev, err)) dev = 0;   // no device yet: the record of device 0
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     Tuning &tu = g_tuning[dev];
     tu.single_narrow_level_sets = single_narrow_level_sets;
     tu.single_wide_level_sets = single_wide_level_sets;
@@ -3861,30 +3874,27 @@ void engine_set_tuning(double single_narrow_level_sets, double single_wide_level
 }
 
 int engine_reset_persistent() {
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
+    std::string err;
+    if (current_device(dev, err)) return 0;
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     int cleared = 0;
-    auto e = g_engines.find(dev);
-    if (e != g_engines.end() && e->second && e->second->barrier_timed_out) {
-        e->second->barrier_timed_out = false;
+    if (g_engines[dev] && g_engines[dev]->barrier_timed_out) {
+        g_engines[dev]->barrier_timed_out = false;
         cleared++;
     }
-    auto b = g_batch.find(dev);
-    if (b != g_batch.end() && b->second && b->second->barrier_timed_out) {
-        b->second->barrier_timed_out = false;
+    if (g_batch[dev] && g_batch[dev]->barrier_timed_out) {
+        g_batch[dev]->barrier_timed_out = false;
         cleared++;
     }
     return cleared;
 }
 
 void engine_get_tuning(double &single_narrow_level_sets, double &single_wide_level_sets, double &batch_single_sets, bool &tuned) {
-    std::lock_guard<std::mutex> lk(g_mu);
     int dev = 0;
-    cudaGetDevice(&dev);
+    std::string err;
+    if (current_device(dev, err)) dev = 0;
+    std::lock_guard<std::mutex> lk(g_dev_mu[dev]);
     const Tuning &tu = g_tuning[dev];
     single_narrow_level_sets = tu.single_narrow_level_sets;
     single_wide_level_sets = tu.single_wide_level_sets;

@@ -15,6 +15,8 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "dp_engine.h"
 #include "gpuqo_b200.h"
 #include "host_idp.h"
@@ -82,6 +84,7 @@ int gpuqo_b200_batch_memory_mb = 32768;
 int gpuqo_b200_persistent = 1;
 int gpuqo_b200_barrier_poll_limit = 0;
 int gpuqo_b200_device_memory_mb = 0;
+int gpuqo_b200_devices = 1;
 }
 
 namespace gqb {
@@ -783,6 +786,53 @@ extern "C" int gpuqo_b200_get_tuning(GpuqoB200Tuning *out) {
     return GPUQO_B200_OK;
 }
 
+namespace gqb {
+
+// Longest-processing-time assignment of weighted work items to n_dev devices:
+// items in decreasing weight (lower index first on ties), each to the device
+// with the least weight so far (lower index first on ties).  Deterministic;
+// every device gets items before any gets a second when there are enough.
+void plan_shards(const double *work, int n, int n_dev, int *dev_of) {
+    if (n_dev < 1) n_dev = 1;
+    std::vector<int> order((size_t)n);
+    for (int i = 0; i < n; i++) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    std::vector<double> load((size_t)n_dev, 0.0);
+    for (int i : order) {
+        int best = 0;
+        for (int d = 1; d < n_dev; d++)
+            if (load[(size_t)d] < load[(size_t)best]) best = d;
+        dev_of[i] = best;
+        load[(size_t)best] += work[i];
+    }
+}
+
+// gpuqo_b200_devices: 1 (default) the calling thread's current device; N > 1
+// the N devices from the current one on (wrapping around the visible ones);
+// 0 every visible device, the current one first
+int batch_devices(std::vector<int> &devs, std::string &err) {
+    int cur = 0, count = 0;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e == cudaSuccess) e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        err = std::string("device query: ") + cudaGetErrorString(e);
+        return GPUQO_B200_ERR_CUDA;
+    }
+    const int want = gpuqo_b200_devices <= 0 ? count : gpuqo_b200_devices;
+    devs.clear();
+    for (int j = 0; j < std::max(want, 1); j++) devs.push_back((cur + j) % std::max(count, 1));
+    return 0;
+}
+
+}  // namespace gqb
+
+extern "C" int gpuqo_b200_plan_shards(const double *work, int n_items, int n_devices, int *device_of_item) {
+    if (!work || !device_of_item || n_items < 0 || n_devices < 1) return GPUQO_B200_ERR_ARGS;
+    plan_shards(work, n_items, n_devices, device_of_item);
+    return GPUQO_B200_OK;
+}
+
 extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC **infos, int n_queries,
                                     QueryTreeC **out) {
     stats_reset();
@@ -841,17 +891,68 @@ extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *
         std::stable_sort(batched.begin(), batched.end(), [&](int a, int b) {
             return infos[a]->n_rels > infos[b]->n_rels;
         });
-        std::vector<const std::vector<uint32_t> *> blobs;
-        for (int i : batched) blobs.push_back(&prep[i].blob);
-        std::vector<std::vector<TreeNode>> nodes;
-        std::vector<double> wave_ms;
-        EngineStats st;
-        std::string err;
         const uint64_t budget = (uint64_t)std::max(gpuqo_b200_batch_memory_mb, 64) << 20;
-        int rc = engine_run_batch(blobs, budget, nodes, st, wave_ms, err);
-        if (rc) {
+        // the devices the batch is spread over (gpuqo_b200_devices), and each
+        // query's device by estimated work (longest first, least loaded)
+        std::vector<int> devs;
+        std::string err;
+        if (int rc = batch_devices(devs, err)) {
             set_error(rc, err);
             return rc;
+        }
+        std::vector<double> work(batched.size());
+        for (size_t j = 0; j < batched.size(); j++) work[j] = engine_work_estimate(prep[batched[j]].blob);
+        std::vector<int> shard(batched.size(), 0);
+        plan_shards(work.data(), (int)work.size(), (int)devs.size(), shard.data());
+        std::vector<std::vector<TreeNode>> nodes(batched.size());
+        std::vector<EngineStats> dst(devs.size());
+        std::vector<int> drc(devs.size(), 0);
+        std::vector<std::string> derr(devs.size());
+        // one host thread per device with queries; each runs its own waves
+        // on its own engines (queries keep their largest-first order)
+        auto run_shard = [&](size_t d) {
+            std::vector<const std::vector<uint32_t> *> blobs;
+            std::vector<size_t> idx;
+            for (size_t j = 0; j < batched.size(); j++)
+                if (shard[j] == (int)d) {
+                    blobs.push_back(&prep[batched[j]].blob);
+                    idx.push_back(j);
+                }
+            if (blobs.empty()) return;
+            if (devs.size() > 1) {
+                const cudaError_t e = cudaSetDevice(devs[d]);
+                if (e != cudaSuccess) {
+                    cudaGetLastError();
+                    drc[d] = GPUQO_B200_ERR_CUDA;
+                    derr[d] = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+                    return;
+                }
+            }
+            std::vector<std::vector<TreeNode>> dn;
+            std::vector<double> wave_ms;
+            drc[d] = engine_run_batch(blobs, budget, dn, dst[d], wave_ms, derr[d]);
+            if (!drc[d])
+                for (size_t q = 0; q < idx.size(); q++) nodes[idx[q]] = std::move(dn[q]);
+        };
+        if (devs.size() == 1) {
+            run_shard(0);
+        } else {
+            std::vector<std::thread> th;
+            for (size_t d = 0; d < devs.size(); d++) th.emplace_back(run_shard, d);
+            for (auto &t : th) t.join();
+        }
+        EngineStats st;
+        for (size_t d = 0; d < devs.size(); d++) {
+            if (drc[d]) {
+                set_error(drc[d], derr[d]);
+                return drc[d];
+            }
+            st.connected_sets += dst[d].connected_sets;
+            st.evaluated_pairs += dst[d].evaluated_pairs;
+            st.memo_bytes = std::max(st.memo_bytes, dst[d].memo_bytes);
+            st.device_ms = std::max(st.device_ms, dst[d].device_ms);   // devices run side by side
+            st.kernel_launches += dst[d].kernel_launches;
+            st.barrier_timeouts += dst[d].barrier_timeouts;
         }
         stats_add(st);
         t_stats.n_subproblems = (uint32_t)batched.size();

@@ -11,6 +11,10 @@
 // Sub-problems outside the batched kernel's scope (plain DPsub, very large
 // biconnected blocks) run one by one on the single-query engine.
 //
+// With gpuqo_b200_devices other than 1 the service has one such scheduler
+// (a lane) per device; a request is given to the lane with the fewest
+// requests in flight and all its exact DPs run there.
+//
 // Each plan is the one gpuqo_run returns for the same query and settings: the
 // sub-problems are identical, only the way they share the GPU differs.
 //
@@ -58,6 +62,7 @@ struct SubTask {
 
 struct Request {
     uint64_t id;
+    int lane = 0;                      // the device lane that runs its exact DPs
     PlannerHandle *planner = nullptr;
     Clock::time_point t_submit, t_done;
     int rc = 0;
@@ -66,18 +71,35 @@ struct Request {
     std::thread th;
 };
 
+// One device of the service (gpuqo_b200_devices): its scheduler thread runs
+// the pending sub-problems of the requests given to this device.
+struct DevLane {
+    int device = 0;
+    std::deque<SubTask *> pending;
+    std::condition_variable cv;
+    std::thread th;
+    int load = 0;                      // requests given to this lane and not finished
+};
+
+// the lane for a new request: the one with the fewest requests in flight
+// (the lowest index on ties)
+static int pick_lane(const std::vector<std::unique_ptr<DevLane>> &lanes) {
+    int best = 0;
+    for (int i = 1; i < (int)lanes.size(); i++)
+        if (lanes[(size_t)i]->load < lanes[(size_t)best]->load) best = i;
+    return best;
+}
+
 class Server {
 public:
-    int device = 0;
     int max_inflight = 16;
     uint64_t wave_bytes = 32ull << 30;
     bool ccc = true;
 
     std::mutex mu;
-    std::condition_variable cv_sched, cv_sub, cv_req;
-    std::deque<SubTask *> pending;
+    std::condition_variable cv_sub, cv_req;
+    std::vector<std::unique_ptr<DevLane>> lanes;
     bool stopping = false;
-    std::thread sched;
 
     std::map<uint64_t, std::unique_ptr<Request>> reqs;
     std::deque<Request *> waiting;   // submitted, no slot yet
@@ -89,16 +111,21 @@ public:
     double device_ms = 0.0, busy_ms = 0.0, starved_ms = 0.0;
 
     int start(std::string &err) {
-        if (cudaGetDevice(&device) != cudaSuccess) {
-            err = "cudaGetDevice failed";
-            return GPUQO_B200_ERR_CUDA;
+        std::vector<int> devs;
+        if (int rc = batch_devices(devs, err)) return rc;
+        for (int d : devs) {
+            lanes.emplace_back(new DevLane());
+            lanes.back()->device = d;
         }
-        sched = std::thread([this] { scheduler(); });
+        for (auto &ln : lanes) {
+            DevLane *l = ln.get();
+            l->th = std::thread([this, l] { scheduler(*l); });
+        }
         return 0;
     }
 
-    // exact DP of one sub-problem, through the scheduler (called by planners)
-    int solve(const HostInfo &h, DpMode mode, std::vector<TreeNode> &nodes, std::string &err) {
+    // exact DP of one sub-problem, through its lane's scheduler (called by planners)
+    int solve(int lane, const HostInfo &h, DpMode mode, std::vector<TreeNode> &nodes, std::string &err) {
         SubTask t;
         t.blob = build_blob(h);
         apply_dpsub_csg(t.blob, mode);
@@ -106,8 +133,8 @@ public:
         t.n = h.n;
         {
             std::unique_lock<std::mutex> lk(mu);
-            pending.push_back(&t);
-            cv_sched.notify_one();
+            lanes[(size_t)lane]->pending.push_back(&t);
+            lanes[(size_t)lane]->cv.notify_one();
             cv_sub.wait(lk, [&] { return t.done; });
         }
         if (t.rc) {
@@ -118,15 +145,16 @@ public:
         return 0;
     }
 
-    void scheduler() {
-        cudaSetDevice(device);
+    void scheduler(DevLane &ln) {
+        cudaSetDevice(ln.device);
+        std::deque<SubTask *> &pending = ln.pending;
         for (;;) {
             std::vector<SubTask *> tasks;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                const bool open = running > 0;
+                const bool open = ln.load > 0;
                 const Clock::time_point t_wait = Clock::now();
-                cv_sched.wait(lk, [&] { return stopping || !pending.empty(); });
+                ln.cv.wait(lk, [&] { return stopping || !pending.empty(); });
                 if (open) starved_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_wait).count();
                 if (stopping && pending.empty()) return;
                 // admit pending sub-problems while the wave's memory fits
@@ -189,7 +217,7 @@ public:
         r->started = true;
         running++;
         r->th = std::thread([this, r] {
-            cudaSetDevice(device);
+            cudaSetDevice(lanes[(size_t)r->lane]->device);
             std::string err;
             int rc = planner_run(r->planner, err);
             std::lock_guard<std::mutex> lk(mu);
@@ -198,6 +226,7 @@ public:
             r->t_done = Clock::now();
             r->done = true;
             running--;
+            lanes[(size_t)r->lane]->load--;
             completed++;
             if (!waiting.empty()) {
                 Request *nx = waiting.front();
@@ -209,14 +238,23 @@ public:
     }
 
     int submit(int algorithm, const GpuqoPlannerInfoC *info, uint64_t *ticket, std::string &err) {
-        SubSolver solver = [this](const HostInfo &h, DpMode m, std::vector<TreeNode> &nodes, std::string &e) {
-            return solve(h, m, nodes, e);
-        };
         auto r = std::make_unique<Request>();
         r->t_submit = Clock::now();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            r->lane = pick_lane(lanes);
+            lanes[(size_t)r->lane]->load++;
+        }
+        const int lane = r->lane;
+        SubSolver solver = [this, lane](const HostInfo &h, DpMode m, std::vector<TreeNode> &nodes, std::string &e) {
+            return solve(lane, h, m, nodes, e);
+        };
         r->planner = planner_new(algorithm, info, gpuqo_idp_n_iters, gpuqo_idp_type, solver, err);
-        if (!r->planner) return GPUQO_B200_ERR_ARGS;
         std::lock_guard<std::mutex> lk(mu);
+        if (!r->planner) {
+            lanes[(size_t)lane]->load--;
+            return GPUQO_B200_ERR_ARGS;
+        }
         r->id = next_id++;
         *ticket = r->id;
         Request *raw = r.get();
@@ -285,9 +323,10 @@ public:
         {
             std::lock_guard<std::mutex> lk(mu);
             stopping = true;
-            cv_sched.notify_all();
+            for (auto &ln : lanes) ln->cv.notify_all();
         }
-        if (sched.joinable()) sched.join();
+        for (auto &ln : lanes)
+            if (ln->th.joinable()) ln->th.join();
     }
 };
 
