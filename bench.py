@@ -346,10 +346,17 @@ def batched_section(seed=7):
             same = same and capi.same_plan(capi.tree_to_py(r), tb)
             L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
         dtp = time.perf_counter() - t
+        hand = st.get("handoff_device_ms", 0.0)
         res[tag] = {"queries": len(qs), "batched_runs": len(runs), "batched_qps": len(qs) / dtb,
                     "plain_qps": len(qs) / dtp,
                     "speedup": dtp / dtb, "batched_device_ms": st["device_ms"],
-                    "batched_launches": st["kernel_launches"], "identical_plans": same}
+                    "batched_launches": st["kernel_launches"], "identical_plans": same,
+                    # the queries that fill the GPU alone run in the same
+                    # single-query kernel in both arms: no batching can make the
+                    # batch faster than their device time, so plain time over
+                    # it bounds the speedup
+                    "handoff_device_ms": hand,
+                    "speedup_bound": (dtp * 1000.0 / hand) if hand > 0 else None}
     return {"workload": "4096 MPDP queries, shapes 40% star / 40% snowflake / 10% chain / 10% cycle, "
                         "relation counts uniform in the range (n8_28: the full [8,28] mix; n8_16: small queries)",
             "arms": "batched = gpuqo_b200_run_batch of all queries (waves of one cooperative launch each); "
@@ -441,7 +448,12 @@ def served_section(n_req=48, seed=5):
                 "plain_fifo_same_plans": plain_same[0],
                 "identical_plans": all(x[0] == 0 and capi.same_plan(x[1], p) for x, p in zip(res, plain)),
                 "waves": st["waves"], "batched_subproblems": st["batched_subproblems"],
-                "device_ms": st["device_ms"], "busy_ms": st["busy_ms"], "starved_ms": st["starved_ms"]})
+                "device_ms": st["device_ms"], "busy_ms": st["busy_ms"], "starved_ms": st["starved_ms"],
+                # the service runs the same exact DPs on the device; at best it
+                # hides all host work behind them, so the plain service time over
+                # the device time per request bounds its gain
+                "speedup_bound": (res_t["plain_mean_service_ms"] * n_req / st["device_ms"])
+                                 if st["device_ms"] > 0 else None})
         out["by_idp_type"][tag] = res_t
     capi.set_int(L, "gpuqo_idp_n_iters", 0)
     capi.set_int(L, "gpuqo_idp_type", capi.GPUQO_IDP2)
@@ -558,17 +570,22 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     e2e_value = whole_job_ms_per_query(e2e_ms, args.steps, world)
-    # bytes crossing the bus per step: the planner-info blob in (header 339
-    # words, 2 words per class, its selectivities, 9 words per class member,
-    # the per-relation class masks, the 3 n^2 tree tables of a tree-shaped
-    # graph; staged in 512-word
-    # buckets); out, one copy of the engine's control block: 33 level counters
-    # (24 B), the pair counter, the barrier words, the tree size, 64 plan nodes (28 B)
+    # bytes crossing the bus per step: the planner-info blob in (the layout of
+    # csrc/dp_layout.h: a 343-word header, 2 words per class, its
+    # selectivities, 9 words per class member, then 16-byte aligned the
+    # per-relation class masks (rows of whole 4-word groups), 2 pair
+    # selectivities per class (rounded up to 4 words) and the plain-class
+    # mask, plus the 3 n^2 tree tables of a tree-shaped graph; staged in
+    # 512-word buckets); out, one copy of the engine's control block: 33 level
+    # counters (24 B), the pair counter, the barrier words, the tree size, 64
+    # plan nodes (28 B)
     q0 = qs[0]
     n_ec = len(q0.eq_classes)
     n_sels = sum(len(e.sels) for e in q0.eq_classes)
     n_fks = sum(len(e.members) for e in q0.eq_classes)
-    words = 339 + 2 * n_ec + n_sels + 9 * n_fks + N_RELS * ((n_ec + 31) // 32) + 3 * N_RELS * N_RELS
+    ec_stride = (((n_ec + 31) // 32) + 3) // 4 * 4
+    words = (343 + 2 * n_ec + n_sels + 9 * n_fks + 3) // 4 * 4
+    words += N_RELS * ec_stride + (2 * n_ec + 3) // 4 * 4 + ec_stride + 3 * N_RELS * N_RELS
     h2d = 4 * ((words + 511) // 512 * 512)
     d2h = 33 * 24 + 8 + 16 + 4 + 4 + 64 * 28
 

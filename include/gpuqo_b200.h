@@ -203,6 +203,7 @@ typedef struct GpuqoB200Stats {
     uint32_t kernel_launches;     /* kernels launched by the DP runs */
     uint32_t fallback_sets;       /* tree-mode sets re-evaluated in exact order (ties, NaN) */
     uint32_t barrier_timeouts;    /* persistent launches whose grid barrier gave up (rerun per level) */
+    double   handoff_device_ms;   /* batch: device time of the queries large enough to run alone */
 } GpuqoB200Stats;
 void gpuqo_b200_get_stats(GpuqoB200Stats *out);
 

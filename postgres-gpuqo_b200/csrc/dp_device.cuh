@@ -661,6 +661,44 @@ __device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_
     uint32_t win[4 * NW];
 #pragma unroll
     for (int w = 0; w < 4 * NW; w++) win[w] = match[w];
+    // every matching class plain (DevInfoView::plain): only the selectivities
+    // and the qual count depend on the classes; the bucket size is 0.1 and
+    // the MCV frequency 0 once any class matched, exactly what the general
+    // loop below computes for such classes
+    bool all_plain = !MASKED;
+    if (!MASKED) {
+        const uint4 *pl = reinterpret_cast<const uint4 *>(d.plain);
+#pragma unroll
+        for (int j = 0; j < NW; j++) {
+            const uint4 p4 = pl[j];
+            all_plain = all_plain && (match[4 * j] & ~p4.x) == 0u && (match[4 * j + 1] & ~p4.y) == 0u &&
+                        (match[4 * j + 2] & ~p4.z) == 0u && (match[4 * j + 3] & ~p4.w) == 0u;
+        }
+    }
+    if (all_plain) {
+#pragma unroll 1
+        for (int base = 0; base < 128 * NW; base += 32) {
+            for (uint32_t mm = win[0]; mm; mm &= mm - 1u) {
+                const int i = base + __ffs(mm) - 1;
+                const bool lo_left = (lowest(d.ec_relids[i]) & L) != 0u;
+                const float2 ps = *reinterpret_cast<const float2 *>(d.pair_sel + 2 * i);
+                lr.sel *= lo_left ? ps.x : ps.y;
+                rl.sel *= lo_left ? ps.y : ps.x;
+                per_tuple += h.cpu_operator_cost;
+                n_quals++;
+            }
+#pragma unroll
+            for (int w = 0; w + 1 < 4 * NW; w++) win[w] = win[w + 1];
+            win[4 * NW - 1] = 0u;
+        }
+        if (n_quals > 0) {
+            lr.bucketsize = rl.bucketsize = 0.1f;
+            lr.mcvfreq = rl.mcvfreq = 0.0f;
+        }
+        out_lr = side_finish<NW>(d, L, l, R, r, lr, n_quals, per_tuple, match);
+        out_rl = side_finish<NW>(d, R, r, L, l, rl, n_quals, per_tuple, match);
+        return;
+    }
 #pragma unroll 1
     for (int base = 0; base < (MASKED ? 32 : 128 * NW); base += 32) {
         for (uint32_t mm = win[0]; mm; mm &= mm - 1u) {

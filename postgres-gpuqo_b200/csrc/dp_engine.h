@@ -34,6 +34,7 @@ struct EngineStats {
     uint32_t kernel_launches = 0;
     uint32_t fallback_sets = 0;
     uint32_t barrier_timeouts = 0;     // persistent launches whose grid barrier gave up (rerun per level)
+    double handoff_ms = 0.0;           // device time of the batch's queries run alone (they fill the GPU)
 };
 
 // Runs one exact DP on the calling thread's current device.  `blob` is the

@@ -1820,8 +1820,9 @@ public:
             CK(cudaMallocHost(&h_blob, cap * 4));
             blob_cap_words = cap;
         }
-        if (n <= cap_n) return 0;
+        // the budget bounds what one DP needs, whatever the engine already holds
         if (int rc = over_budget(engine_bytes_needed(n), "the exact DP's dense memo and level lists", err)) return rc;
+        if (n <= cap_n) return 0;
         drop_graphs();
         cudaFree(a.memo);
         cudaFree(a.memo_left);
@@ -1855,12 +1856,12 @@ public:
     int dpsize_cap_n = -1;             // DPsize buffers sized for this many relations
 
     int ensure_dpsize(int n, std::string &err) {
-        if (n <= dpsize_cap_n) return 0;
         const uint64_t ms = max_level_sets(n);
         const uint64_t tiles = ms / kScanTile + 2;
         if (int rc = over_budget(engine_bytes_needed(n) + (1ull << n) * 4 + ms * 16 + tiles * 4,
                                  "DPsize's dense memo, level lists and place arrays", err))
             return rc;
+        if (n <= dpsize_cap_n) return 0;
         drop_graphs();
         cudaFree(a.pos);
         cudaFree(a.bmask);
@@ -3635,7 +3636,9 @@ int engine_run_batch(const std::vector<const std::vector<uint32_t> *> &blobs, ui
         }
         if (!eng) eng.reset(new Engine());
         const int n = reinterpret_cast<const DevHeader *>(blobs[i]->data())->n;
+        const double before = st.device_ms;
         if (int rc = eng->run(*blobs[i], n, kModeMpdp, true, false, out[i], st, err)) return rc;
+        st.handoff_ms += st.device_ms - before;
     }
     // tree-shaped queries first (waves of kb_dp<true>), then the others; the
     // order within each part is the caller's (largest first)

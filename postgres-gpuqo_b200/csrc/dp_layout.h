@@ -136,6 +136,11 @@ struct DevInfoView {
     // with x on the outer side (o = 0) or y there (o = 1); NaN for classes of
     // another size, which take the general path
     const float *pair_sel;
+    // plain[w] bit b: class 32 w + b has two members whose variables carry no
+    // statistics and no index (ndistinct unknown, MCV frequency 0): as the
+    // inner side of a join such a class always contributes the bucket-size
+    // estimate 0.1, the MCV frequency 0 and no unique index (ec_stride words)
+    const uint32_t *plain;
 };
 
 GQB_HD inline int ec_words(int n_ec) { return (n_ec + 31) / 32; }
@@ -162,11 +167,13 @@ GQB_HD inline DevInfoView make_view(const void *blob) {
     v.vars = reinterpret_cast<const DevVar *>(p);
     v.rel_ecs = reinterpret_cast<const uint32_t *>(v.h) + rel_ecs_offset(v.h->n_ec, v.h->n_sels, v.h->n_fks);
     v.pair_sel = reinterpret_cast<const float *>(v.rel_ecs + v.h->n * ec_stride(v.h->n_ec));
+    v.plain = reinterpret_cast<const uint32_t *>(v.pair_sel + ((2 * v.h->n_ec + 3) & ~3));
     return v;
 }
 
 GQB_HD inline uint32_t blob_words_for(int n, int n_ec, int n_sels, int n_fks) {
-    return rel_ecs_offset(n_ec, n_sels, n_fks) + (uint32_t)(n * ec_stride(n_ec) + 2 * n_ec);
+    return rel_ecs_offset(n_ec, n_sels, n_fks) + (uint32_t)(n * ec_stride(n_ec) + ((2 * n_ec + 3) & ~3) +
+                                                            ec_stride(n_ec));
 }
 
 // fills DevInfoView::rel_ecs from the class member masks (compact bits)
@@ -182,7 +189,8 @@ GQB_HD inline void fill_rel_ecs(const DevInfoView &v, int n) {
         }
 }
 
-// fills DevInfoView::pair_sel and DevHeader::all_pairs from the class arrays
+// fills DevInfoView::pair_sel, DevInfoView::plain and DevHeader::all_pairs
+// from the class arrays
 // and DevHeader::fksel (after those are written): ec_selectivity
 // (gpuqo_row_estimation.cuh:49-88) of a two-member class {x < y} is the FK
 // selectivity of the outer member's key into the inner one, else of the
@@ -192,6 +200,7 @@ GQB_HD inline void fill_rel_ecs(const DevInfoView &v, int n) {
 GQB_HD inline void fill_pair_sel(const DevInfoView &v) {
     DevHeader *h = const_cast<DevHeader *>(v.h);
     float *ps = const_cast<float *>(v.pair_sel);
+    for (int w = 0; w < ec_stride(h->n_ec); w++) const_cast<uint32_t *>(v.plain)[w] = 0u;
     uint32_t all = 1u;
     for (int i = 0; i < h->n_ec; i++) {
         const uint32_t rr = v.ec_relids[i];
@@ -214,6 +223,13 @@ GQB_HD inline void fill_pair_sel(const DevInfoView &v) {
         const float sel = v.sels[off_s];
         ps[2 * i] = fk_xy ? h->fksel[y] : (fk_yx ? h->fksel[x] : sel);
         ps[2 * i + 1] = fk_yx ? h->fksel[x] : (fk_xy ? h->fksel[y] : sel);
+        bool plain = true;
+        for (int j = 0; j < 2; j++) {
+            const DevVar &dv = v.vars[off_f + j];
+            plain = plain && (dv.flags & (1u | kVarMcvRatio)) == 0u && (dv.flags & kVarNoDistinct) != 0u &&
+                    dv.mcvfreq == 0.0f;
+        }
+        if (plain) const_cast<uint32_t *>(v.plain)[i / 32] |= 1u << (i % 32);
     }
     h->all_pairs = (h->n_ec > 0) ? all : 0u;
 }

@@ -110,6 +110,7 @@ void stats_add(const EngineStats &s) {
     t_stats.kernel_launches += s.kernel_launches;
     t_stats.fallback_sets += s.fallback_sets;
     t_stats.barrier_timeouts += s.barrier_timeouts;
+    t_stats.handoff_device_ms += s.handoff_ms;
     t_stats.n_subproblems += 1;
 }
 
@@ -953,6 +954,7 @@ extern "C" int gpuqo_b200_run_batch(int gpuqo_algorithm_arg, GpuqoPlannerInfoC *
             st.device_ms = std::max(st.device_ms, dst[d].device_ms);   // devices run side by side
             st.kernel_launches += dst[d].kernel_launches;
             st.barrier_timeouts += dst[d].barrier_timeouts;
+            st.handoff_ms += dst[d].handoff_ms;
         }
         stats_add(st);
         t_stats.n_subproblems = (uint32_t)batched.size();

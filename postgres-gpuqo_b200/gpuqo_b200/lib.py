@@ -27,7 +27,7 @@ class Stats(C.Structure):
                 ("device_ms", C.c_double), ("eval_kernel_ms", C.c_double),
                 ("eval_kernel_launches", C.c_uint32), ("n_subproblems", C.c_uint32),
                 ("kernel_launches", C.c_uint32), ("fallback_sets", C.c_uint32),
-                ("barrier_timeouts", C.c_uint32)]
+                ("barrier_timeouts", C.c_uint32), ("handoff_device_ms", C.c_double)]
 
     def to_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

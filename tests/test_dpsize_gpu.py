@@ -48,14 +48,19 @@ def test_dpsize_golden(case):
 
 
 def test_dpsize_same_optimum_as_dpsub():
-    """Both searches cover every csg-cmp pair: equal root cost."""
+    """Both searches cover every csg-cmp pair, so the root costs agree; not
+    always bit for bit: where two splits of a set tie on total cost, DPsize
+    and DPsub may keep different ones (different startup cost or rows), and
+    the costs above them then differ in the last bits.  Tolerance: 1e-6
+    relative."""
     for c in CASES:
         if c["idp_n_iters"]:
             continue
         a = lib.run(c["query"], capi.GPUQO_DPSIZE)
         b = lib.run(c["query"], capi.GPUQO_CPU_DPSUB)
         assert a.error == 0 and b.error == 0
-        assert a.tree[3] == b.tree[3] or (a.tree[3] != a.tree[3] and b.tree[3] != b.tree[3]), c["name"]
+        x, y = a.tree[3], b.tree[3]
+        assert (x != x and y != y) or abs(x - y) <= 1e-6 * max(abs(x), abs(y)), c["name"]
 
 
 def test_dpsize_batch_and_server():
