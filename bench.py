@@ -96,8 +96,10 @@ def measured_peaks():
 
 
 def profiled_traffic():
-    """DRAM bytes per k_dp_tree launch from the committed ncu summary, if any."""
-    p = os.path.join(REPO, "profiles", "k_dp_tree_snowflake25.md")
+    """DRAM bytes (read + write) per timed k_dp_tree launch, from the ncu
+    capture of this benchmark's own command (the four snowflake-25 seeds)
+    summarised in profiles/k_dp_tree_snowflake25_traffic.txt, if present."""
+    p = os.path.join(REPO, "profiles", "k_dp_tree_snowflake25_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -110,14 +112,43 @@ def profiled_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons sampled DURING the timed region: an
+    NVML poller thread reads them every 2 ms (the timed regions are only a
+    few milliseconds long); where NVML is not available, nvidia-smi every
+    100 ms.  Reading clocks changes no GPU setting."""
+
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.samples = []          # (sm_mhz, max_mhz, reasons bitmask)
+        self.stop = threading.Event()
+        self.t = None
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            hnd = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(hnd, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(hnd, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(hnd)
+                        self.samples.append((float(sm), float(mx), int(rs)))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.002)
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.samples = []
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
@@ -137,15 +168,24 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        elif self.t is not None:
+            self.t.join(timeout=2)
 
     def summary(self):
         sm, mx, reasons = [], [], set()
+        for s_mhz, m_mhz, bits in self.samples:
+            sm.append(s_mhz)
+            mx.append(m_mhz)
+            for nm, bit in self.REASONS:
+                if bits & bit:
+                    reasons.add(nm)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
@@ -162,7 +202,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def cpu_model():

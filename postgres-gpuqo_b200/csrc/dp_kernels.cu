@@ -1325,7 +1325,7 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
 // k_ovf_chunks / k_ovf_finalize: large sets split over all warps
 // ---------------------------------------------------------------------------
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_ovf_chunks(const uint32_t *__restrict__ blob, uint32_t blob_words, int k,
+__global__ void __launch_bounds__(kBlock, 3) k_ovf_chunks(const uint32_t *__restrict__ blob, uint32_t blob_words, int k,
                                                        LevelCounters *__restrict__ lc, const float4 *__restrict__ memo,
                                                        const uint32_t *__restrict__ ovf_set,
                                                        const uint32_t *__restrict__ ovf_P,
