@@ -128,3 +128,19 @@ def test_batch_plain_dpsub_rides_the_batch():
     for q, t in zip(qs, trees):
         want, _ = harness.run_port(q, 3)
         assert same_tree(t, want), q.name
+
+
+def test_batch_mix_8_28_sample_vs_oracle():
+    """A sample of the benchmark's own batched workload (4096 queries, shapes
+    40/40/10/10, relation counts uniform in [8, 28], seed 7): every 50th query
+    of at most 22 relations (stars of at most 19, whose oracle run grows as
+    2^n), batched together, against the oracle restatement of cpu_dpsub_bicc."""
+    qs = query.batch_mix(4096, seed=7, nmin=8, nmax=28)
+    eligible = [q for q in qs if q.n <= 22 and not (q.name.startswith("star") and q.n > 19)]
+    sample = eligible[::50]
+    assert len(sample) >= 40
+    trees, rc = lib.run_batch(sample, capi.GPUQO_DPSUB, bicc=True)
+    assert rc == 0
+    for q, t in zip(sample, trees):
+        want, _ = harness.run_port(q, 5)
+        assert same_tree(t, want), q.name

@@ -10,7 +10,10 @@ from gpuqo_b200 import query
 
 
 GOLDEN = load_golden()
-PORT_CASES = [c for c in GOLDEN if c["query"].n <= 20]
+# cases the plain-C port replays in seconds; the 18-relation clique (3^18
+# candidate splits, half an hour of single-threaded CPU) is checked against the
+# GPU only, the port's clique cases stop at 14 relations
+PORT_CASES = [c for c in GOLDEN if c["query"].n <= 20 and c["tag"] != "clique18"]
 
 
 @pytest.mark.parametrize("case", PORT_CASES, ids=[f'{c["tag"]}-{c["name"]}-a{c["algorithm"]}' for c in PORT_CASES])
