@@ -236,6 +236,17 @@ int gpuqo_b200_reset_persistent(void);
  * reported the same way. */
 extern int gpuqo_b200_device_memory_mb;
 
+/* Exact DPs (DPsub, MPDP) over at least this many relations use the sparse
+ * memo: the connected sets are enumerated on the host, an open-addressing
+ * table on the device maps each set to its memo slot, and one launch per
+ * level evaluates every set with 64-bit relation sets.  Default 32, the end of
+ * the dense memo (one entry per subset of up to 31 relations); the sparse memo
+ * reaches 63 relations when the graph has at most 2^25 connected sets and no
+ * set more than 2^26 candidate splits.  A lower value sends smaller queries
+ * the same way (their plans are the dense memo's, bit for bit); 0 or a value
+ * above 63 keeps the default. */
+extern int gpuqo_b200_sparse_from_rels;
+
 /*
  * Device-resident timing of the exact DP of one query (< 32 relations, no
  * IDP): the planner info is converted and uploaded once, then the captured DP

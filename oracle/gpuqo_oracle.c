@@ -32,8 +32,10 @@
  * is what the reference's host build does.
  *
  * Memo: dense, indexed by (relid mask >> 1), instead of the reference's
- * std::unordered_map; lookups are equivalent (a set is present iff it was
- * inserted).  Limited to n <= 28 relations.
+ * std::unordered_map, up to 28 relations; lookups are equivalent (a set is
+ * present iff it was inserted).  From 29 to 63 relations (or from
+ * oracle_sparse_from_rels on) a hash memo over the connected sets only, same
+ * visiting order and candidates (run_dp_sparse).
  */
 #include "gpuqo_oracle.h"
 
@@ -516,15 +518,12 @@ typedef struct {
 } Dp;
 
 /* gpuqo_cpu_common.cuh:169-211 (make_join_relation + do_join, strict '<') */
-static void dp_join(Dp *dp, mask_t left_id, mask_t right_id) {
-    const Info *info = dp->info;
-    MemoEntry *le = &dp->memo[left_id >> 1];
-    MemoEntry *re = &dp->memo[right_id >> 1];
+static void join_into(const Info *info, MemoEntry *je, mask_t left_id, const MemoEntry *le, mask_t right_id,
+                      const MemoEntry *re) {
     Rel jr;
     jr.rows = estimate_join_rows(info, left_id, &le->rel, right_id, &re->rel);
     jr.cost = calc_join_cost(info, left_id, &le->rel, right_id, &re->rel, jr.rows);
     jr.width = le->rel.width + re->rel.width;
-    MemoEntry *je = &dp->memo[(left_id | right_id) >> 1];
     if (je->present) {
         if (jr.cost.total < je->rel.cost.total) {
             je->rel = jr;
@@ -537,6 +536,11 @@ static void dp_join(Dp *dp, mask_t left_id, mask_t right_id) {
         je->left = left_id;
         je->right = right_id;
     }
+}
+
+static void dp_join(Dp *dp, mask_t left_id, mask_t right_id) {
+    join_into(dp->info, &dp->memo[(left_id | right_id) >> 1], left_id, &dp->memo[left_id >> 1], right_id,
+              &dp->memo[right_id >> 1]);
 }
 
 /* gpuqo_cpu_dpsub.cu:32-78 */
@@ -671,6 +675,291 @@ static Tree *run_dp(const Info *info, bool bicc) {
     for (int i = 0; i < n; i++) final_id |= info->base[i].id;
     Tree *t = build_tree(&dp, final_id);
     free(dp.memo);
+    return t;
+}
+
+/* ------------------------------------------------------------------------ */
+/* sparse memo: the same DP over the connected sets only (29 to 63 relations) */
+/* ------------------------------------------------------------------------ */
+/*
+ * The reference's memo is a std::unordered_map (gpuqo_cpu_sequential.cu:63)
+ * holding only the sets that were joined, and its non-IDP enumeration visits
+ * every subset in increasing integer order but skips those that are not
+ * connected (gpuqo_cpu_dpsub.cuh:26-40).  This driver visits exactly the
+ * connected sets, in the same increasing integer order, with a hash memo; the
+ * candidates of each set are the reference's, in the reference's order:
+ *   DPsub: every L of S, ascending (gpuqo_cpu_dpsub.cu:35-75), joined when
+ *          both L and S - L are present, i.e. connected; here the connected
+ *          subsets of S are listed and sorted, which is the same sequence;
+ *   MPDP:  per block of S in find_blocks order, every lb of the block
+ *          ascending, grown on both sides, joined when the sides cover S
+ *          (gpuqo_cpu_dpsub_bicc.cu:180-232).  For a block that is a simple
+ *          cycle of m >= 4 relations only the m(m - 1) arcs can cover S (a
+ *          non-contiguous lb grows to the part hanging off one of its arcs),
+ *          so the arcs are taken in ascending order and the other lb, which
+ *          join nothing, are skipped.  A block of more than 26 relations that
+ *          is not a cycle is refused (2^26 candidates per set).
+ * Bound: at most 2^24 connected sets.
+ */
+int oracle_sparse_from_rels = ORACLE_MAX_DENSE + 1;
+
+#define SPARSE_MAX_SETS (1u << 24)
+#define SPARSE_MAX_BLOCK 26
+
+typedef struct {
+    mask_t *keys;      /* 0 = empty slot (no set is empty) */
+    uint32_t *val;
+    uint32_t cap;      /* power of two */
+    uint32_t count;
+} SetMap;
+
+static uint32_t setmap_slot(mask_t k, uint32_t cap) {
+    return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 40) & (cap - 1u);
+}
+
+static bool setmap_init(SetMap *m, uint32_t want) {
+    m->cap = 16;
+    while (m->cap < 2u * want) m->cap <<= 1;
+    m->count = 0;
+    m->keys = (mask_t *)calloc(m->cap, sizeof(mask_t));
+    m->val = (uint32_t *)calloc(m->cap, sizeof(uint32_t));
+    return m->keys && m->val;
+}
+
+static void setmap_free(SetMap *m) {
+    free(m->keys);
+    free(m->val);
+}
+
+static long setmap_get(const SetMap *m, mask_t k) {
+    for (uint32_t i = setmap_slot(k, m->cap);; i = (i + 1u) & (m->cap - 1u)) {
+        if (m->keys[i] == k) return (long)m->val[i];
+        if (m->keys[i] == 0) return -1;
+    }
+}
+
+/* insert if absent; returns false when it was present (or on no memory) */
+static bool setmap_add(SetMap *m, mask_t k, uint32_t v) {
+    if (2u * (m->count + 1u) > m->cap) {
+        SetMap g;
+        g.cap = m->cap * 2u;
+        g.count = 0;
+        g.keys = (mask_t *)calloc(g.cap, sizeof(mask_t));
+        g.val = (uint32_t *)calloc(g.cap, sizeof(uint32_t));
+        if (!g.keys || !g.val) {
+            setmap_free(&g);
+            return false;
+        }
+        for (uint32_t i = 0; i < m->cap; i++)
+            if (m->keys[i]) setmap_add(&g, m->keys[i], m->val[i]);
+        setmap_free(m);
+        *m = g;
+    }
+    uint32_t i = setmap_slot(k, m->cap);
+    for (; m->keys[i]; i = (i + 1u) & (m->cap - 1u))
+        if (m->keys[i] == k) return false;
+    m->keys[i] = k;
+    m->val[i] = v;
+    m->count++;
+    return true;
+}
+
+typedef struct {
+    mask_t *v;
+    uint32_t n, cap;
+} MaskList;
+
+static bool masklist_push(MaskList *l, mask_t x) {
+    if (l->n == l->cap) {
+        uint32_t c = l->cap ? 2u * l->cap : 64u;
+        mask_t *nv = (mask_t *)realloc(l->v, (size_t)c * sizeof(mask_t));
+        if (!nv) return false;
+        l->v = nv;
+        l->cap = c;
+    }
+    l->v[l->n++] = x;
+    return true;
+}
+
+static int cmp_mask(const void *a, const void *b) {
+    const mask_t x = *(const mask_t *)a, y = *(const mask_t *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* the connected subsets of `within` (all of them when within is every
+ * relation), by extension with one neighbour at a time; false past `limit` */
+static bool connected_subsets(const Info *info, mask_t within, uint32_t limit, MaskList *out) {
+    SetMap seen;
+    if (!setmap_init(&seen, 64)) return false;
+    bool ok = true;
+    for (mask_t x = within; x && ok; x &= x - 1) {
+        ok = masklist_push(out, lowest(x)) && setmap_add(&seen, lowest(x), 0);
+    }
+    uint32_t lvl_start = 0;
+    while (ok && lvl_start < out->n) {
+        const uint32_t lvl_end = out->n;
+        for (uint32_t i = lvl_start; i < lvl_end && ok; i++) {
+            const mask_t S = out->v[i];
+            mask_t nb = 0;
+            for (mask_t x = S; x; x &= x - 1) nb |= info->edge[lowest_pos(x) - 1];
+            nb &= within & ~S;
+            for (; nb && ok; nb &= nb - 1) {
+                const mask_t T = S | lowest(nb);
+                if (setmap_get(&seen, T) >= 0) continue;
+                if (out->n >= limit) {
+                    ok = false;
+                    break;
+                }
+                ok = setmap_add(&seen, T, 0) && masklist_push(out, T);
+            }
+        }
+        lvl_start = lvl_end;
+    }
+    setmap_free(&seen);
+    return ok;
+}
+
+typedef struct {
+    const Info *info;
+    SetMap index;       /* set -> entry */
+    MemoEntry *memo;    /* in ascending set order */
+} SparseDp;
+
+static MemoEntry *sparse_entry(const SparseDp *dp, mask_t id) {
+    const long i = setmap_get(&dp->index, id);
+    return i < 0 ? NULL : &dp->memo[i];
+}
+
+static void sparse_join(SparseDp *dp, MemoEntry *je, mask_t left_id, mask_t right_id) {
+    const MemoEntry *le = sparse_entry(dp, left_id), *re = sparse_entry(dp, right_id);
+    if (le && re && le->present && re->present) join_into(dp->info, je, left_id, le, right_id, re);
+}
+
+static bool is_simple_cycle(const Info *info, mask_t block) {
+    if (popc(block) < 4) return false;
+    for (mask_t x = block; x; x &= x - 1)
+        if (popc(info->edge[lowest_pos(x) - 1] & block) != 2) return false;
+    return true;
+}
+
+/* MPDP candidates of one set (see above); false for an oversized block */
+static bool sparse_bicc_set(SparseDp *dp, MemoEntry *je, mask_t set) {
+    const Info *info = dp->info;
+    mask_t blocks[MAXN * 2];
+    const int nb = find_blocks(info, set, blocks);
+    for (int b = 0; b < nb; b++) {
+        const mask_t block = blocks[b];
+        const int m = popc(block);
+        if (is_simple_cycle(info, block)) {
+            /* walk the cycle from its lowest relation; arcs are contiguous runs */
+            mask_t order[MAXN];
+            int v = lowest_pos(block), prev = -1;
+            for (int i = 0; i < m; i++) {
+                order[i] = nth(v);
+                const mask_t nbrs = info->edge[v - 1] & block & ~(prev >= 0 ? nth(prev) : 0);
+                prev = v;
+                v = lowest_pos(nbrs);
+            }
+            mask_t arcs[MAXN * MAXN];
+            int na = 0;
+            for (int st = 0; st < m; st++) {
+                mask_t a = 0;
+                for (int len = 1; len < m; len++) {
+                    a |= order[(st + len - 1) % m];
+                    arcs[na++] = a;
+                }
+            }
+            qsort(arcs, (size_t)na, sizeof(mask_t), cmp_mask);
+            for (int i = 0; i < na; i++) {
+                const mask_t lb = arcs[i], rb = block & ~lb;
+                const mask_t left_id = grow(lowest(lb), set & ~rb, info->edge);
+                const mask_t right_id = grow(lowest(rb), set & ~lb, info->edge);
+                if ((left_id | right_id) == set) sparse_join(dp, je, left_id, right_id);
+            }
+            continue;
+        }
+        if (m > SPARSE_MAX_BLOCK) {
+            fprintf(stderr, "gpuqo_oracle: a block of %d relations exceeds the sparse driver\n", m);
+            return false;
+        }
+        mask_t lb = lowest(block);
+        while (lb != block) {
+            const mask_t rb = block & ~lb;
+            const mask_t left_id = grow(lowest(lb), set & ~rb, info->edge);
+            const mask_t right_id = grow(lowest(rb), set & ~lb, info->edge);
+            if ((left_id | right_id) == set) sparse_join(dp, je, left_id, right_id);
+            lb = next_subset(lb, block);
+        }
+    }
+    return true;
+}
+
+/* DPsub candidates of one set: its connected subsets, ascending */
+static bool sparse_dpsub_set(SparseDp *dp, MemoEntry *je, mask_t set) {
+    MaskList subs = {0};
+    if (!connected_subsets(dp->info, set, SPARSE_MAX_SETS, &subs)) {
+        free(subs.v);
+        return false;
+    }
+    qsort(subs.v, subs.n, sizeof(mask_t), cmp_mask);
+    for (uint32_t i = 0; i < subs.n; i++) {
+        const mask_t left_id = subs.v[i];
+        if (left_id == set) continue;
+        sparse_join(dp, je, left_id, set & ~left_id);
+    }
+    free(subs.v);
+    return true;
+}
+
+static Tree *build_tree_sparse(const SparseDp *dp, mask_t id) {
+    const MemoEntry *e = sparse_entry(dp, id);
+    if (!e || !e->present) return NULL;
+    Tree *t = (Tree *)calloc(1, sizeof(Tree));
+    t->id = id;
+    t->rows = e->rel.rows;
+    t->cost = e->rel.cost;
+    t->width = e->rel.width;
+    if (popc(id) > 1) {
+        t->left = build_tree_sparse(dp, e->left);
+        t->right = build_tree_sparse(dp, e->right);
+    }
+    return t;
+}
+
+static Tree *run_dp_sparse(const Info *info, bool bicc) {
+    const int n = info->n_rels;
+    mask_t full = 0;
+    for (int i = 0; i < n; i++) full |= info->base[i].id;
+    MaskList sets = {0};
+    if (!connected_subsets(info, full, SPARSE_MAX_SETS, &sets)) {
+        fprintf(stderr, "gpuqo_oracle: more than %u connected sets\n", SPARSE_MAX_SETS);
+        free(sets.v);
+        return NULL;
+    }
+    qsort(sets.v, sets.n, sizeof(mask_t), cmp_mask);
+    SparseDp dp;
+    dp.info = info;
+    dp.memo = (MemoEntry *)calloc(sets.n, sizeof(MemoEntry));
+    Tree *t = NULL;
+    bool ok = dp.memo && setmap_init(&dp.index, sets.n);
+    for (uint32_t i = 0; ok && i < sets.n; i++) ok = setmap_add(&dp.index, sets.v[i], i);
+    for (int i = 0; ok && i < n; i++) {
+        MemoEntry *e = sparse_entry(&dp, info->base[i].id);
+        e->present = true;
+        e->rel.rows = info->base[i].rows;
+        e->rel.cost = info->base[i].cost;
+        e->rel.width = info->base[i].width;
+        e->left = e->right = 0;
+    }
+    for (uint32_t i = 0; ok && i < sets.n; i++) {
+        const mask_t set = sets.v[i];
+        if (popc(set) < 2) continue;
+        ok = bicc ? sparse_bicc_set(&dp, &dp.memo[i], set) : sparse_dpsub_set(&dp, &dp.memo[i], set);
+    }
+    if (ok) t = build_tree_sparse(&dp, full);
+    if (dp.memo) setmap_free(&dp.index);
+    free(dp.memo);
+    free(sets.v);
     return t;
 }
 
@@ -851,13 +1140,14 @@ void oracle_free_query_tree(QueryTreeC *qt) {
 
 QueryTreeC *gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC *info_c) {
     if (gpuqo_algorithm != 3 && gpuqo_algorithm != 5) return NULL;
-    if (info_c->n_rels > ORACLE_MAX_DENSE || info_c->n_rels < 1) return NULL;
+    if (info_c->n_rels > MAXN - 1 || info_c->n_rels < 1) return NULL;
     Info info, remapped;
     convert_info(info_c, &info);
     int from_of_to[MAXN];
     int n_to = bfs_order(&info, from_of_to);
     remap_info(&info, &remapped, from_of_to, n_to);
-    Tree *t = run_dp(&remapped, gpuqo_algorithm == 5);
+    const bool sparse = n_to > ORACLE_MAX_DENSE || (oracle_sparse_from_rels > 0 && n_to >= oracle_sparse_from_rels);
+    Tree *t = sparse ? run_dp_sparse(&remapped, gpuqo_algorithm == 5) : run_dp(&remapped, gpuqo_algorithm == 5);
     QueryTreeC *res = tree_to_c(t, from_of_to, n_to);
     free_tree(t);
     free_info(&remapped);

@@ -71,6 +71,11 @@ typedef struct QueryTreeC {
 QueryTreeC *gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC *info);
 void oracle_free_query_tree(QueryTreeC *qt);
 
+/* Plans of at least this many relations use the hash memo over the connected
+ * sets (always from 29 relations on; up to 63).  Lower it to run small plans
+ * through that driver too. */
+extern int oracle_sparse_from_rels;
+
 
 /* One make_join_relation evaluation on the caller's (unrelabelled) info. */
 void oracle_eval_join(GpuqoPlannerInfoC *info, uint64_t left_id, uint64_t right_id,

@@ -15,9 +15,11 @@ enum DpMode : int {
     kModeDpsize = 2,  // DPsize (gpuqo_algorithm=dpsize): cpu_dpsize's level-list order and ties
 };
 
-// One node of the extracted plan, compact masks (bit i = relation i).
+// One node of the extracted plan, compact masks (bit i = relation i; the
+// dense-memo kernels write sets of up to 32 relations, the sparse exact DP of
+// 32 to 63 relations the full 64 bits).
 struct TreeNode {
-    uint32_t set;
+    uint64_t set;
     int32_t left, right;          // node indices, -1 for leaves
     float rows, startup, total;
     int32_t width;
@@ -66,6 +68,18 @@ double engine_work_estimate(const std::vector<uint32_t> &blob);
 void plan_shards(const double *work, int n, int n_dev, int *dev_of);
 int batch_devices(std::vector<int> &devs, std::string &err);
 uint64_t batch_query_bytes(int n);
+
+// Exact DP of 32 to 63 relations (MPDP, or plain DPsub on its valid pairs)
+// with the connected sets enumerated on the host and a device hash-table memo
+// (dp_wide.cu); sparse query graphs only (at most wide_set_capacity()
+// connected sets, else GPUQO_B200_ERR_TOO_LARGE).
+struct HostInfo;
+int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, EngineStats &st,
+                    std::string &err);
+uint64_t wide_set_capacity();
+// whether an exact DP of n relations in this mode runs on the sparse memo
+// (n > 31, or n >= gpuqo_b200_sparse_from_rels for DPsub and MPDP)
+bool use_sparse_memo(int n, DpMode mode);
 
 // Device-memory estimate (bytes) of one exact DP over n relations.
 uint64_t engine_bytes_needed(int n);

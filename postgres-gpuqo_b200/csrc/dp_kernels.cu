@@ -776,27 +776,21 @@ __device__ __forceinline__ void edge_next(const uint32_t *adj, uint32_t S, EdgeI
 // persistent kernels (the next edge's memo entries are requested before the
 // current edge is costed); at 64 registers (the 4-blocks persistent kernel and
 // the per-level kernel) it spills, and those keep the plain loop.
-// G == 0: a group width gw chosen at run time (1 .. 16, groups of gw lanes,
-// 32 / gw groups per warp and the warp's remaining lanes idle), reduced by
-// gathering the group's lanes instead of a butterfly; first_set / stride_sets
-// then count groups of that width.
 template <int G, bool MASKED, bool PIPE>
 __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first_set, uint32_t stride_sets,
                                             const uint32_t *sets, uint32_t count, int k, float4 *memo,
-                                            uint32_t *memo_left, unsigned long long &pairs, int gw = 0) {
+                                            uint32_t *memo_left, unsigned long long &pairs) {
     const DevHeader &h = *d.h;
     const int lane = threadIdx.x & 31;
-    const int Gw = (G == 0) ? gw : G;
-    const int grp = lane / Gw, gl = lane % Gw;
-    const bool lane_used = grp < 32 / Gw;
-    const uint32_t group_mask = (Gw == 32) ? kFull : (((1u << Gw) - 1u) << (grp * Gw));
+    const int grp = lane / G, gl = lane % G;
+    const uint32_t group_mask = (G == 32) ? kFull : (((1u << G) - 1u) << (grp * G));
     const uint32_t E = (uint32_t)(k - 1);                 // split edges of a k-set
-    const uint32_t per_lane = (E + Gw - 1u) / Gw;
+    const uint32_t per_lane = (E + G - 1u) / G;
     // plain-DPsub index of the mirror: pext(S - L, S) - 1 = 2^k - 3 - p
     const uint32_t mirror_base = (k >= 32 ? 0xFFFFFFFFu : ((1u << k) - 1u)) - 2u;
     for (uint32_t base = first_set; base < count; base += stride_sets) {
         const uint32_t i = base + (uint32_t)grp;
-        const bool has = lane_used && i < count;
+        const bool has = i < count;
         const uint32_t S = has ? __ldcg(sets + i) : 0u;
         EdgeIter it;
         it.vs = S;
@@ -863,7 +857,7 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         };
         if (G != 32 && !PIPE) {
             for (uint32_t j = 0; j < per_lane; j++) {
-                const uint32_t e = (uint32_t)gl + j * Gw;
+                const uint32_t e = (uint32_t)gl + j * G;
                 if (has && e < E) {
                     while (it.e <= e) edge_next(h.adj, S, it, a, b);
                     uint32_t L0, p0, p1, ecm;
@@ -877,7 +871,7 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
             bool cact = false;
             auto fetch = [&](uint32_t j, uint32_t &L0, uint32_t &p0, uint32_t &p1, uint32_t &ecm, float4 &lv,
                              float4 &rv) -> bool {
-                const uint32_t e = (uint32_t)gl + j * Gw;
+                const uint32_t e = (uint32_t)gl + j * G;
                 if (!(has && e < E)) return false;
                 while (it.e <= e) edge_next(h.adj, S, it, a, b);
                 decode(L0, p0, p1, ecm);
@@ -901,7 +895,7 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
             }
         } else {
             for (uint32_t j = 0; j < per_lane; j++) {
-                const uint32_t e = (uint32_t)gl + j * Gw;
+                const uint32_t e = (uint32_t)gl + j * G;
                 const bool active = has && e < E;
                 // smallest lane t with scan_t > e (every lane takes part in the shuffles)
                 int lo = 0;
@@ -923,33 +917,16 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
             }
         }
         uint32_t kh = (uint32_t)(best.key >> 32), kl = (uint32_t)best.key, fp = best.first_p;
-        if (G == 0) {
-            // every lane reads its group's other lanes (sources inside its
-            // own group; idle lanes read lanes of their partial group)
-            const uint32_t h0 = kh, l0 = kl, f0 = fp;
-            for (int j = 1; j < Gw; j++) {
-                const int src = (grp * Gw + (gl + j) % Gw) & 31;
-                const uint32_t oh = __shfl_sync(kFull, h0, src);
-                const uint32_t ol = __shfl_sync(kFull, l0, src);
-                const uint32_t of = __shfl_sync(kFull, f0, src);
-                if (oh < kh || (oh == kh && ol < kl)) {
-                    kh = oh;
-                    kl = ol;
-                }
-                if (of < fp) fp = of;
-            }
-        } else {
 #pragma unroll
-            for (int off = G / 2; off >= 1; off >>= 1) {
-                uint32_t oh = __shfl_xor_sync(kFull, kh, off);
-                uint32_t ol = __shfl_xor_sync(kFull, kl, off);
-                uint32_t of = __shfl_xor_sync(kFull, fp, off);
-                if (oh < kh || (oh == kh && ol < kl)) {
-                    kh = oh;
-                    kl = ol;
-                }
-                if (of < fp) fp = of;
+        for (int off = G / 2; off >= 1; off >>= 1) {
+            uint32_t oh = __shfl_xor_sync(kFull, kh, off);
+            uint32_t ol = __shfl_xor_sync(kFull, kl, off);
+            uint32_t of = __shfl_xor_sync(kFull, fp, off);
+            if (oh < kh || (oh == kh && ol < kl)) {
+                kh = oh;
+                kl = ol;
             }
+            if (of < fp) fp = of;
         }
         const bool nan_first = has && best.first_p == fp && best.first_nan;
         const unsigned nm = __ballot_sync(kFull, nan_first) & group_mask;
@@ -963,34 +940,6 @@ __device__ __forceinline__ void tree_groups(const DevInfoView &d, uint32_t first
         }
         pairs += best.n_valid;
     }
-}
-
-// Lanes per set of a tree level (count sets of k relations, k - 1 split
-// edges each) for the persistent tree kernel: the width that ends the level
-// soonest when every group walks its edges one after the other, counting
-// whole rounds of groups over the grid and one edge's time per round for
-// loading the set.  Widths 1 .. 16 run with any group size (G == 0 in
-// tree_groups); 32 (one set per warp, the cooperative edge index) is taken
-// when it is at least as fast.
-__device__ __forceinline__ int tree_group_width(uint32_t count, int k, uint32_t nwarps) {
-    const uint32_t E = (uint32_t)(k - 1);
-    uint64_t best_cost = ~0ull;
-    int best = 32;
-    const int gmax = E < 16u ? (int)E : 16;
-    for (int g = 1; g <= gmax; g++) {
-        const uint64_t groups = (uint64_t)nwarps * (uint64_t)(32 / g);
-        const uint64_t rounds = ((uint64_t)count + groups - 1) / groups;
-        const uint64_t cost = rounds * ((E + (uint32_t)g - 1u) / (uint32_t)g + 1u);
-        if (cost < best_cost) {
-            best_cost = cost;
-            best = g;
-        }
-    }
-    if (E <= 32u) {
-        const uint64_t rounds = ((uint64_t)count + nwarps - 1) / nwarps;
-        if (rounds * 2u <= best_cost) best = 32;   // one edge per lane plus the set load
-    }
-    return best;
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_eval_tree(const uint32_t *__restrict__ blob, uint32_t blob_words, int k,
@@ -1297,16 +1246,18 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
         uint32_t *nxt = (k & 1) ? setsA : setsB;
         const uint32_t count = __ldcg(&lvl[k].n_sets);
         if (k < n) level_sets_phase(adj, binom, st, n, k + 1, cur, count, nxt, lvl + k + 1);
-        // lanes take whole split edges (tree_groups): k - 1 per set, in
-        // groups of the width that ends the level soonest
-        const int G = tree_group_width(count, k, nwarps);
-        (void)target_lanes;
-        if (G < 32) {
-            const uint32_t gpw = 32u / (uint32_t)G;
-            if (masked)
-                tree_groups<0, true, kPipe>(d, gwarp * gpw, nwarps * gpw, cur, count, k, memo, memo_left, pairs, G);
-            else
-                tree_groups<0, false, kPipe>(d, gwarp * gpw, nwarps * gpw, cur, count, k, memo, memo_left, pairs, G);
+        // lanes take whole split edges (tree_groups): k - 1 per set
+        int max_group = 1;
+        while (max_group < 32 && max_group < k - 1) max_group <<= 1;
+        int G = 2;
+        while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
+        G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
+        if (G == 2) {
+            if (masked) tree_groups<2, true, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
+            else tree_groups<2, false, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
+        } else if (G == 8) {
+            if (masked) tree_groups<8, true, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
+            else tree_groups<8, false, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
         } else {
             if (masked) tree_groups<32, true, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
             else tree_groups<32, false, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);

@@ -1,0 +1,840 @@
+// dp_wide.cu - exact DP of 32 to 63 relations (after the BFS relabelling).
+//
+// The reference plans up to 63 relations exactly with 64-bit relation sets
+// and a hash-table memo (gpuqo_main_internal.cu:177-185, Bitmapset64;
+// gpuqo_hashtable.cuh:121-166).  The dense memo of the main engine stops at
+// 31 relations (2^n entries); beyond, only the connected sets are stored:
+//   * the host enumerates the connected sets level by level (extension by a
+//     neighbour, deduplicated) - the graphs planned exactly at this size are
+//     sparse, with thousands to millions of connected sets, and the count is
+//     checked against the memo's capacity before anything is allocated;
+//   * k_wide_insert builds a device open-addressing table (64-bit keys,
+//     atomicCAS, linear probing) from each set to its slot; the memo is
+//     indexed by slot: (rows, startup, total, width word) and the outer side;
+//   * per level, k_wide_eval costs every connected set with one warp: the
+//     set's biconnected blocks (the reference's DFS order), every candidate
+//     split of every block grown to a csg-cmp pair, both sides looked up in
+//     the table, join_eval_w's cost, and a warp reduction of
+//     (cost, enumeration index) with 64-bit indices - the MPDP index
+//     (gpuqo_cpu_dpsub_bicc.cu:46-236), or for plain DPsub the index of the
+//     split in cpu_dpsub's subset order (gpuqo_cpu_dpsub.cu:32-78), which
+//     selects the same first strict minimum over the valid pairs only.
+// The plan is read back from the memo on the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "dp_device.cuh"
+#include "dp_engine.h"
+#include "gpuqo_b200.h"
+#include "host_info.h"
+
+extern "C" int gpuqo_b200_device_memory_mb;
+
+namespace gqb {
+
+namespace {
+
+constexpr uint32_t kFullW = 0xFFFFFFFFu;
+constexpr int kWideBlock = 256;
+constexpr int kWideMaxRels = 63;
+constexpr uint64_t kWideMaxCandidates = 1ull << 24;   // candidate splits of one set
+constexpr uint64_t kWideMaxTotal = 1ull << 35;        // candidate splits of the whole DP
+
+// planner info on the device (global memory; read through the read-only path)
+struct WideInfo {
+    DevHeader h;                       // cost parameters (cost_nestloop / cost_hashjoin / memo_width_word)
+    int n, n_ec;
+    uint64_t composite;                // relations that are composite entries (IDP sub-problems)
+    uint64_t adj[64];
+    float rows[64], tuples[64], startup[64], total[64], fksel[64];
+    int width[64];
+    const uint64_t *ec_relids;         // [n_ec]
+    const uint32_t *ec_off;            // [n_ec] off_sels << 16 | off_fks
+    const float *sels;                 // [n_sels]
+    const uint64_t *fks;               // [n_fks]
+    const DevVar *vars;                // [n_fks]
+};
+
+__device__ __forceinline__ uint64_t lowest64(uint64_t x) { return x & (0ull - x); }
+__device__ __forceinline__ int lowest_idx64(uint64_t x) { return __ffsll((long long)x) - 1; }
+
+__device__ __forceinline__ uint64_t grow64(uint64_t from, uint64_t subset, const uint64_t *adj) {
+    uint64_t V = 0, N = from;
+    while (N) {
+        const int i = lowest_idx64(N);
+        V |= 1ull << i;
+        N = (N | adj[i]) & subset & ~V;
+    }
+    return V;
+}
+
+__device__ __forceinline__ uint64_t pdep64(uint64_t val, uint64_t mask) {
+    uint64_t r = 0;
+    while (mask && val) {
+        const uint64_t low = lowest64(mask);
+        if (val & 1ull) r |= low;
+        val >>= 1;
+        mask ^= low;
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint64_t pext64(uint64_t x, uint64_t mask) {
+    uint64_t r = 0;
+    for (; x; x &= x - 1ull) r |= 1ull << __popcll(mask & (lowest64(x) - 1ull));
+    return r;
+}
+
+// cpu_dpsub's index of the split (L, S - L): L = pdep(p + 1, S)
+__device__ __forceinline__ uint64_t dpsub_index64(uint64_t L, uint64_t S) { return pext64(L, S) - 1ull; }
+
+// biconnected blocks of S in the reference's DFS output order (find_blocks on
+// 64-bit sets); prefix: the reference's candidate indices (2^|b| - 2 per
+// block), eprefix: the enumerated ones (a simple cycle of m >= 4 relations
+// enumerates its m(m - 1) arcs)
+struct BlocksW {
+    int nb;
+    uint64_t cyc;
+    uint64_t mask[64];
+    uint64_t sub[64];
+    uint64_t prefix[65];
+    uint64_t eprefix[65];
+};
+
+__device__ void find_blocks64(uint64_t S, const uint64_t *adj, BlocksW &B) {
+    uint8_t disc[64], low[64], parent[64], stk_u[64], vstk[64];
+    uint64_t stk_e[64], desc[64];
+    int sp = 0, vsp = 0, t = 0;
+    uint64_t visited = 0;
+    B.nb = 0;
+    B.cyc = 0;
+    uint64_t total = 0, etotal = 0;
+    const int root = lowest_idx64(S);
+    visited |= 1ull << root;
+    disc[root] = (uint8_t)t++;
+    low[root] = 255;
+    parent[root] = 255;
+    desc[root] = 1ull << root;
+    vstk[vsp++] = (uint8_t)root;
+    stk_u[sp] = (uint8_t)root;
+    stk_e[sp] = adj[root] & S;
+    sp++;
+    while (sp > 0) {
+        const int u = stk_u[sp - 1];
+        const uint64_t e = stk_e[sp - 1];
+        if (e == 0) {
+            sp--;
+            if (sp > 0) {
+                const int p = stk_u[sp - 1];
+                if (low[u] >= disc[p]) {
+                    uint64_t blk = 1ull << p;
+                    int w;
+                    do {
+                        w = vstk[--vsp];
+                        blk |= 1ull << w;
+                    } while (w != u);
+                    const int m = __popcll(blk);
+                    bool cycle = m >= 4;
+                    for (uint64_t x = blk; cycle && x; x &= x - 1ull) cycle = __popcll(adj[lowest_idx64(x)] & blk) == 2;
+                    B.prefix[B.nb] = total;
+                    B.eprefix[B.nb] = etotal;
+                    if (cycle) B.cyc |= 1ull << B.nb;
+                    B.sub[B.nb] = desc[u];
+                    B.mask[B.nb++] = blk;
+                    // m <= 63 (at most 63 relations), and the blocks' sizes minus one
+                    // sum to |S| - 1, so both totals stay below 2^63
+                    total += (1ull << m) - 2ull;
+                    etotal += cycle ? (uint64_t)m * (uint64_t)(m - 1) : ((1ull << m) - 2ull);
+                }
+                if (low[u] < low[p]) low[p] = low[u];
+                desc[p] |= desc[u];
+                stk_e[sp - 1] &= ~(1ull << u);
+            }
+            continue;
+        }
+        const int v = lowest_idx64(e);
+        if (!((visited >> v) & 1ull)) {
+            visited |= 1ull << v;
+            parent[v] = (uint8_t)u;
+            disc[v] = (uint8_t)t++;
+            low[v] = 255;
+            desc[v] = 1ull << v;
+            vstk[vsp++] = (uint8_t)v;
+            stk_u[sp] = (uint8_t)v;
+            stk_e[sp] = adj[v] & S;
+            sp++;
+        } else {
+            if (parent[u] != v && disc[v] < disc[u]) {
+                if (disc[v] < low[u]) low[u] = disc[v];
+            }
+            stk_e[sp - 1] = e & ~(1ull << v);
+        }
+    }
+    B.prefix[B.nb] = total;
+    B.eprefix[B.nb] = etotal;
+}
+
+// arc j of a cycle block (see cached_arc): walk from the block's lowest
+// relation towards its lower neighbour; arc j starts at walk position
+// j / (m - 1) and has length j % (m - 1) + 1
+__device__ uint64_t cycle_arc64(uint64_t blk, const uint64_t *adj, uint64_t j) {
+    const uint32_t m = (uint32_t)__popcll(blk);
+    uint64_t pre[65];
+    int v = lowest_idx64(blk);
+    int prev = 63 - __clzll((long long)(adj[v] & blk));
+    pre[0] = 0ull;
+    for (uint32_t i = 0; i < m; i++) {
+        pre[i + 1] = pre[i] | (1ull << v);
+        const int nx = lowest_idx64(adj[v] & blk & ~(1ull << prev));
+        prev = v;
+        v = nx;
+    }
+    const uint64_t s = j / (m - 1u), e = s + j % (m - 1u) + 1u;
+    return e <= m ? (pre[e] ^ pre[s]) : ((pre[m] ^ pre[s]) | pre[e - m]);
+}
+
+// candidate c of S: its two sides and its index in the reference's MPDP order;
+// false when the grown sides do not cover S
+__device__ bool wide_candidate(uint64_t S, const BlocksW &B, const uint64_t *adj, uint64_t c, int &b, uint64_t &L,
+                               uint64_t &R, uint64_t &key) {
+    while (b + 1 < B.nb && B.eprefix[b + 1] <= c) b++;
+    const uint64_t blk = B.mask[b];
+    const uint64_t j = c - B.eprefix[b];
+    if (__popcll(blk) == 2) {
+        const uint64_t lo = lowest64(blk);
+        const uint64_t lb = (j == 0u) ? lo : (blk ^ lo);
+        const uint64_t sub = B.sub[b];
+        if (lb & sub) {
+            L = sub;
+            R = S ^ sub;
+        } else {
+            L = S ^ sub;
+            R = sub;
+        }
+        key = B.prefix[b] + j;
+        return true;
+    }
+    uint64_t lb;
+    if ((B.cyc >> b) & 1ull) {
+        lb = cycle_arc64(blk, adj, j);
+        key = B.prefix[b] + pext64(lb, blk) - 1ull;
+        if (blk == S) {
+            L = lb;
+            R = S ^ lb;
+            return true;
+        }
+    } else {
+        lb = pdep64(j + 1ull, blk);
+        key = B.prefix[b] + j;
+    }
+    const uint64_t rb = blk ^ lb;
+    L = grow64(lowest64(lb), S & ~rb, adj);
+    R = grow64(lowest64(rb), S & ~lb, adj);
+    return (L | R) == S;
+}
+
+// gpuqo_row_estimation.cuh:26-88 on 64-bit sets
+__device__ float fkselc_of_ec64(const WideInfo &w, int off_fk, uint64_t ec, uint64_t outer, uint64_t inner) {
+    for (uint64_t tmp = outer; tmp; tmp &= tmp - 1ull) {
+        const uint64_t out_id = lowest64(tmp);
+        const int out_idx = __popcll((out_id - 1ull) & ec);
+        const uint64_t match = inner & w.fks[off_fk + out_idx];
+        if (match) return w.fksel[lowest_idx64(match)];
+    }
+    return __int_as_float(0x7fffffff);
+}
+
+__device__ float ec_selectivity64(const WideInfo &w, int i, uint64_t ec, uint64_t ml, uint64_t mr) {
+    const uint32_t off = w.ec_off[i];
+    const int off_sels = (int)(off >> 16), off_fks = (int)(off & 0xFFFFu);
+    float fk = fkselc_of_ec64(w, off_fks, ec, ml, mr);
+    if (!isnan(fk)) return fk;
+    fk = fkselc_of_ec64(w, off_fks, ec, mr, ml);
+    if (!isnan(fk)) return fk;
+    const int size = __popcll(ec);
+    int il = __popcll((lowest64(ml) - 1ull) & ec);
+    int ir = __popcll((lowest64(mr) - 1ull) & ec);
+    if (il > ir) {
+        const int t = il;
+        il = ir;
+        ir = t;
+    }
+    return w.sels[off_sels + il * size - il * (il + 1) / 2 + (ir - il - 1)];
+}
+
+// join_eval_t's general path (every class, in class order) on 64-bit sets
+__device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, uint64_t R, const RelVal &r) {
+    const DevHeader &h = w.h;
+    const bool inner_single = (R & (R - 1ull)) == 0ull;
+    Htsz hz;
+    if (r.hz) {
+        hz.numbuckets = 1 << ((r.hz >> 1) & 31u);
+        hz.numbatches = 1 << (r.hz >> 6);
+    } else {
+        hz = exec_choose_hash_table_size(r.rows, r.width, h.work_mem);
+    }
+    const int nbuckets = f2i_x86((float)hz.numbuckets * (float)hz.numbatches);
+    float sel = 1.0f, per_tuple = 0.0f, bucketsize = 1.0f, mcvfreq = 1.0f;
+    int n_quals = 0;
+    bool inner_unique = false, any_index = false;
+    for (int i = 0; i < w.n_ec; i++) {
+        const uint64_t ec = w.ec_relids[i];
+        const uint64_t ml = ec & L, mr = ec & R;
+        if (!ml || !mr) continue;
+        sel *= ec_selectivity64(w, i, ec, ml, mr);
+        per_tuple += h.cpu_operator_cost;
+        n_quals++;
+        const int off_fks = (int)(w.ec_off[i] & 0xFFFFu);
+        bool first = true;
+        for (uint64_t m = mr; m; m &= m - 1ull) {
+            const uint64_t in_id = lowest64(m);
+            const DevVar v = w.vars[off_fks + __popcll((in_id - 1ull) & ec)];
+            if (first && inner_single) {
+                if ((v.flags & 1u) && (v.flags & 2u)) inner_unique = true;
+                if (v.flags & 1u) any_index = true;
+            }
+            first = false;
+            const float this_bs = bucketsize_one(v, nbuckets);
+            if (bucketsize > this_bs) bucketsize = this_bs;
+            if (mcvfreq > v.mcvfreq) mcvfreq = v.mcvfreq;
+        }
+    }
+    RelVal out;
+    const float rows = sel * l.rows * r.rows;
+    out.rows = rows > 1.0f ? roundf(rows) : 1.0f;
+    out.width = l.width + r.width;
+    Extra extra;
+    extra.inner_unique = inner_unique;
+    extra.indexed_join_quals = false;
+    extra.joinrows = out.rows;
+    extra.outer_match_frac = inner_unique ? out.rows / (l.rows * r.rows) : 0.0f;
+    extra.match_count = r.rows;
+    float min_s, min_t, s, t;
+    cost_nestloop(h, l, r.rows, r.startup, r.total, extra, per_tuple, min_s, min_t);
+    if (h.enable_hashjoin) {
+        cost_hashjoin(h, l, r, extra, n_quals, per_tuple, hz, bucketsize, mcvfreq, s, t);
+        if (t < min_t) {
+            min_s = s;
+            min_t = t;
+        }
+    }
+    if (any_index && !((w.composite >> lowest_idx64(R)) & 1ull)) {
+        extra.indexed_join_quals = true;
+        for (int i = 0; i < w.n_ec; i++) {
+            const uint64_t ec = w.ec_relids[i];
+            const uint64_t ml = ec & L, mr = ec & R;
+            if (!ml || !mr) continue;
+            const int off_fks = (int)(w.ec_off[i] & 0xFFFFu);
+            const DevVar v = w.vars[off_fks + __popcll((lowest64(mr) - 1ull) & ec)];
+            if (!(v.flags & 1u)) continue;
+            cost_nestloop(h, l, v.idx_rows, v.idx_startup, v.idx_total, extra, per_tuple, s, t);
+            if (t < min_t) {
+                min_s = s;
+                min_t = t;
+            }
+        }
+    }
+    out.startup = min_s;
+    out.total = min_t;
+    return out;
+}
+
+// open-addressing table from a connected set to its memo slot
+struct WideTable {
+    unsigned long long *keys;          // [cap], 0 = empty (no set is empty)
+    uint32_t *slot;                    // [cap]
+    uint32_t cap_log2;
+};
+
+__device__ __forceinline__ uint32_t wide_hash(uint64_t key, uint32_t cap_log2) {
+    return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - cap_log2));
+}
+
+__global__ void k_wide_insert(WideTable t, const unsigned long long *__restrict__ sets, uint32_t count,
+                              unsigned *__restrict__ err) {
+    const uint32_t cap = 1u << t.cap_log2;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const unsigned long long key = sets[i];
+        uint32_t pos = wide_hash(key, t.cap_log2);
+        bool done = false;
+        for (uint32_t probe = 0; probe < cap && !done; probe++, pos = (pos + 1u) & (cap - 1u)) {
+            const unsigned long long old = atomicCAS(t.keys + pos, 0ull, key);
+            if (old == 0ull || old == key) {
+                t.slot[pos] = i;
+                done = true;
+            }
+        }
+        if (!done) atomicExch(err, 1u);   // table full: cannot happen at half load
+    }
+}
+
+__device__ __forceinline__ uint32_t wide_lookup(const WideTable &t, uint64_t key, unsigned *err) {
+    const uint32_t cap = 1u << t.cap_log2;
+    uint32_t pos = wide_hash(key, t.cap_log2);
+    for (uint32_t probe = 0; probe < cap; probe++, pos = (pos + 1u) & (cap - 1u)) {
+        const unsigned long long k = __ldg(t.keys + pos);
+        if (k == key) return __ldg(t.slot + pos);
+        if (k == 0ull) break;
+    }
+    atomicExch(err, 2u);                  // a side that is not a connected set: cannot happen
+    return 0u;
+}
+
+__device__ __forceinline__ RelVal wide_rel(const float4 *memo, uint32_t slot, uint32_t packed) {
+    return unpack_rel(__ldcg(memo + slot), packed);
+}
+
+// one warp per connected set of level k (sets[first .. first + count))
+__global__ void __launch_bounds__(kWideBlock) k_wide_eval(const WideInfo *__restrict__ wi, WideTable t,
+                                                          const unsigned long long *__restrict__ sets, uint32_t first,
+                                                          uint32_t count, int index_order, float4 *__restrict__ memo,
+                                                          unsigned long long *__restrict__ memo_left,
+                                                          unsigned long long *__restrict__ pairs_out,
+                                                          unsigned *__restrict__ err) {
+    const WideInfo &w = *wi;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long pairs = 0;
+    BlocksW B;
+    for (uint32_t i = gwarp; i < count; i += nwarps) {
+        const uint64_t S = sets[first + i];
+        find_blocks64(S, w.adj, B);
+        const uint64_t P = B.eprefix[B.nb];
+        if (P > kWideMaxCandidates) {   // a dense block: far beyond what an exact DP at this size can afford
+            if (lane == 0) atomicExch(err, 3u);
+            continue;
+        }
+        // lane best: (ordered cost, index) lexicographic; first valid
+        // candidate (index, NaN) for the reference's NaN rule
+        uint32_t best_c = kFullW;
+        uint64_t best_k = ~0ull, first_k = ~0ull;
+        bool first_nan = false;
+        RelVal best_v, nan_v;
+        uint64_t best_l = 0, nan_l = 0;
+        int b = 0;
+        for (uint64_t c = (uint64_t)lane; c < P; c += 32u) {
+            uint64_t L, R, key;
+            if (!wide_candidate(S, B, w.adj, c, b, L, R, key)) continue;
+            if (index_order) key = dpsub_index64(L, S);
+            const RelVal l = wide_rel(memo, wide_lookup(t, L, err), w.h.hz_packed);
+            const RelVal r = wide_rel(memo, wide_lookup(t, R, err), w.h.hz_packed);
+            const RelVal out = join_eval_w(w, L, l, R, r);
+            const bool nan = isnan(out.total);
+            pairs++;
+            if (key < first_k) {
+                first_k = key;
+                first_nan = nan;
+                if (nan) {
+                    nan_v = out;
+                    nan_l = L;
+                }
+            }
+            if (!nan) {
+                const uint32_t oc = ord_float(out.total);
+                if (oc < best_c || (oc == best_c && key < best_k)) {
+                    best_c = oc;
+                    best_k = key;
+                    best_v = out;
+                    best_l = L;
+                }
+            }
+        }
+        // warp: minimum cost, then minimum index among it; first candidate
+        const uint32_t mc = __reduce_min_sync(kFullW, best_c);
+        const uint64_t kc = (best_c == mc) ? best_k : ~0ull;
+        const uint32_t kh = __reduce_min_sync(kFullW, (uint32_t)(kc >> 32));
+        const uint32_t kl = __reduce_min_sync(kFullW, (uint32_t)(kc >> 32) == kh ? (uint32_t)kc : kFullW);
+        const uint64_t mk = ((uint64_t)kh << 32) | kl;
+        const uint32_t fh = __reduce_min_sync(kFullW, (uint32_t)(first_k >> 32));
+        const uint32_t fl = __reduce_min_sync(kFullW, (uint32_t)(first_k >> 32) == fh ? (uint32_t)first_k : kFullW);
+        const uint64_t mf = ((uint64_t)fh << 32) | fl;
+        const bool nan_first = first_k == mf && first_nan && mf != ~0ull;
+        const unsigned nm = __ballot_sync(kFullW, nan_first);
+        const uint32_t slot = (lane == 0) ? wide_lookup(t, S, err) : 0u;
+        const uint32_t sslot = __shfl_sync(kFullW, slot, 0);
+        const RelVal *wv = nullptr;
+        uint64_t wl = 0;
+        if (nm) {
+            if (nan_first) {
+                wv = &nan_v;
+                wl = nan_l;
+            }
+        } else if (best_c == mc && best_k == mk && mc != kFullW) {
+            wv = &best_v;
+            wl = best_l;
+        }
+        if (wv) {
+            memo[sslot] = make_float4(wv->rows, wv->startup, wv->total,
+                                      __uint_as_float(memo_width_word(w.h, wv->rows, wv->width)));
+            memo_left[sslot] = wl;
+        }
+    }
+    for (int off = 16; off >= 1; off >>= 1) pairs += __shfl_xor_sync(kFullW, pairs, off);
+    if (lane == 0 && pairs) atomicAdd(pairs_out, pairs);
+}
+
+// candidate splits of every set of two or more relations, summed: the work
+// bound checked before the levels (a set above kWideMaxCandidates counts
+// beyond kWideMaxTotal on its own)
+__global__ void k_wide_work(const WideInfo *__restrict__ wi, const unsigned long long *__restrict__ sets,
+                            uint32_t count, unsigned long long *__restrict__ total) {
+    const WideInfo &w = *wi;
+    BlocksW B;
+    unsigned long long acc = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint64_t S = sets[i];
+        if (__popcll(S) < 2) continue;
+        find_blocks64(S, w.adj, B);
+        const uint64_t P = B.eprefix[B.nb];
+        acc += P > kWideMaxCandidates ? kWideMaxTotal + 1u : P;   // one such set refuses the DP
+    }
+    for (int off = 16; off >= 1; off >>= 1) acc += __shfl_xor_sync(kFullW, acc, off);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(total, acc);
+}
+
+__global__ void k_wide_base(const WideInfo *__restrict__ wi, WideTable t, float4 *__restrict__ memo,
+                            unsigned long long *__restrict__ memo_left, unsigned *__restrict__ err) {
+    const WideInfo &w = *wi;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w.n) return;
+    // gpuqo_cpu_sequential.cu:80-92: base relation memo entries
+    const uint32_t s = wide_lookup(t, 1ull << i, err);
+    memo[s] = make_float4(w.rows[i], w.startup[i], w.total[i],
+                          __uint_as_float(memo_width_word(w.h, w.rows[i], w.width[i])));
+    memo_left[s] = 0ull;
+}
+
+#define CKW(call)                                                                         \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+            cudaGetLastError();                                                           \
+            rc = (e_ == cudaErrorMemoryAllocation) ? GPUQO_B200_ERR_NOMEM : GPUQO_B200_ERR_CUDA; \
+            goto done;                                                                    \
+        }                                                                                 \
+    } while (0)
+
+}  // namespace
+
+uint64_t wide_set_capacity() { return 1ull << 25; }
+
+int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, EngineStats &st,
+                    std::string &err) {
+    const int n = info.n;
+    if (n < 1 || n > kWideMaxRels) {
+        err = "the sparse exact DP takes 1..63 relations";
+        return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    if (mode != kModeMpdp && mode != kModeDpsub) {
+        err = "beyond 31 relations the exact DP serves DPsub and MPDP only";
+        return GPUQO_B200_ERR_UNSUPPORTED;
+    }
+    if (info.ec_sels.size() >= 65536 || info.ec_fks.size() >= 65536) {
+        err = "too many equivalence-class entries";
+        return GPUQO_B200_ERR_ARGS;
+    }
+    // compact adjacency (relation i = bit i)
+    std::vector<uint64_t> adj(n);
+    for (int i = 0; i < n; i++) adj[i] = info.edge[i] >> 1;
+    // connected sets by level: extension of level k by a neighbour, deduplicated.
+    // Device bytes per set: key + slot at up to 4 table slots per set, the set,
+    // its memo entry and its left side; a device-memory budget lowers the cap.
+    constexpr uint64_t kBytesPerSet = 4 * 12 + 8 + 16 + 8;
+    uint64_t cap_sets = wide_set_capacity();
+    bool budget_bound = false;
+    if (gpuqo_b200_device_memory_mb > 0) {
+        const uint64_t by_budget = ((uint64_t)gpuqo_b200_device_memory_mb << 20) / kBytesPerSet;
+        if (by_budget < cap_sets) {
+            cap_sets = by_budget;
+            budget_bound = true;
+        }
+    }
+    auto too_many = [&]() {
+        if (budget_bound) {
+            err = "more than " + std::to_string(cap_sets) + " connected sets: beyond gpuqo_b200_device_memory_mb (" +
+                  std::to_string(gpuqo_b200_device_memory_mb) + " MB) for the sparse exact DP";
+            return GPUQO_B200_ERR_NOMEM;
+        }
+        err = "more than " + std::to_string(cap_sets) + " connected sets: beyond the sparse memo of the exact DP "
+              "(use IDP)";
+        return GPUQO_B200_ERR_TOO_LARGE;
+    };
+    std::vector<uint64_t> all;
+    std::vector<uint32_t> lvl_off(1, 0);
+    {
+        std::vector<uint64_t> cur;
+        for (int i = 0; i < n; i++) cur.push_back(1ull << i);
+        for (int k = 1; k <= n; k++) {
+            if (all.size() + cur.size() > cap_sets) return too_many();
+            std::sort(cur.begin(), cur.end());
+            all.insert(all.end(), cur.begin(), cur.end());
+            lvl_off.push_back((uint32_t)all.size());
+            if (k == n) break;
+            std::unordered_set<uint64_t> next;
+            next.reserve(cur.size() * 4);
+            for (uint64_t S : cur) {
+                uint64_t N = 0;
+                for (uint64_t x = S; x; x &= x - 1ull) N |= adj[__builtin_ctzll(x)];
+                N &= ~S;
+                for (; N; N &= N - 1ull) {
+                    next.insert(S | (N & (0ull - N)));
+                    if (all.size() + next.size() > cap_sets) return too_many();
+                }
+            }
+            cur.assign(next.begin(), next.end());
+        }
+    }
+    const uint64_t full = (n == 64) ? ~0ull : ((1ull << n) - 1ull);
+    if (all.back() != full) {
+        err = "query graph is not connected";
+        return GPUQO_B200_ERR_ARGS;
+    }
+    const uint32_t total = (uint32_t)all.size();
+    uint32_t cap_log2 = 1;
+    while ((1ull << cap_log2) < 2ull * total) cap_log2++;
+    const uint64_t cap = 1ull << cap_log2;
+    const size_t n_ec = info.ec_relids.size(), n_sels = info.ec_sels.size(), n_fks = info.ec_fks.size();
+    const uint64_t bytes = cap * 12ull + (uint64_t)total * (8 + 16 + 8) + n_ec * 12 + n_sels * 4 + n_fks * 40 +
+                           sizeof(WideInfo) + 64;
+    if (gpuqo_b200_device_memory_mb > 0 && bytes > ((uint64_t)gpuqo_b200_device_memory_mb << 20)) {
+        err = "the sparse exact DP needs " + std::to_string(bytes >> 20) + " MB of device memory; "
+              "gpuqo_b200_device_memory_mb allows " + std::to_string(gpuqo_b200_device_memory_mb);
+        return GPUQO_B200_ERR_NOMEM;
+    }
+    // planner info (host)
+    WideInfo hw;
+    std::memset(&hw, 0, sizeof(hw));
+    hw.n = n;
+    hw.n_ec = (int)n_ec;
+    hw.h.n = n;
+    hw.h.cpu_operator_cost = info.p.cpu_operator_cost;
+    hw.h.cpu_tuple_cost = info.p.cpu_tuple_cost;
+    hw.h.seq_page_cost = info.p.seq_page_cost;
+    hw.h.disable_cost = info.p.disable_cost;
+    hw.h.work_mem = info.p.work_mem;
+    hw.h.enable_nestloop = info.p.enable_nestloop ? 1 : 0;
+    hw.h.enable_hashjoin = info.p.enable_hashjoin ? 1 : 0;
+    long long width_sum = 0;
+    bool width_ok = true;
+    for (int i = 0; i < n; i++) {
+        width_sum += info.base[i].width;
+        width_ok = width_ok && info.base[i].width >= 0;
+        hw.adj[i] = adj[i];
+        hw.rows[i] = info.base[i].rows;
+        hw.tuples[i] = info.base[i].tuples;
+        hw.startup[i] = info.base[i].cost.startup;
+        hw.total[i] = info.base[i].cost.total;
+        hw.width[i] = info.base[i].width;
+        hw.fksel[i] = (float)(1.0 / (double)std::fmax(1.0f, info.base[i].tuples));
+        if (info.base[i].composite) hw.composite |= 1ull << i;
+    }
+    hw.h.hz_packed = (width_ok && width_sum < (1ll << kWidthBits)) ? 1u : 0u;
+    std::vector<uint64_t> h_relids(n_ec), h_fks(n_fks);
+    std::vector<uint32_t> h_off(n_ec);
+    std::vector<DevVar> h_vars(n_fks);
+    {
+        int off_sels = 0, off_fks = 0;
+        for (size_t e = 0; e < n_ec; e++) {
+            h_relids[e] = info.ec_relids[e] >> 1;
+            h_off[e] = ((uint32_t)off_sels << 16) | (uint32_t)off_fks;
+            int j = 0;
+            for (uint64_t m = h_relids[e]; m; m &= m - 1ull, j++) {
+                const int rel = __builtin_ctzll(m);
+                const int f = off_fks + j;
+                h_fks[f] = info.ec_fks[f] >> 1;
+                const VarInfo &vi = info.ec_vars[f];
+                DevVar &dv = h_vars[f];
+                std::memset(&dv, 0, sizeof(dv));
+                dv.idx_rows = vi.index.rows;
+                dv.idx_startup = vi.index.cost.startup;
+                dv.idx_total = vi.index.cost.total;
+                dv.flags = (vi.index.available ? 1u : 0u) | (vi.index.unique ? 2u : 0u);
+                devvar_bucket_terms(dv, vi.stats.stadistinct, vi.stats.stanullfrac, vi.stats.mcvfreq, hw.rows[rel],
+                                    hw.tuples[rel]);
+            }
+            off_sels += j * (j - 1) / 2;
+            off_fks += j;
+        }
+    }
+    int rc = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    WideInfo *d_info = nullptr;
+    uint64_t *d_relids = nullptr, *d_fks = nullptr;
+    uint32_t *d_off = nullptr, *d_slot = nullptr;
+    float *d_sels = nullptr;
+    DevVar *d_vars = nullptr;
+    unsigned long long *d_keys = nullptr, *d_sets = nullptr, *d_left = nullptr, *d_pairs = nullptr;
+    float4 *d_memo = nullptr;
+    unsigned *d_err = nullptr;
+    std::vector<float4> h_memo;
+    std::vector<uint64_t> h_left;
+    unsigned h_err = 0;
+    unsigned long long h_pairs = 0, h_work = 0;
+    uint32_t launches = 0;
+    float ms = 0.f;
+    int sm_count = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+    CKW(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CKW(cudaEventCreate(&ev0));
+    CKW(cudaEventCreate(&ev1));
+    CKW(cudaMalloc(&d_info, sizeof(WideInfo)));
+    CKW(cudaMalloc(&d_relids, std::max<size_t>(n_ec, 1) * 8));
+    CKW(cudaMalloc(&d_off, std::max<size_t>(n_ec, 1) * 4));
+    CKW(cudaMalloc(&d_sels, std::max<size_t>(n_sels, 1) * 4));
+    CKW(cudaMalloc(&d_fks, std::max<size_t>(n_fks, 1) * 8));
+    CKW(cudaMalloc(&d_vars, std::max<size_t>(n_fks, 1) * sizeof(DevVar)));
+    CKW(cudaMalloc(&d_keys, cap * 8));
+    CKW(cudaMalloc(&d_slot, cap * 4));
+    CKW(cudaMalloc(&d_sets, (size_t)total * 8));
+    CKW(cudaMalloc(&d_memo, (size_t)total * sizeof(float4)));
+    CKW(cudaMalloc(&d_left, (size_t)total * 8));
+    CKW(cudaMalloc(&d_pairs, 16));   // [0] evaluated pairs, [1] the work bound
+    CKW(cudaMalloc(&d_err, 4));
+    hw.ec_relids = d_relids;
+    hw.ec_off = d_off;
+    hw.sels = d_sels;
+    hw.fks = d_fks;
+    hw.vars = d_vars;
+    CKW(cudaMemcpyAsync(d_info, &hw, sizeof(WideInfo), cudaMemcpyHostToDevice, stream));
+    if (n_ec) {
+        CKW(cudaMemcpyAsync(d_relids, h_relids.data(), n_ec * 8, cudaMemcpyHostToDevice, stream));
+        CKW(cudaMemcpyAsync(d_off, h_off.data(), n_ec * 4, cudaMemcpyHostToDevice, stream));
+    }
+    if (n_sels) CKW(cudaMemcpyAsync(d_sels, info.ec_sels.data(), n_sels * 4, cudaMemcpyHostToDevice, stream));
+    if (n_fks) {
+        CKW(cudaMemcpyAsync(d_fks, h_fks.data(), n_fks * 8, cudaMemcpyHostToDevice, stream));
+        CKW(cudaMemcpyAsync(d_vars, h_vars.data(), n_fks * sizeof(DevVar), cudaMemcpyHostToDevice, stream));
+    }
+    CKW(cudaMemcpyAsync(d_sets, all.data(), (size_t)total * 8, cudaMemcpyHostToDevice, stream));
+    CKW(cudaMemsetAsync(d_keys, 0, cap * 8, stream));
+    CKW(cudaMemsetAsync(d_pairs, 0, 16, stream));
+    CKW(cudaMemsetAsync(d_err, 0, 4, stream));
+    {
+        WideTable t{d_keys, d_slot, cap_log2};
+        CKW(cudaEventRecord(ev0, stream));
+        const uint32_t ib = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8, (total + 255) / 256);
+        k_wide_insert<<<ib, 256, 0, stream>>>(t, d_sets, total, d_err);
+        k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
+        k_wide_work<<<ib, 256, 0, stream>>>(d_info, d_sets, total, d_pairs + 1);
+        launches += 3;
+        CKW(cudaGetLastError());
+        // refuse before the levels when the DP would evaluate too many splits
+        // (a large biconnected block that is not a cycle)
+        CKW(cudaMemcpyAsync(&h_work, d_pairs + 1, 8, cudaMemcpyDeviceToHost, stream));
+        CKW(cudaStreamSynchronize(stream));
+        if (h_work > kWideMaxTotal) {
+            err = "the sparse exact DP would evaluate more than " + std::to_string(h_work) +
+                  " candidate splits (a large biconnected block that is not a cycle; the bound is 2^35, 2^24 per "
+                  "set): use IDP";
+            rc = GPUQO_B200_ERR_TOO_LARGE;
+            goto done;
+        }
+        for (int k = 2; k <= n; k++) {
+            const uint32_t first = lvl_off[k - 1], count = lvl_off[k] - lvl_off[k - 1];
+            if (count == 0) continue;
+            launches++;
+            const uint32_t blocks = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8,
+                                                                 ((uint64_t)count * 32 + kWideBlock - 1) / kWideBlock);
+            k_wide_eval<<<blocks, kWideBlock, 0, stream>>>(d_info, t, d_sets, first, count,
+                                                           mode == kModeDpsub ? 1 : 0, d_memo, d_left, d_pairs,
+                                                           d_err);
+            CKW(cudaGetLastError());
+        }
+        CKW(cudaEventRecord(ev1, stream));
+    }
+    h_memo.resize(total);
+    h_left.resize(total);
+    CKW(cudaMemcpyAsync(h_memo.data(), d_memo, (size_t)total * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+    CKW(cudaMemcpyAsync(h_left.data(), d_left, (size_t)total * 8, cudaMemcpyDeviceToHost, stream));
+    CKW(cudaMemcpyAsync(&h_err, d_err, 4, cudaMemcpyDeviceToHost, stream));
+    CKW(cudaMemcpyAsync(&h_pairs, d_pairs, 8, cudaMemcpyDeviceToHost, stream));
+    CKW(cudaStreamSynchronize(stream));
+    CKW(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (h_err) {
+        err = h_err == 3 ? "a connected set with more than 2^24 candidate splits (a dense biconnected block): "
+                           "beyond the sparse exact DP (use IDP)"
+                         : "sparse memo table inconsistent";
+        rc = h_err == 3 ? GPUQO_B200_ERR_TOO_LARGE : GPUQO_B200_ERR_CUDA;
+        goto done;
+    }
+    {
+        // plan: walk the outer sides from the full set (host, sorted slots)
+        auto slot_of = [&](uint64_t s) -> uint32_t {
+            const int k = __builtin_popcountll(s);
+            auto b = all.begin() + lvl_off[k - 1], e = all.begin() + lvl_off[k];
+            return (uint32_t)(std::lower_bound(b, e, s) - all.begin());
+        };
+        const uint32_t wmask = hw.h.hz_packed ? kWidthMask : 0xFFFFFFFFu;
+        nodes.clear();
+        std::vector<std::pair<uint64_t, std::pair<int, int>>> stack;   // set, (parent, side)
+        stack.push_back({full, {-1, 0}});
+        while (!stack.empty() && nodes.size() < 2 * (size_t)n) {
+            const auto it = stack.back();
+            stack.pop_back();
+            const uint64_t s = it.first;
+            const uint32_t sl = slot_of(s);
+            const float4 v = h_memo[sl];
+            TreeNode t;
+            t.set = s;
+            t.left = t.right = -1;
+            t.rows = v.x;
+            t.startup = v.y;
+            t.total = v.z;
+            uint32_t wb;
+            std::memcpy(&wb, &v.w, 4);
+            t.width = (int32_t)(wb & wmask);
+            const int me = (int)nodes.size();
+            nodes.push_back(t);
+            if (it.second.first >= 0) {
+                if (it.second.second == 0) nodes[(size_t)it.second.first].left = me;
+                else nodes[(size_t)it.second.first].right = me;
+            }
+            const uint64_t l = h_left[sl] & s;
+            if (__builtin_popcountll(s) > 1 && l != 0 && l != s) {
+                stack.push_back({s ^ l, {me, 1}});
+                stack.push_back({l, {me, 0}});
+            }
+        }
+        if (nodes.size() != 2 * (size_t)n - 1) {
+            err = "plan extraction produced " + std::to_string(nodes.size()) + " nodes";
+            rc = GPUQO_B200_ERR_CUDA;
+            goto done;
+        }
+        st.connected_sets += total - (uint32_t)n;
+        st.evaluated_pairs += h_pairs;
+        st.memo_bytes = std::max<uint64_t>(st.memo_bytes, bytes);
+        st.device_ms += ms;
+        st.kernel_launches += launches;
+    }
+done:
+    cudaFree(d_info);
+    cudaFree(d_relids);
+    cudaFree(d_off);
+    cudaFree(d_sels);
+    cudaFree(d_fks);
+    cudaFree(d_vars);
+    cudaFree(d_keys);
+    cudaFree(d_slot);
+    cudaFree(d_sets);
+    cudaFree(d_memo);
+    cudaFree(d_left);
+    cudaFree(d_pairs);
+    cudaFree(d_err);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+    return rc;
+}
+
+}  // namespace gqb

@@ -85,6 +85,7 @@ int gpuqo_b200_persistent = 1;
 int gpuqo_b200_barrier_poll_limit = 0;
 int gpuqo_b200_device_memory_mb = 0;
 int gpuqo_b200_devices = 1;
+int gpuqo_b200_sparse_from_rels = 32;
 }
 
 namespace gqb {
@@ -511,11 +512,24 @@ std::vector<uint32_t> build_blob(const HostInfo &info) {
     return blob;
 }
 
-// Exact DP of a relabelled info with <= 31 relations on the GPU.
+bool use_sparse_memo(int n, DpMode mode) {
+    if (n > 31) return true;
+    const int from = gpuqo_b200_sparse_from_rels;
+    return from > 0 && from < 32 && n >= from && mode != kModeDpsize;
+}
+
+// Exact DP of a relabelled info on the GPU: up to 31 relations with the dense
+// memo, 32 to 63 with the sparse memo of the connected sets (dp_wide.cu).
 int exact_dp(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, std::string &err) {
-    if (info.n > 31) {
-        err = "exact DP over " + std::to_string(info.n) + " relations exceeds the dense-memo limit (31)";
+    if (info.n > 63) {
+        err = "exact DP over " + std::to_string(info.n) + " relations exceeds the 64-bit relation sets";
         return GPUQO_B200_ERR_TOO_LARGE;
+    }
+    if (use_sparse_memo(info.n, mode)) {
+        EngineStats st;
+        const int rc = engine_run_wide(info, mode, nodes, st, err);
+        if (rc == 0) stats_add(st);
+        return rc;
     }
     if (info.ec_sels.size() >= 65536 || info.ec_fks.size() >= 65536) {
         err = "too many equivalence-class entries";
@@ -593,7 +607,7 @@ static QueryTreeC *nodes_to_c(const std::vector<TreeNode> &nodes, int idx, const
     const TreeNode &t = nodes[idx];
     QueryTreeC *q = (QueryTreeC *)palloc(sizeof(QueryTreeC));
     mask64 orig = 0;
-    for (uint32_t x = t.set; x; x &= x - 1u) orig |= bit64(from_of_to[__builtin_ctz(x)] + 1);
+    for (uint64_t x = t.set; x; x &= x - 1ull) orig |= bit64(from_of_to[__builtin_ctzll(x)] + 1);
     q->id = make_bms(orig);
     q->left = nodes_to_c(nodes, t.left, from_of_to);
     q->right = nodes_to_c(nodes, t.right, from_of_to);

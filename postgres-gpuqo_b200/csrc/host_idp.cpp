@@ -8,9 +8,9 @@
 //   Remapper (composite relations, re-estimated classes)  gpuqo_remapper.cu:34-300
 //   makeBFSIndexRemapper                                   gpuqo_bfs_indexing.cu:14-55
 //   estimate_join_rows/selectivity on plan nodes           gpuqo_row_estimation.cuh:26-148
-// Every sub-problem (at most 31 relations after remapping) is solved by the
-// GPU engine through exact_dp(), without a BFS relabelling, as the reference
-// calls gpuqo_run_switch on the remapped info.
+// Every sub-problem (at most 63 relations after remapping; above 31 on the
+// sparse memo) is solved by the GPU engine through exact_dp(), without a BFS
+// relabelling, as the reference calls gpuqo_run_switch on the remapped info.
 //
 // The remapper's lookups, which the reference performs by scanning its list
 // of entries, use an owner table instead (entries partition the relations,
@@ -766,8 +766,7 @@ static QT *nodes_to_qt(const std::vector<TreeNode> &nodes, int idx, Arena &A) {
     if (idx < 0) return nullptr;
     const TreeNode &t = nodes[idx];
     QT *q = A.make();
-    for (int k = 0; k < 32; k++)
-        if (t.set & (1u << k)) q->id.set(k + 1);
+    for (uint64_t x = t.set; x; x &= x - 1ull) q->id.set(__builtin_ctzll(x) + 1);
     q->rows = t.rows;
     q->cost.startup = t.startup;
     q->cost.total = t.total;
@@ -1117,7 +1116,7 @@ struct Planner {
                 C.msg = "gpuqo_idp_type: only IDP2 and UNION are provided";
                 return GPUQO_B200_ERR_UNSUPPORTED;
             }
-        } else if (g.n <= 31) {
+        } else if (g.n <= 63) {
             if (C.cancelled()) {
                 C.msg = "cancelled before the exact DP";
                 return GPUQO_B200_ERR_CANCELLED;
@@ -1172,7 +1171,7 @@ QueryTreeC *run_planned(int algorithm, GpuqoPlannerInfoC *info_c) {
     std::string err;
     const int n = info_c->n_rels;
     const bool idp = gpuqo_idp_n_iters > 1 && gpuqo_idp_n_iters < n;
-    if (!idp && n > 31) {
+    if (!idp && n > 63) {
         set_error(GPUQO_B200_ERR_UNSUPPORTED,
                   std::to_string(n) + " relations need IDP (set gpuqo_idp_n_iters between 2 and n-1)");
         return nullptr;

@@ -47,6 +47,7 @@ extern "C" bool gpuqo_dpsub_ccc_enable;
 namespace gqb {
 
 void set_error(int code, const std::string &msg);
+int exact_dp(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, std::string &err);
 
 using Clock = std::chrono::steady_clock;
 
@@ -126,6 +127,12 @@ public:
 
     // exact DP of one sub-problem, through its lane's scheduler (called by planners)
     int solve(int lane, const HostInfo &h, DpMode mode, std::vector<TreeNode> &nodes, std::string &err) {
+        // sub-problems on the sparse memo (32 to 63 relations, or fewer under
+        // gpuqo_b200_sparse_from_rels) run directly on the request's thread
+        if (use_sparse_memo(h.n, mode)) {
+            cudaSetDevice(lanes[(size_t)lane]->device);
+            return exact_dp(h, mode, nodes, err);
+        }
         SubTask t;
         t.blob = build_blob(h);
         apply_dpsub_csg(t.blob, mode);

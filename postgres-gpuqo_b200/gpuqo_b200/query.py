@@ -296,6 +296,63 @@ def cycle(n: int, seed: int, rich: bool = False) -> Query:
                      _plain_edges(pairs, rng), rng, rich=rich)
 
 
+def _key_edges(pairs, lrows):
+    """Key joins: in each pair (a, b) a references b's primary key
+    (selectivity 1 / rows of b), so a path's row estimate stays that of its
+    first relation and long paths do not overflow float32."""
+    return [(a, b, 1.0 / f32(round(float(lrows[b]))), "a") for (a, b) in pairs]
+
+
+def key_chain(n: int, seed: int, rich: bool = False) -> Query:
+    """A chain of n relations joined on keys, each referencing the next."""
+    rng = np.random.default_rng([seed, 10, n])
+    lrows = _loguniform(rng, 1e2, 1e7, n)
+    lwidth = [int(w) for w in rng.integers(4, 65, n)]
+    pairs = [(a, a + 1) for a in range(n - 1)]
+    return _assemble(f"key_chain{n}_s{seed}", n, lrows, lwidth, _key_edges(pairs, lrows), rng, rich=rich)
+
+
+def key_cycle(n: int, seed: int, rich: bool = False) -> Query:
+    """A cycle of n relations joined on keys (one biconnected block)."""
+    rng = np.random.default_rng([seed, 11, n])
+    lrows = _loguniform(rng, 1e2, 1e7, n)
+    lwidth = [int(w) for w in rng.integers(4, 65, n)]
+    pairs = [(a, a + 1) for a in range(n - 1)] + [(n - 1, 0)]
+    return _assemble(f"key_cycle{n}_s{seed}", n, lrows, lwidth, _key_edges(pairs, lrows), rng, rich=rich)
+
+
+def ring_path(n: int, seed: int, rich: bool = False) -> Query:
+    """Rings of 4 to 6 relations alternating with paths of 4 to 8 relations
+    (biconnected blocks that are cycles, joined by bridges), key joins along
+    the way."""
+    rng = np.random.default_rng([seed, 12, n])
+    lrows = _loguniform(rng, 1e2, 1e7, n)
+    lwidth = [int(w) for w in rng.integers(4, 65, n)]
+    pairs = []
+    cur, nxt, ring = 0, 1, True
+    while nxt < n:
+        m = int(rng.integers(4, 7)) if ring else int(rng.integers(4, 9)) + 1
+        seg = list(range(nxt, min(n, nxt + m - 1)))
+        nxt += len(seg)
+        path = [cur] + seg
+        pairs += [(path[i], path[i + 1]) for i in range(len(path) - 1)]
+        if ring and len(seg) == m - 1:
+            pairs.append((path[-1], cur))
+        cur = seg[len(seg) // 2] if ring else seg[-1]
+        ring = not ring
+    return _assemble(f"ring_path{n}_s{seed}", n, lrows, lwidth, _key_edges(pairs, lrows), rng, rich=rich)
+
+
+def lollipop(n: int, seed: int, rich: bool = False) -> Query:
+    """A cycle of n // 3 relations with a path of the others hanging off it."""
+    rng = np.random.default_rng([seed, 13, n])
+    lrows = _loguniform(rng, 1e2, 1e7, n)
+    lwidth = [int(w) for w in rng.integers(4, 65, n)]
+    m = n // 3
+    pairs = [(a, a + 1) for a in range(m - 1)] + [(m - 1, 0), (0, m)] + [(a, a + 1) for a in range(m, n - 1)]
+    return _assemble(f"lollipop{n}_s{seed}", n, lrows, lwidth, _key_edges(pairs, lrows), rng, rich=rich)
+
+
 def random_graph(n: int, seed: int, extra_edge_p: float = 0.2,
                  rich: bool = False, equal: bool = False) -> Query:
     """A random connected graph: a random spanning tree plus extra edges with
@@ -361,7 +418,9 @@ def multi_member_classes(n: int, seed: int) -> Query:
 
 
 SHAPES = {"star": star, "snowflake": snowflake, "clique": clique,
-          "chain": chain, "cycle": cycle}
+          "chain": chain, "cycle": cycle, "key_chain": key_chain,
+          "key_cycle": key_cycle, "ring_path": ring_path,
+          "lollipop": lollipop}
 
 
 def make(shape: str, n: int, seed: int, **kw) -> Query:

@@ -19,10 +19,10 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: minutes-long case")
 
 
-def load_golden():
+def load_golden(name="cases.jsonl"):
     from gpuqo_b200.query import Query
     out = []
-    with open(GOLDEN) as f:
+    with open(os.path.join(REPO, "tests", "golden", name)) as f:
         for line in f:
             rec = json.loads(line)
             rec["query"] = Query.from_dict(rec["query"])

@@ -13,12 +13,15 @@ gpuqo_spanning_tree_enable set: the reference replaces the join graph by its
 minimum spanning tree before any algorithm runs (exact DP or IDP).
 ``dpsize_cases.jsonl`` (``--dpsize``) holds the plans of the reference's
 cpu_dpsize (algorithm code 2), the tie order the library's DPsize follows.
+``wide_cases.jsonl`` (``--wide``) holds cpu_dpccp (code 7) plans of 32 to 63
+relations, the optimum the sparse exact DP must reach.
 
 Usage (needs the reference library; run where the reference sources are):
     python tests/golden/make_golden.py            # small + full-size cases
     python tests/golden/make_golden.py --quick    # skip the minutes-long ones
     python tests/golden/make_golden.py --spanning # the spanning-tree fixtures
     python tests/golden/make_golden.py --dpsize   # the DPsize fixtures
+    python tests/golden/make_golden.py --wide     # the 32-63 relation fixtures
 """
 import argparse
 import json
@@ -113,6 +116,25 @@ def dpsize_cases():
     return out
 
 
+def wide_cases():
+    """(tag, query, algorithm, idp_n_iters, idp_type) of 32 to 63 relations,
+    planned by the reference's cpu_dpccp (code 7): the reference's only exact
+    DP that finishes at these sizes (its DPsub and MPDP visit all 2^n subsets
+    of the relations).  The fixtures pin the optimum (root rows and total
+    cost) of the sparse exact DP, whose tie order is DPsub's or MPDP's."""
+    DPCCP = 7
+    return [("wide_key_chain32", query.key_chain(32, 11), DPCCP, 0, 1),
+            ("wide_key_chain40", query.key_chain(40, 1), DPCCP, 0, 1),
+            ("wide_key_chain63", query.key_chain(63, 4), DPCCP, 0, 1),
+            ("wide_key_cycle40", query.key_cycle(40, 2), DPCCP, 0, 1),
+            ("wide_key_cycle48_rich", query.key_cycle(48, 8, rich=True), DPCCP, 0, 1),
+            ("wide_key_cycle63", query.key_cycle(63, 5), DPCCP, 0, 1),
+            ("wide_lollipop40", query.lollipop(40, 4), DPCCP, 0, 1),
+            ("wide_lollipop63_rich", query.lollipop(63, 7, rich=True), DPCCP, 0, 1),
+            ("wide_ring_path40", query.ring_path(40, 3), DPCCP, 0, 1),
+            ("wide_ring_path36_rich", query.ring_path(36, 10, rich=True), DPCCP, 0, 1)]
+
+
 def tree_json(t):
     if t is None:
         return None
@@ -125,11 +147,13 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "cases.jsonl"))
     ap.add_argument("--spanning", action="store_true", help="write spanning_cases.jsonl instead")
     ap.add_argument("--dpsize", action="store_true", help="write dpsize_cases.jsonl (cpu_dpsize) instead")
+    ap.add_argument("--wide", action="store_true", help="write wide_cases.jsonl (cpu_dpccp, 32-63 relations)")
     args = ap.parse_args()
     if not harness.ref_available():
         sys.exit("oracle/_ref/libgpuqo_ref.so missing: run `make -C oracle ref` first")
-    if args.spanning or args.dpsize:
-        fname, gen = ("spanning_cases.jsonl", spanning_cases) if args.spanning else ("dpsize_cases.jsonl", dpsize_cases)
+    if args.spanning or args.dpsize or args.wide:
+        fname, gen = (("spanning_cases.jsonl", spanning_cases) if args.spanning else
+                      ("wide_cases.jsonl", wide_cases) if args.wide else ("dpsize_cases.jsonl", dpsize_cases))
         with open(os.path.join(HERE, fname), "w") as f:
             for tag, q, alg, k, typ in gen():
                 t0 = time.time()

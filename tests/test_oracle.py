@@ -59,3 +59,41 @@ def test_generators_deterministic():
     assert q.n == 25 and len(q.eq_classes) == 24
     # connected, tree-shaped
     assert sum(len(e) for e in q.edges) == 2 * 24
+
+
+# the sparse driver (hash memo over the connected sets): the oracle at 29 to 63
+# relations, pinned to the reference's plans below that
+SPARSE_PIN = ([c for c in GOLDEN if c["query"].n <= 14 and not c["tag"].startswith("clique")][:40] +
+              [c for c in GOLDEN if c["tag"] in ("chain30", "cycle30", "chain30_bicc", "cycle30_bicc", "clique10")] +
+              [c for c in GOLDEN if c["tag"] == "snowflake25"][:1])
+
+
+@pytest.fixture
+def sparse_from():
+    import ctypes as C
+    lib = harness.load_port()
+    v = C.c_int.in_dll(lib, "oracle_sparse_from_rels")
+    old = v.value
+    yield lambda x: setattr(v, "value", x)
+    v.value = old
+
+
+def test_sparse_driver_matches_golden(sparse_from):
+    sparse_from(2)
+    for c in SPARSE_PIN:
+        tree, _ = harness.run_port(c["query"], c["algorithm"])
+        assert same_tree(tree, c["expected"]), (c["tag"], c["name"], c["algorithm"])
+
+
+WIDE = load_golden("wide_cases.jsonl")
+
+
+@pytest.mark.parametrize("case", WIDE, ids=[c["tag"] for c in WIDE])
+def test_sparse_driver_reaches_reference_dpccp_optimum(case):
+    """32 to 63 relations: the reference's cpu_dpccp optimum (root rows and
+    total cost) is what the oracle's DPsub and MPDP reach."""
+    ref = case["expected"]
+    for alg in (3, 5):
+        tree, _ = harness.run_port(case["query"], alg)
+        assert tree is not None
+        assert (tree[1], tree[3]) == (ref[1], ref[3]), (alg, tree[1:4], ref[1:4])

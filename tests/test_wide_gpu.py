@@ -1,0 +1,144 @@
+"""GPU parity of the sparse exact DP (the memo over connected sets only).
+
+Exact DPsub and MPDP beyond 31 relations (the end of the dense memo) run on
+the sparse memo: the connected sets are enumerated on the host, a device
+open-addressing table maps each to its memo slot, and one launch per level
+evaluates every set with 64-bit relation sets.  Checks:
+
+* forced onto the sparse memo (gpuqo_b200_sparse_from_rels = 2), every golden
+  case of up to 30 relations returns the reference's plan bit for bit, in
+  both tie orders (DPsub and MPDP);
+* at 32 to 63 relations the plan equals the oracle's (its sparse driver) bit
+  for bit, and the root's rows and total cost equal the optimum that the
+  reference's cpu_dpccp reaches on the same query (wide_cases.jsonl: the
+  reference's only exact DP that finishes at these sizes);
+* the sparse memo serves IDP sub-problems and the planner service;
+* limits end in a status, not a fault: too many connected sets
+  (GPUQO_B200_ERR_TOO_LARGE, or GPUQO_B200_ERR_NOMEM under a device-memory
+  budget), too many candidate splits (a large block that is not a cycle),
+  DPsize beyond 31 relations (GPUQO_B200_ERR_UNSUPPORTED).
+"""
+import ctypes as C
+
+import pytest
+
+from conftest import load_golden, same_tree
+
+import harness
+from gpuqo_b200 import capi, lib, query
+
+pytestmark = pytest.mark.gpu
+
+ERR_NOMEM, ERR_TOO_LARGE, ERR_UNSUPPORTED = 3, 4, 5
+
+SMALL = [c for c in load_golden() if c["query"].n <= 30]
+WIDE = load_golden("wide_cases.jsonl")
+
+
+@pytest.fixture
+def knob():
+    L = lib.load()
+    yield lambda name, v: capi.set_int(L, name, v)
+    capi.set_int(L, "gpuqo_b200_sparse_from_rels", 32)
+    capi.set_int(L, "gpuqo_b200_device_memory_mb", 0)
+
+
+def _run(q, alg, **kw):
+    return lib.run(q, capi.GPUQO_DPSUB, bicc=(alg == 5), **kw)
+
+
+@pytest.mark.parametrize("case", SMALL, ids=[f'{c["tag"]}-{c["name"]}-a{c["algorithm"]}' for c in SMALL])
+def test_sparse_memo_returns_golden_plans(case, knob):
+    knob("gpuqo_b200_sparse_from_rels", 2)
+    r = _run(case["query"], case["algorithm"])
+    assert r.error == 0, r.error
+    assert same_tree(r.tree, case["expected"])
+
+
+@pytest.mark.parametrize("alg", [3, 5])
+@pytest.mark.parametrize("case", WIDE, ids=[c["tag"] for c in WIDE])
+def test_wide_matches_oracle_and_reference_optimum(case, alg):
+    q = case["query"]
+    assert 32 <= q.n <= 63
+    r = _run(q, alg)
+    assert r.error == 0, r.error
+    want, _ = harness.run_port(q, alg)
+    assert same_tree(r.tree, want), (q.name, alg)
+    ref = case["expected"]
+    assert (r.tree[1], r.tree[3]) == (ref[1], ref[3]), (q.name, alg, r.tree[1:4], ref[1:4])
+    again = _run(q, alg)
+    assert same_tree(again.tree, r.tree)       # deterministic, and the scratch is reusable
+
+
+def test_wide_serves_idp_subproblems_and_the_service():
+    """IDP2 with 40-relation sub-problems on a 100-relation chain of key joins:
+    every sub-problem above 31 relations runs on the sparse memo; the plan
+    covers the relations and each join is the oracle's arithmetic of its
+    children.  The same request through the service returns the same plan."""
+    q = query.key_chain(100, 21)
+    r = lib.run(q, capi.GPUQO_DPSUB, bicc=True, idp_n_iters=40, idp_type=capi.GPUQO_IDP2)
+    assert r.error == 0
+    _check_arithmetic(q, r.tree)
+    srv = lib.Server(max_inflight=4, wave_memory_mb=1024)
+    try:
+        t = srv.submit(q, capi.GPUQO_DPSUB, bicc=True, idp_n_iters=40, idp_type=capi.GPUQO_IDP2)
+        wide = query.key_cycle(44, 22)
+        t2 = srv.submit(wide, capi.GPUQO_DPSUB, bicc=True, idp_n_iters=0, idp_type=capi.GPUQO_IDP2)
+        rc, tree, _ = srv.wait(t)
+        rc2, tree2, _ = srv.wait(t2)
+    finally:
+        srv.stop()
+    assert rc == 0 and same_tree(tree, r.tree)
+    assert rc2 == 0 and same_tree(tree2, harness.run_port(wide, 5)[0])
+
+
+def _check_arithmetic(q, tree):
+    n_nodes = 0
+
+    def walk(t):
+        nonlocal n_nodes
+        n_nodes += 1
+        if t[5] is None:
+            return
+        l, r = t[5], t[6]
+        walk(l)
+        walk(r)
+        assert l[0] & r[0] == 0 and (l[0] | r[0]) == t[0]
+        assert (t[1], t[2], t[3], float(t[4])) == harness.eval_join(q, l[0], r[0], l[1:5], r[1:5])
+
+    walk(tree)
+    assert n_nodes == 2 * q.n - 1
+
+
+def _ladder(n_rungs, seed):
+    """Two chains of key joins joined rung by rung: one biconnected block of
+    every relation that is not a cycle."""
+    import numpy as np
+    from gpuqo_b200.query import _assemble, _key_edges, _loguniform
+    n = 2 * n_rungs
+    rng = np.random.default_rng([seed, 14, n])
+    lrows = _loguniform(rng, 1e2, 1e7, n)
+    pairs = ([(i, i + 1) for i in range(n_rungs - 1)] + [(n_rungs + i, n_rungs + i + 1) for i in range(n_rungs - 1)] +
+             [(i, n_rungs + i) for i in range(n_rungs)])
+    return _assemble(f"ladder{n}_s{seed}", n, lrows, [8] * n, _key_edges(pairs, lrows), rng)
+
+
+def test_wide_limits_end_in_a_status(knob):
+    # a star of 34: 2^33 connected sets
+    r = _run(query.star(34, 23), 5)
+    assert r.tree is None and r.error == ERR_TOO_LARGE
+    # the same under a budget of 64 MB: refused as out of memory, early
+    knob("gpuqo_b200_device_memory_mb", 64)
+    r = _run(query.star(34, 23), 5)
+    assert r.tree is None and r.error == ERR_NOMEM
+    knob("gpuqo_b200_device_memory_mb", 0)
+    # a 32-relation ladder: few connected sets, but blocks of up to 32
+    # relations that are not cycles (2^32 splits for the whole set)
+    r = _run(_ladder(16, 24), 5)
+    assert r.tree is None and r.error == ERR_TOO_LARGE
+    # DPsize has no sparse memo
+    r = lib.run(query.key_chain(40, 25), capi.GPUQO_DPSIZE)
+    assert r.tree is None and r.error == ERR_UNSUPPORTED
+    # and the library is unaffected
+    q = WIDE[0]["query"]
+    assert same_tree(_run(q, 5).tree, harness.run_port(q, 5)[0])
