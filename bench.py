@@ -95,15 +95,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) per timed k_dp_tree launch, from the ncu
-    capture of this benchmark's own command (the four snowflake-25 seeds)
-    summarised in profiles/k_dp_tree_snowflake25_traffic.txt, if present."""
+def profiled_figure(key):
+    """A figure of profiles/k_dp_tree_snowflake25_traffic.txt (the ncu
+    captures of this benchmark's own workload): dram_bytes_per_launch (DRAM
+    read + write per timed k_dp_tree launch, the four snowflake-25 seeds) or
+    l2_throughput_pct_of_peak; None when absent."""
     p = os.path.join(REPO, "profiles", "k_dp_tree_snowflake25_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -635,7 +636,7 @@ def main():
         per_launch_bytes = alg_bytes / max(1, eval_launches)
         per_launch_s = (eval_ms / 1000.0) / max(1, eval_launches)
         achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
-        traffic = profiled_traffic()
+        traffic = profiled_figure("dram_bytes_per_launch")
         line = {
             "metric": METRIC, "value": value, "unit": "ms/query", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": False,
@@ -650,7 +651,10 @@ def main():
             "pairs_per_s": pairs / (tot_ms / 1000.0) if tot_ms > 0 else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_dp_tree (MPDP, persistent)", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None},
+                         "kernel": "k_dp_tree (MPDP, persistent)", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None,
+                         "traffic_source": "profiles/k_dp_tree_snowflake25_traffic.txt (ncu of this benchmark's "
+                                           "workload, mean of the timed launches)",
+                         "l2_throughput_pct_of_peak": profiled_figure("l2_throughput_pct_of_peak")},
             "e2e": {"value": e2e_value, "unit": "ms/query", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": kernels,

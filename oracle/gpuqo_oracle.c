@@ -1165,6 +1165,10 @@ QueryTreeC *gpuqo_run(int gpuqo_algorithm, GpuqoPlannerInfoC *info_c) {
  */
 void oracle_eval_join(GpuqoPlannerInfoC *info_c, uint64_t left_id, uint64_t right_id,
                       const float *vals_in, float *vals_out) {
+    if (info_c->n_rels < 1 || info_c->n_rels > MAXN - 1) {
+        for (int i = 0; i < 4; i++) vals_out[i] = NAN;
+        return;
+    }
     Info info;
     convert_info(info_c, &info);
     Rel l, r;

@@ -130,7 +130,10 @@ def run_port(q: Query, algorithm: int, idp_n_iters: int = 0,
 
 
 def eval_join(q: Query, left_id: int, right_id: int, lvals, rvals):
-    """Oracle join evaluation (rows, startup, total, width) of one join."""
+    """Oracle join evaluation (rows, startup, total, width) of one join
+    (queries of at most 63 relations, the oracle's relation sets)."""
+    if q.n > 63:
+        raise ValueError(f"the oracle takes at most 63 relations, not {q.n}")
     lib = load_port()
     f = lib.oracle_eval_join
     f.argtypes = [C.POINTER(capi.GpuqoPlannerInfoC), C.c_uint64, C.c_uint64,

@@ -71,11 +71,12 @@ def test_wide_matches_oracle_and_reference_optimum(case, alg):
 
 
 def test_wide_serves_idp_subproblems_and_the_service():
-    """IDP2 with 40-relation sub-problems on a 100-relation chain of key joins:
+    """IDP2 with 40-relation sub-problems on a 60-relation chain of key joins:
     every sub-problem above 31 relations runs on the sparse memo; the plan
     covers the relations and each join is the oracle's arithmetic of its
-    children.  The same request through the service returns the same plan."""
-    q = query.key_chain(100, 21)
+    children (the oracle takes at most 63 relations).  The same request
+    through the service returns the same plan."""
+    q = query.key_chain(60, 21)
     r = lib.run(q, capi.GPUQO_DPSUB, bicc=True, idp_n_iters=40, idp_type=capi.GPUQO_IDP2)
     assert r.error == 0
     _check_arithmetic(q, r.tree)
