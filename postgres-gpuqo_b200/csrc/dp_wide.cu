@@ -61,6 +61,7 @@ struct WideInfo {
     const uint64_t *fks;               // [n_fks]
     const DevVar *vars;                // [n_fks]
 };
+constexpr size_t kWideInfoBytes = (sizeof(WideInfo) + 15) & ~size_t(15);
 
 __device__ __forceinline__ uint64_t lowest64(uint64_t x) { return x & (0ull - x); }
 __device__ __forceinline__ int lowest_idx64(uint64_t x) { return __ffsll((long long)x) - 1; }
@@ -108,9 +109,16 @@ struct BlocksW {
     uint64_t eprefix[65];
 };
 
-__device__ void find_blocks64(uint64_t S, const uint64_t *adj, BlocksW &B) {
-    uint8_t disc[64], low[64], parent[64], stk_u[64], vstk[64];
+// DFS state of find_blocks64 (local memory for one thread per set, shared
+// memory for one lane per warp)
+struct DfsScratch {
     uint64_t stk_e[64], desc[64];
+    uint8_t disc[64], low[64], parent[64], stk_u[64], vstk[64];
+};
+
+__device__ void find_blocks64(uint64_t S, const uint64_t *adj, BlocksW &B, DfsScratch &D) {
+    uint8_t *disc = D.disc, *low = D.low, *parent = D.parent, *stk_u = D.stk_u, *vstk = D.vstk;
+    uint64_t *stk_e = D.stk_e, *desc = D.desc;
     int sp = 0, vsp = 0, t = 0;
     uint64_t visited = 0;
     B.nb = 0;
@@ -181,12 +189,11 @@ __device__ void find_blocks64(uint64_t S, const uint64_t *adj, BlocksW &B) {
     B.eprefix[B.nb] = etotal;
 }
 
-// arc j of a cycle block (see cached_arc): walk from the block's lowest
-// relation towards its lower neighbour; arc j starts at walk position
-// j / (m - 1) and has length j % (m - 1) + 1
-__device__ uint64_t cycle_arc64(uint64_t blk, const uint64_t *adj, uint64_t j) {
+// prefix masks of a cycle block's walk: from the block's lowest relation
+// towards its lower neighbour, pre[i] holds the first i relations of the walk
+// (pre[0] = 0 .. pre[m] = the block)
+__device__ void cycle_walk64(uint64_t blk, const uint64_t *adj, uint64_t *pre) {
     const uint32_t m = (uint32_t)__popcll(blk);
-    uint64_t pre[65];
     int v = lowest_idx64(blk);
     int prev = 63 - __clzll((long long)(adj[v] & blk));
     pre[0] = 0ull;
@@ -196,14 +203,31 @@ __device__ uint64_t cycle_arc64(uint64_t blk, const uint64_t *adj, uint64_t j) {
         prev = v;
         v = nx;
     }
+}
+
+// arc j of a cycle of m relations from its walk prefixes: it starts at walk
+// position j / (m - 1) and has length j % (m - 1) + 1
+__device__ __forceinline__ uint64_t cycle_arc64(const uint64_t *pre, uint32_t m, uint64_t j) {
     const uint64_t s = j / (m - 1u), e = s + j % (m - 1u) + 1u;
     return e <= m ? (pre[e] ^ pre[s]) : ((pre[m] ^ pre[s]) | pre[e - m]);
 }
 
+// per-warp shared scratch of k_wide_eval: the set's blocks and the walk
+// prefixes of its cycle blocks (the cycle blocks' sizes plus one sum to at
+// most 102 for 63 relations), written by lane 0
+struct WarpScratch {
+    BlocksW B;
+    DfsScratch dfs;
+    uint64_t pre[128];
+    uint8_t pre_off[64];
+};
+constexpr size_t kEvalSmem = kWideInfoBytes + (kWideBlock / 32) * sizeof(WarpScratch);
+
 // candidate c of S: its two sides and its index in the reference's MPDP order;
 // false when the grown sides do not cover S
-__device__ bool wide_candidate(uint64_t S, const BlocksW &B, const uint64_t *adj, uint64_t c, int &b, uint64_t &L,
+__device__ bool wide_candidate(uint64_t S, const WarpScratch &ws, const uint64_t *adj, uint64_t c, int &b, uint64_t &L,
                                uint64_t &R, uint64_t &key) {
+    const BlocksW &B = ws.B;
     while (b + 1 < B.nb && B.eprefix[b + 1] <= c) b++;
     const uint64_t blk = B.mask[b];
     const uint64_t j = c - B.eprefix[b];
@@ -223,7 +247,7 @@ __device__ bool wide_candidate(uint64_t S, const BlocksW &B, const uint64_t *adj
     }
     uint64_t lb;
     if ((B.cyc >> b) & 1ull) {
-        lb = cycle_arc64(blk, adj, j);
+        lb = cycle_arc64(ws.pre + ws.pre_off[b], (uint32_t)__popcll(blk), j);
         key = B.prefix[b] + pext64(lb, blk) - 1ull;
         if (blk == S) {
             L = lb;
@@ -398,15 +422,32 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval(const WideInfo *__rest
                                                           unsigned long long *__restrict__ memo_left,
                                                           unsigned long long *__restrict__ pairs_out,
                                                           unsigned *__restrict__ err) {
-    const WideInfo &w = *wi;
+    extern __shared__ __align__(16) unsigned char wsm[];
+    WideInfo &w = *reinterpret_cast<WideInfo *>(wsm);
+    for (uint32_t x = threadIdx.x; x < (uint32_t)(sizeof(WideInfo) / 4); x += blockDim.x)
+        reinterpret_cast<uint32_t *>(wsm)[x] = reinterpret_cast<const uint32_t *>(wi)[x];
+    __syncthreads();
     const int lane = threadIdx.x & 31;
+    WarpScratch &ws = reinterpret_cast<WarpScratch *>(wsm + kWideInfoBytes)[threadIdx.x >> 5];
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long pairs = 0;
-    BlocksW B;
     for (uint32_t i = gwarp; i < count; i += nwarps) {
         const uint64_t S = sets[first + i];
-        find_blocks64(S, w.adj, B);
+        __syncwarp();   // every lane is done with the previous set's scratch
+        if (lane == 0) {
+            find_blocks64(S, w.adj, ws.B, ws.dfs);
+            uint32_t off = 0;
+            for (int b = 0; b < ws.B.nb; b++) {
+                ws.pre_off[b] = (uint8_t)off;
+                if ((ws.B.cyc >> b) & 1ull) {
+                    cycle_walk64(ws.B.mask[b], w.adj, ws.pre + off);
+                    off += (uint32_t)__popcll(ws.B.mask[b]) + 1u;
+                }
+            }
+        }
+        __syncwarp();
+        const BlocksW &B = ws.B;
         const uint64_t P = B.eprefix[B.nb];
         if (P > kWideMaxCandidates) {   // a dense block: far beyond what an exact DP at this size can afford
             if (lane == 0) atomicExch(err, 3u);
@@ -422,7 +463,7 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval(const WideInfo *__rest
         int b = 0;
         for (uint64_t c = (uint64_t)lane; c < P; c += 32u) {
             uint64_t L, R, key;
-            if (!wide_candidate(S, B, w.adj, c, b, L, R, key)) continue;
+            if (!wide_candidate(S, ws, w.adj, c, b, L, R, key)) continue;
             if (index_order) key = dpsub_index64(L, S);
             const RelVal l = wide_rel(memo, wide_lookup(t, L, err), w.h.hz_packed);
             const RelVal r = wide_rel(memo, wide_lookup(t, R, err), w.h.hz_packed);
@@ -488,11 +529,12 @@ __global__ void k_wide_work(const WideInfo *__restrict__ wi, const unsigned long
                             uint32_t count, unsigned long long *__restrict__ total) {
     const WideInfo &w = *wi;
     BlocksW B;
+    DfsScratch D;
     unsigned long long acc = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         const uint64_t S = sets[i];
         if (__popcll(S) < 2) continue;
-        find_blocks64(S, w.adj, B);
+        find_blocks64(S, w.adj, B, D);
         const uint64_t P = B.eprefix[B.nb];
         acc += P > kWideMaxCandidates ? kWideMaxTotal + 1u : P;   // one such set refuses the DP
     }
@@ -727,6 +769,7 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         k_wide_insert<<<ib, 256, 0, stream>>>(t, d_sets, total, d_err);
         k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
         k_wide_work<<<ib, 256, 0, stream>>>(d_info, d_sets, total, d_pairs + 1);
+        CKW(cudaFuncSetAttribute(k_wide_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem));
         launches += 3;
         CKW(cudaGetLastError());
         // refuse before the levels when the DP would evaluate too many splits
@@ -746,7 +789,7 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
             launches++;
             const uint32_t blocks = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8,
                                                                  ((uint64_t)count * 32 + kWideBlock - 1) / kWideBlock);
-            k_wide_eval<<<blocks, kWideBlock, 0, stream>>>(d_info, t, d_sets, first, count,
+            k_wide_eval<<<blocks, kWideBlock, kEvalSmem, stream>>>(d_info, t, d_sets, first, count,
                                                            mode == kModeDpsub ? 1 : 0, d_memo, d_left, d_pairs,
                                                            d_err);
             CKW(cudaGetLastError());
