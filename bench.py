@@ -245,11 +245,11 @@ def cpu_reference_sample(queries, algorithm, steps=None, budget_s=20.0, min_runs
 GOLDEN = os.path.join(REPO, "tests", "golden", "cases.jsonl")
 
 
-def golden_cases(tag, algorithm):
+def golden_cases(tag, algorithm, path=GOLDEN):
     """The committed golden queries of one tag with the reference's plans."""
     from gpuqo_b200.query import Query
     out = []
-    with open(GOLDEN) as f:
+    with open(path) as f:
         for line in f:
             rec = json.loads(line)
             if rec["tag"] == tag and rec["algorithm"] == algorithm:
@@ -307,6 +307,45 @@ def configs_section(cpu=True):
         res["star12"]["reference_cpu_note"] = ("the reference's own engines (oracle/_ref) on the same stars: "
                                                "dpe_dpsub with gpuqo_dpe_n_threads = all host threads and "
                                                "gpuqo_dpe_pairs_per_depbuf 65536, cpu_dpsub on one thread")
+    res.update(wide_section(cpu))
+    return res
+
+
+WIDE_GOLDEN = os.path.join(REPO, "tests", "golden", "wide_cases.jsonl")
+
+
+def wide_section(cpu=True):
+    """Exact MPDP of 40 to 63 relations on the sparse memo, through gpuqo_run
+    from host structures (wall time and device time), with the root's rows
+    and total cost against the optimum of the reference's cpu_dpccp (the
+    committed fixtures), and that engine's own time on the same query."""
+    from gpuqo_b200 import capi, lib
+    res = {}
+    for tag in ("wide_key_chain63", "wide_key_cycle63", "wide_lollipop63_rich", "wide_ring_path40"):
+        cases = golden_cases(tag, capi.GPUQO_CPU_DPCCP, WIDE_GOLDEN)
+        if not cases:
+            continue
+        c = cases[0]
+        q = c["query"]
+        lib.run(q, capi.GPUQO_DPSUB, bicc=True)                          # warm-up
+        wall, dev = [], []
+        for _ in range(5):
+            r = lib.run(q, capi.GPUQO_DPSUB, bicc=True)
+            if r.error or r.tree is None:
+                raise RuntimeError(f"sparse exact DP failed on {q.name}: {r.error}")
+            wall.append(r.seconds * 1000.0)
+            dev.append(r.stats["device_ms"])
+        entry = {"workload": f"{q.n}-relation {q.name.rsplit('_s', 1)[0].rstrip('0123456789')} (MPDP, sparse memo)",
+                 "ms_per_query_wall": statistics.median(wall), "device_ms": statistics.median(dev),
+                 "connected_sets": r.stats["connected_sets"], "evaluated_pairs": r.stats["evaluated_pairs"],
+                 "kernel_launches": r.stats["kernel_launches"],
+                 "reference_optimum_reached": (r.tree[1], r.tree[3]) == (c["expected"][1], c["expected"][3])}
+        if cpu:
+            med, mean, used, nr = cpu_reference_sample([q], capi.GPUQO_CPU_DPCCP, budget_s=3.0, threads=1)
+            entry["reference_cpu_dpccp"] = {"median_ms_per_query": med, "threads": used, "runs": nr,
+                                            "note": "the reference's exact DP that runs at this size; its DPsub "
+                                                    "and MPDP visit all 2^n subsets"}
+        res[tag.replace("wide_", "wide:")] = entry
     return res
 
 

@@ -665,7 +665,7 @@ __device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_
     // and the qual count depend on the classes; the bucket size is 0.1 and
     // the MCV frequency 0 once any class matched, exactly what the general
     // loop below computes for such classes
-    bool all_plain = !MASKED;
+    bool all_plain = !MASKED || (ec_mask & ~d.plain[0]) == 0u;   // MASKED: at most 32 classes
     if (!MASKED) {
         const uint4 *pl = reinterpret_cast<const uint4 *>(d.plain);
 #pragma unroll
@@ -677,7 +677,7 @@ __device__ __forceinline__ void join_eval_mirror_w(const DevInfoView &d, uint32_
     }
     if (all_plain) {
 #pragma unroll 1
-        for (int base = 0; base < 128 * NW; base += 32) {
+        for (int base = 0; base < (MASKED ? 32 : 128 * NW); base += 32) {
             for (uint32_t mm = win[0]; mm; mm &= mm - 1u) {
                 const int i = base + __ffs(mm) - 1;
                 const bool lo_left = (lowest(d.ec_relids[i]) & L) != 0u;

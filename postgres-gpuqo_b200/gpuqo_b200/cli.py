@@ -20,7 +20,9 @@ ALGS = {"mpdp": (capi.GPUQO_DPSUB, True), "dpsub": (capi.GPUQO_DPSUB, False)}
 
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m gpuqo_b200.cli")
-    ap.add_argument("--shape", default="snowflake", choices=["star", "snowflake", "chain", "cycle", "clique"])
+    ap.add_argument("--shape", default="snowflake", choices=sorted(query.SHAPES),
+                    help="query graph; key_chain, key_cycle, lollipop and ring_path reach 63 relations "
+                         "(the sparse exact DP beyond 31)")
     ap.add_argument("--n", type=int, default=25)
     ap.add_argument("--nmin", type=int, default=8)
     ap.add_argument("--seed", type=int, default=0)
