@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <unordered_set>
 #include <vector>
@@ -569,6 +570,46 @@ __global__ void k_wide_base(const WideInfo *__restrict__ wi, WideTable t, float4
 
 uint64_t wide_set_capacity() { return 1ull << 25; }
 
+// Whether every biconnected block of the (connected) graph is a bridge or a
+// simple cycle: a block of m relations holding at most m edges.  Blocks by
+// Hopcroft-Tarjan on the host (recursive, at most 63 relations deep).
+static bool is_cactus(const std::vector<uint64_t> &adj) {
+    const int n = (int)adj.size();
+    std::vector<int> disc(n, -1), low(n, 0), vstack;
+    int t = 0;
+    bool ok = true;
+    std::function<void(int, int)> dfs = [&](int u, int parent) {
+        disc[u] = low[u] = t++;
+        vstack.push_back(u);
+        for (uint64_t x = adj[u]; x && ok; x &= x - 1ull) {
+            const int v = __builtin_ctzll(x);
+            if (disc[v] < 0) {
+                dfs(v, u);
+                low[u] = std::min(low[u], low[v]);
+                if (low[v] >= disc[u]) {
+                    uint64_t blk = 1ull << u;
+                    int w;
+                    do {
+                        w = vstack.back();
+                        vstack.pop_back();
+                        blk |= 1ull << w;
+                    } while (w != v);
+                    int m = 0, deg2 = 0;
+                    for (uint64_t y = blk; y; y &= y - 1ull) {
+                        m++;
+                        deg2 += __builtin_popcountll(adj[__builtin_ctzll(y)] & blk);
+                    }
+                    if (deg2 / 2 > m) ok = false;
+                }
+            } else if (v != parent) {
+                low[u] = std::min(low[u], disc[v]);
+            }
+        }
+    };
+    if (n > 0) dfs(0, -1);
+    return ok;
+}
+
 int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, EngineStats &st,
                     std::string &err) {
     const int n = info.n;
@@ -640,6 +681,7 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         err = "query graph is not connected";
         return GPUQO_B200_ERR_ARGS;
     }
+    const bool cactus = is_cactus(adj);
     const uint32_t total = (uint32_t)all.size();
     uint32_t cap_log2 = 1;
     while ((1ull << cap_log2) < 2ull * total) cap_log2++;
@@ -768,14 +810,20 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         const uint32_t ib = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8, (total + 255) / 256);
         k_wide_insert<<<ib, 256, 0, stream>>>(t, d_sets, total, d_err);
         k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
-        k_wide_work<<<ib, 256, 0, stream>>>(d_info, d_sets, total, d_pairs + 1);
         CKW(cudaFuncSetAttribute(k_wide_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem));
-        launches += 3;
-        CKW(cudaGetLastError());
+        launches += 2;
         // refuse before the levels when the DP would evaluate too many splits
-        // (a large biconnected block that is not a cycle)
-        CKW(cudaMemcpyAsync(&h_work, d_pairs + 1, 8, cudaMemcpyDeviceToHost, stream));
-        CKW(cudaStreamSynchronize(stream));
+        // (a large biconnected block that is not a cycle); a cactus graph
+        // cannot: every block of a connected set lies in a block of the graph,
+        // so its blocks are bridges and whole cycles, at most 63 * 62 splits
+        if (!cactus) {
+            k_wide_work<<<ib, 256, 0, stream>>>(d_info, d_sets, total, d_pairs + 1);
+            launches++;
+            CKW(cudaGetLastError());
+            CKW(cudaMemcpyAsync(&h_work, d_pairs + 1, 8, cudaMemcpyDeviceToHost, stream));
+            CKW(cudaStreamSynchronize(stream));
+        }
+        CKW(cudaGetLastError());
         if (h_work > kWideMaxTotal) {
             err = "the sparse exact DP would evaluate more than " + std::to_string(h_work) +
                   " candidate splits (a large biconnected block that is not a cycle; the bound is 2^35, 2^24 per "
