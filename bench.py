@@ -98,8 +98,8 @@ def measured_peaks():
 def profiled_figure(key):
     """A figure of profiles/k_dp_tree_snowflake25_traffic.txt (the ncu
     captures of this benchmark's own workload): dram_bytes_per_launch (DRAM
-    read + write per timed k_dp_tree launch, the four snowflake-25 seeds) or
-    l2_throughput_pct_of_peak; None when absent."""
+    read + write per timed k_dp_tree launch, the four snowflake-25 seeds),
+    l2_throughput_pct_of_peak or issue_active_pct; None when absent."""
     p = os.path.join(REPO, "profiles", "k_dp_tree_snowflake25_traffic.txt")
     if not os.path.exists(p):
         return None
@@ -693,7 +693,8 @@ def main():
                          "kernel": "k_dp_tree (MPDP, persistent)", "eval_kernel_share": eval_ms / tot_ms if tot_ms else None,
                          "traffic_source": "profiles/k_dp_tree_snowflake25_traffic.txt (ncu of this benchmark's "
                                            "workload, mean of the timed launches)",
-                         "l2_throughput_pct_of_peak": profiled_figure("l2_throughput_pct_of_peak")},
+                         "l2_throughput_pct_of_peak": profiled_figure("l2_throughput_pct_of_peak"),
+                         "issue_active_pct": profiled_figure("issue_active_pct")},
             "e2e": {"value": e2e_value, "unit": "ms/query", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": kernels,
