@@ -321,7 +321,8 @@ def wide_section(cpu=True):
     committed fixtures), and that engine's own time on the same query."""
     from gpuqo_b200 import capi, lib
     res = {}
-    for tag in ("wide_key_chain63", "wide_key_cycle63", "wide_lollipop63_rich", "wide_ring_path40"):
+    for tag in ("wide_key_chain63", "wide_key_cycle63", "wide_lollipop63_rich", "wide_ring_path40",
+                "wide_snowflake32", "wide_snowflake34"):
         cases = golden_cases(tag, capi.GPUQO_CPU_DPCCP, WIDE_GOLDEN)
         if not cases:
             continue
@@ -339,8 +340,8 @@ def wide_section(cpu=True):
                  "ms_per_query_wall": statistics.median(wall), "device_ms": statistics.median(dev),
                  "connected_sets": r.stats["connected_sets"], "evaluated_pairs": r.stats["evaluated_pairs"],
                  "kernel_launches": r.stats["kernel_launches"],
-                 "reference_optimum_reached": (r.tree[1], r.tree[3]) == (c["expected"][1], c["expected"][3])}
-        if cpu:
+                 "reference_optimum_reached": r.tree[3] == c["expected"][3]}
+        if cpu and not tag.startswith("wide_snowflake"):   # cpu_dpccp takes 40-90 s on those
             med, mean, used, nr = cpu_reference_sample([q], capi.GPUQO_CPU_DPCCP, budget_s=3.0, threads=1)
             entry["reference_cpu_dpccp"] = {"median_ms_per_query": med, "threads": used, "runs": nr,
                                             "note": "the reference's exact DP that runs at this size; its DPsub "

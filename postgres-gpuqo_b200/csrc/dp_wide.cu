@@ -61,6 +61,11 @@ struct WideInfo {
     const float *sels;                 // [n_sels]
     const uint64_t *fks;               // [n_fks]
     const DevVar *vars;                // [n_fks]
+    // [n_ec] per class: the selectivity with its lower member outer, with its
+    // higher member outer, and whether it is plain (two members whose
+    // variables carry no statistics and no index: bucket size 0.1, MCV
+    // frequency 0); w unused
+    const float4 *pair;
 };
 constexpr size_t kWideInfoBytes = (sizeof(WideInfo) + 15) & ~size_t(15);
 
@@ -313,6 +318,16 @@ __device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, ui
         const uint64_t ec = w.ec_relids[i];
         const uint64_t ml = ec & L, mr = ec & R;
         if (!ml || !mr) continue;
+        const float4 pf = __ldg(w.pair + i);
+        if (__float_as_uint(pf.z) != 0u) {
+            // a plain class: what the general steps below compute for it
+            sel *= (lowest64(ec) & L) ? pf.x : pf.y;
+            per_tuple += h.cpu_operator_cost;
+            n_quals++;
+            if (bucketsize > 0.1f) bucketsize = 0.1f;
+            if (mcvfreq > 0.0f) mcvfreq = 0.0f;
+            continue;
+        }
         sel *= ec_selectivity64(w, i, ec, ml, mr);
         per_tuple += h.cpu_operator_cost;
         n_quals++;
@@ -382,22 +397,28 @@ __device__ __forceinline__ uint32_t wide_hash(uint64_t key, uint32_t cap_log2) {
     return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - cap_log2));
 }
 
-__global__ void k_wide_insert(WideTable t, const unsigned long long *__restrict__ sets, uint32_t count,
-                              unsigned *__restrict__ err) {
+// one set into the table with its slot (linear probing; the table is never
+// more than half full, so a free slot is always found)
+__device__ __forceinline__ void wide_insert_one(const WideTable &t, unsigned long long key, uint32_t slot,
+                                                unsigned *err) {
     const uint32_t cap = 1u << t.cap_log2;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const unsigned long long key = sets[i];
-        uint32_t pos = wide_hash(key, t.cap_log2);
-        bool done = false;
-        for (uint32_t probe = 0; probe < cap && !done; probe++, pos = (pos + 1u) & (cap - 1u)) {
-            const unsigned long long old = atomicCAS(t.keys + pos, 0ull, key);
-            if (old == 0ull || old == key) {
-                t.slot[pos] = i;
-                done = true;
-            }
+    uint32_t pos = wide_hash(key, t.cap_log2);
+    for (uint32_t probe = 0; probe < cap; probe++, pos = (pos + 1u) & (cap - 1u)) {
+        const unsigned long long old = atomicCAS(t.keys + pos, 0ull, key);
+        if (old == 0ull || old == key) {
+            t.slot[pos] = slot;
+            return;
         }
-        if (!done) atomicExch(err, 1u);   // table full: cannot happen at half load
     }
+    atomicExch(err, 1u);
+}
+
+// sets[first .. first + count) into the table, each with its index as slot
+__global__ void k_wide_insert(WideTable t, const unsigned long long *__restrict__ sets, uint32_t first,
+                              uint32_t count, unsigned *__restrict__ err) {
+    for (uint32_t i = first + blockIdx.x * blockDim.x + threadIdx.x; i < first + count;
+         i += gridDim.x * blockDim.x)
+        wide_insert_one(t, sets[i], i, err);
 }
 
 __device__ __forceinline__ uint32_t wide_lookup(const WideTable &t, uint64_t key, unsigned *err) {
@@ -555,6 +576,268 @@ __global__ void k_wide_base(const WideInfo *__restrict__ wi, WideTable t, float4
     memo_left[s] = 0ull;
 }
 
+// ---------------------------------------------------------------------------
+// tree-shaped query graphs: no block search
+// ---------------------------------------------------------------------------
+// Per-root tables of a tree-shaped graph, row r for the preorder from r with
+// children in increasing index order (the DFS order of the reference's block
+// search): sub = the relation's subtree, before = the relations ahead of it,
+// anc = its ancestors, par = its parent.  Every connected set S is a subtree
+// rooted at r = lowest(S); its blocks are its edges, each emitted when the DFS
+// returns from the child end c, so the block of edge (par c, c) is number
+//     post = |S & before[c]| - |S & anc[c]| + |S & sub[c]| - 1
+// and its two candidates (the side holding the lower end first) have the
+// reference's indices 2 post and 2 post + 1.
+struct WideTree {
+    const unsigned long long *sub, *before, *anc;   // [n * n]
+    const uint8_t *par;                             // [n * n]
+};
+
+__device__ __forceinline__ int nth_bit64(uint64_t x, int e) {   // the e-th set bit of x, from 0
+    const uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+    const int c = __popc(lo);
+    return e < c ? (int)__fns(lo, 0u, e + 1) : 32 + (int)__fns(hi, 0u, e - c + 1);
+}
+
+// level k + 1 of a tree-shaped graph from level k: adding a neighbour u to a
+// connected S makes u a leaf of T = S + u, and T is emitted only from the S
+// whose u is T's largest leaf, so every connected set appears once.  Output
+// at sets[out_first + atomic index], entered into the table with that slot;
+// an index at or beyond out_count (which the host counted exactly) raises
+// err 4 instead of writing.
+__global__ void __launch_bounds__(256) k_wide_tree_enum(const WideInfo *__restrict__ wi, WideTable t,
+                                                        unsigned long long *__restrict__ sets, uint32_t first,
+                                                        uint32_t count, uint32_t out_first, uint32_t out_count,
+                                                        unsigned *__restrict__ out_n, unsigned *__restrict__ err) {
+    __shared__ unsigned long long adj[64];
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) adj[i] = wi->adj[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounds = (count + stride - 1u) / stride;
+    for (uint32_t rd = 0; rd < rounds; rd++) {
+        const uint32_t i = rd * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        uint64_t S = 0ull, N = 0ull, leaves = 0ull;
+        if (i < count) {
+            S = sets[first + i];
+            for (uint64_t x = S; x; x &= x - 1ull) {
+                const int v = lowest_idx64(x);
+                const uint64_t a = adj[v];
+                N |= a;
+                if (__popcll(a & S) == 1) leaves |= 1ull << v;
+            }
+            N &= ~S;
+        }
+        const bool single = (S & (S - 1ull)) == 0ull;
+        const int deg = __popcll(N);
+        const int maxdeg = (int)__reduce_max_sync(kFullW, (uint32_t)deg);
+        for (int j = 0; j < maxdeg; j++) {
+            bool ok = false;
+            uint64_t T = 0ull;
+            if (j < deg) {
+                const uint64_t bu = lowest64(N);
+                N ^= bu;
+                T = S | bu;
+                const uint64_t p = adj[lowest_idx64(bu)] & S;          // u's only neighbour in S
+                const uint64_t others = single ? S : (leaves & ~p);    // T's other leaves
+                ok = others < bu;                                       // u is T's largest leaf
+            }
+            const unsigned m = __ballot_sync(kFullW, ok);
+            if (m) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(out_n, (unsigned)__popc(m));
+                base = __shfl_sync(kFullW, base, 0);
+                if (ok) {
+                    const uint32_t idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                    if (idx < out_count) {
+                        sets[out_first + idx] = T;
+                        wide_insert_one(t, T, out_first + idx, err);
+                    } else {
+                        atomicExch(err, 4u);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// level k of a tree-shaped graph: groups of G lanes (a power of two) per set,
+// a lane per edge (two when k - 1 > 32), both orientations of each edge
+__global__ void __launch_bounds__(kWideBlock) k_wide_eval_tree(const WideInfo *__restrict__ wi, WideTable t,
+                                                               WideTree tt, const unsigned long long *__restrict__ sets,
+                                                               uint32_t first, uint32_t count, int k, int G,
+                                                               int index_order, float4 *__restrict__ memo,
+                                                               unsigned long long *__restrict__ memo_left,
+                                                               unsigned long long *__restrict__ pairs_out,
+                                                               unsigned *__restrict__ err) {
+    extern __shared__ __align__(16) unsigned char wsm[];
+    WideInfo &w = *reinterpret_cast<WideInfo *>(wsm);
+    for (uint32_t x = threadIdx.x; x < (uint32_t)(sizeof(WideInfo) / 4); x += blockDim.x)
+        reinterpret_cast<uint32_t *>(wsm)[x] = reinterpret_cast<const uint32_t *>(wi)[x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t gpw = 32u / (uint32_t)G;
+    const int grp = lane / G, gl = lane % G;
+    const uint32_t group_mask = (G == 32) ? kFullW : (((1u << G) - 1u) << (grp * G));
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int n = w.n;
+    const uint32_t E = (uint32_t)(k - 1);
+    unsigned long long pairs = 0;
+    for (uint32_t i0 = gwarp * gpw; i0 < count; i0 += nwarps * gpw) {
+        const uint32_t i = i0 + (uint32_t)grp;
+        const uint64_t S = (i < count) ? sets[first + i] : 0ull;
+        // a listed set has k relations among the n (anything else is an
+        // enumeration fault: reported, never indexed with)
+        const bool has = i < count && __popcll(S) == k && (S >> n) == 0ull;
+        if (i < count && !has && gl == 0) atomicExch(err, 5u);
+        const int r = has ? lowest_idx64(S) : 0;
+        const uint64_t Sn = S & ~(1ull << r);
+        uint32_t best_c = kFullW;
+        uint64_t best_k = ~0ull, first_k = ~0ull, best_l = 0ull, nan_l = 0ull;
+        bool first_nan = false;
+        RelVal best_v, nan_v;
+        best_v.rows = best_v.startup = best_v.total = 0.0f;
+        best_v.width = 0;
+        best_v.hz = 0u;
+        nan_v = best_v;
+        auto update = [&](uint64_t key, uint64_t L, const RelVal &out) {
+            const bool nan = isnan(out.total);
+            if (key < first_k) {
+                first_k = key;
+                first_nan = nan;
+                if (nan) {
+                    nan_v = out;
+                    nan_l = L;
+                }
+            }
+            if (!nan) {
+                const uint32_t oc = ord_float(out.total);
+                if (oc < best_c || (oc == best_c && key < best_k)) {
+                    best_c = oc;
+                    best_k = key;
+                    best_v = out;
+                    best_l = L;
+                }
+            }
+        };
+        for (uint32_t e = (uint32_t)gl; has && e < E; e += (uint32_t)G) {
+            const int v = nth_bit64(Sn, (int)e);
+            const int p = tt.par[r * n + v];
+            const uint64_t comp = S & __ldg(tt.sub + r * n + v);
+            const uint64_t L0 = (v < p) ? comp : (S ^ comp);     // the side holding the edge's lower end
+            const uint64_t R0 = S ^ L0;
+            uint64_t k0, k1;
+            if (index_order) {
+                k0 = dpsub_index64(L0, S);
+                k1 = dpsub_index64(R0, S);
+            } else {
+                const uint64_t post = (uint64_t)(__popcll(S & __ldg(tt.before + r * n + v)) -
+                                                 __popcll(S & __ldg(tt.anc + r * n + v)) + __popcll(comp) - 1);
+                k0 = 2ull * post;
+                k1 = k0 + 1ull;
+            }
+            const RelVal lv = wide_rel(memo, wide_lookup(t, L0, err), w.h.hz_packed);
+            const RelVal rv = wide_rel(memo, wide_lookup(t, R0, err), w.h.hz_packed);
+            update(k0, L0, join_eval_w(w, L0, lv, R0, rv));
+            update(k1, R0, join_eval_w(w, R0, rv, L0, lv));
+            pairs += 2;
+        }
+        // group minimum of (cost, index) and of the first index (butterfly
+        // within the aligned group; every lane of the warp takes part)
+        uint32_t mc = best_c, kh = (uint32_t)(best_k >> 32), kl = (uint32_t)best_k;
+        uint32_t fh = (uint32_t)(first_k >> 32), fl = (uint32_t)first_k;
+        for (int off = G / 2; off >= 1; off >>= 1) {
+            const uint32_t oc = __shfl_xor_sync(kFullW, mc, off);
+            const uint32_t oh = __shfl_xor_sync(kFullW, kh, off);
+            const uint32_t ol = __shfl_xor_sync(kFullW, kl, off);
+            if (oc < mc || (oc == mc && (oh < kh || (oh == kh && ol < kl)))) {
+                mc = oc;
+                kh = oh;
+                kl = ol;
+            }
+            const uint32_t ofh = __shfl_xor_sync(kFullW, fh, off);
+            const uint32_t ofl = __shfl_xor_sync(kFullW, fl, off);
+            if (ofh < fh || (ofh == fh && ofl < fl)) {
+                fh = ofh;
+                fl = ofl;
+            }
+        }
+        const uint64_t mk = ((uint64_t)kh << 32) | kl, mf = ((uint64_t)fh << 32) | fl;
+        const bool nan_first = has && first_k == mf && first_nan && mf != ~0ull;
+        const unsigned nm = __ballot_sync(kFullW, nan_first) & group_mask;
+        const RelVal *wv = nullptr;
+        uint64_t wl = 0ull;
+        if (has) {
+            if (nm) {
+                if (nan_first) {
+                    wv = &nan_v;
+                    wl = nan_l;
+                }
+            } else if (best_c == mc && best_k == mk && mc != kFullW) {
+                wv = &best_v;
+                wl = best_l;
+            }
+        }
+        if (wv) {
+            const uint32_t slot = wide_lookup(t, S, err);
+            memo[slot] = make_float4(wv->rows, wv->startup, wv->total,
+                                     __uint_as_float(memo_width_word(w.h, wv->rows, wv->width)));
+            memo_left[slot] = wl;
+        }
+    }
+    for (int off = 16; off >= 1; off >>= 1) pairs += __shfl_xor_sync(kFullW, pairs, off);
+    if (lane == 0 && pairs) atomicAdd(pairs_out, pairs);
+}
+
+// the plan, walked from the full set by one thread (at most 2n - 1 nodes)
+__global__ void k_wide_extract(WideTable t, const float4 *__restrict__ memo,
+                               const unsigned long long *__restrict__ memo_left, uint64_t full, int n,
+                               uint32_t wmask, TreeNode *__restrict__ out, int *__restrict__ n_out,
+                               unsigned *__restrict__ err) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint64_t st_set[128];
+    int st_parent[128], st_side[128];
+    int sp = 0, cnt = 0;
+    st_set[sp] = full;
+    st_parent[sp] = -1;
+    st_side[sp] = 0;
+    sp++;
+    while (sp > 0 && cnt < 2 * n - 1) {
+        sp--;
+        const uint64_t s = st_set[sp];
+        const int parent = st_parent[sp], side = st_side[sp];
+        const uint32_t slot = wide_lookup(t, s, err);
+        const float4 v = __ldcg(memo + slot);
+        TreeNode nd;
+        nd.set = s;
+        nd.left = -1;
+        nd.right = -1;
+        nd.rows = v.x;
+        nd.startup = v.y;
+        nd.total = v.z;
+        nd.width = (int32_t)(__float_as_uint(v.w) & wmask);
+        const int me = cnt++;
+        out[me] = nd;
+        if (parent >= 0) {
+            if (side == 0) out[parent].left = me;
+            else out[parent].right = me;
+        }
+        const uint64_t l = __ldcg(memo_left + slot) & s;
+        if (__popcll(s) > 1 && l != 0ull && l != s && sp + 2 <= 128) {
+            st_set[sp] = s ^ l;
+            st_parent[sp] = me;
+            st_side[sp] = 1;
+            sp++;
+            st_set[sp] = l;
+            st_parent[sp] = me;
+            st_side[sp] = 0;
+            sp++;
+        }
+    }
+    *n_out = cnt;
+}
+
 #define CKW(call)                                                                         \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
@@ -610,6 +893,82 @@ static bool is_cactus(const std::vector<uint64_t> &adj) {
     return ok;
 }
 
+// Connected sets of a tree per size (index 1..n), counted without listing
+// them: g_v(x) = x * prod over v's children c of (1 + g_c(x)) counts the sets
+// whose relation nearest the root is v; doubles, exact below 2^53.
+static std::vector<double> tree_level_counts(const std::vector<uint64_t> &adj) {
+    const int n = (int)adj.size();
+    std::vector<int> order(1, 0), parent(n, -1);
+    std::vector<bool> seen(n, false);
+    seen[0] = true;
+    for (size_t q = 0; q < order.size(); q++) {
+        const int u = order[q];
+        for (uint64_t x = adj[u]; x; x &= x - 1ull) {
+            const int v = __builtin_ctzll(x);
+            if (!seen[v]) {
+                seen[v] = true;
+                parent[v] = u;
+                order.push_back(v);
+            }
+        }
+    }
+    std::vector<std::vector<double>> g(n, std::vector<double>(n + 1, 0.0));
+    std::vector<double> out(n + 1, 0.0);
+    for (int q = n - 1; q >= 0; q--) {
+        const int v = order[q];
+        std::vector<double> acc(n + 1, 0.0);
+        acc[1] = 1.0;
+        for (uint64_t x = adj[v]; x; x &= x - 1ull) {
+            const int c = __builtin_ctzll(x);
+            if (parent[c] != v) continue;
+            std::vector<double> nx(n + 1, 0.0);
+            for (int a = 1; a <= n; a++) {
+                if (acc[a] == 0.0) continue;
+                nx[a] += acc[a];
+                for (int b = 1; a + b <= n; b++) nx[a + b] += acc[a] * g[c][b];
+            }
+            acc.swap(nx);
+        }
+        g[v] = acc;
+        for (int k = 1; k <= n; k++) out[k] += acc[k];
+    }
+    return out;
+}
+
+// per-root tables of a tree (WideTree), rows of n
+static void tree_tables(const std::vector<uint64_t> &adj, std::vector<uint64_t> &sub, std::vector<uint64_t> &before,
+                        std::vector<uint64_t> &anc, std::vector<uint8_t> &par) {
+    const int n = (int)adj.size();
+    sub.assign((size_t)n * n, 0ull);
+    before.assign((size_t)n * n, 0ull);
+    anc.assign((size_t)n * n, 0ull);
+    par.assign((size_t)n * n, 255);
+    for (int r = 0; r < n; r++) {
+        uint64_t *S = &sub[(size_t)r * n], *B = &before[(size_t)r * n], *A = &anc[(size_t)r * n];
+        uint8_t *P = &par[(size_t)r * n];
+        std::vector<int> stack(1, r), order;
+        uint64_t ahead = 0ull;
+        while (!stack.empty()) {
+            const int u = stack.back();
+            stack.pop_back();
+            B[u] = ahead;
+            ahead |= 1ull << u;
+            order.push_back(u);
+            uint64_t kids = adj[u] & ~(P[u] == 255 ? 0ull : (1ull << P[u]));
+            // pushed from the highest index, so that the lowest is visited first
+            while (kids) {
+                const int c = 63 - __builtin_clzll(kids);
+                kids &= ~(1ull << c);
+                P[c] = (uint8_t)u;
+                A[c] = A[u] | (1ull << u);
+                stack.push_back(c);
+            }
+        }
+        for (int v = 0; v < n; v++) S[v] = 1ull << v;
+        for (int q = (int)order.size() - 1; q > 0; q--) S[P[order[q]]] |= S[order[q]];
+    }
+}
+
 int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &nodes, EngineStats &st,
                     std::string &err) {
     const int n = info.n;
@@ -627,8 +986,12 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     }
     // compact adjacency (relation i = bit i)
     std::vector<uint64_t> adj(n);
-    for (int i = 0; i < n; i++) adj[i] = info.edge[i] >> 1;
-    // connected sets by level: extension of level k by a neighbour, deduplicated.
+    int degree_sum = 0;
+    for (int i = 0; i < n; i++) {
+        adj[i] = info.edge[i] >> 1;
+        degree_sum += __builtin_popcountll(adj[i]);
+    }
+    const uint64_t full = (n == 64) ? ~0ull : ((1ull << n) - 1ull);
     // Device bytes per set: key + slot at up to 4 table slots per set, the set,
     // its memo entry and its left side; a device-memory budget lowers the cap.
     constexpr uint64_t kBytesPerSet = 4 * 12 + 8 + 16 + 8;
@@ -651,14 +1014,27 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
               "(use IDP)";
         return GPUQO_B200_ERR_TOO_LARGE;
     };
+    // Connected sets by level.  A tree's are counted on the host and listed
+    // on the device level by level (k_wide_tree_enum); other graphs' are
+    // listed on the host by extension with one neighbour, deduplicated.
+    const bool tree = degree_sum == 2 * (n - 1);
     std::vector<uint64_t> all;
     std::vector<uint32_t> lvl_off(1, 0);
-    {
+    if (tree) {
+        const std::vector<double> cnt = tree_level_counts(adj);
+        double tot = 0.0;
+        for (int k = 1; k <= n; k++) tot += cnt[k];
+        if (cnt[n] != 1.0) {
+            err = "query graph is not connected";
+            return GPUQO_B200_ERR_ARGS;
+        }
+        if (tot > (double)cap_sets) return too_many();
+        for (int k = 1; k <= n; k++) lvl_off.push_back(lvl_off.back() + (uint32_t)cnt[k]);
+    } else {
         std::vector<uint64_t> cur;
         for (int i = 0; i < n; i++) cur.push_back(1ull << i);
         for (int k = 1; k <= n; k++) {
             if (all.size() + cur.size() > cap_sets) return too_many();
-            std::sort(cur.begin(), cur.end());
             all.insert(all.end(), cur.begin(), cur.end());
             lvl_off.push_back((uint32_t)all.size());
             if (k == n) break;
@@ -675,20 +1051,20 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
             }
             cur.assign(next.begin(), next.end());
         }
+        if (all.back() != full) {
+            err = "query graph is not connected";
+            return GPUQO_B200_ERR_ARGS;
+        }
     }
-    const uint64_t full = (n == 64) ? ~0ull : ((1ull << n) - 1ull);
-    if (all.back() != full) {
-        err = "query graph is not connected";
-        return GPUQO_B200_ERR_ARGS;
-    }
-    const bool cactus = is_cactus(adj);
-    const uint32_t total = (uint32_t)all.size();
+    const bool cactus = tree || is_cactus(adj);
+    const uint32_t total = lvl_off[n];
     uint32_t cap_log2 = 1;
     while ((1ull << cap_log2) < 2ull * total) cap_log2++;
     const uint64_t cap = 1ull << cap_log2;
     const size_t n_ec = info.ec_relids.size(), n_sels = info.ec_sels.size(), n_fks = info.ec_fks.size();
+    const uint64_t tree_bytes = tree ? (uint64_t)n * n * 25 : 0ull;
     const uint64_t bytes = cap * 12ull + (uint64_t)total * (8 + 16 + 8) + n_ec * 12 + n_sels * 4 + n_fks * 40 +
-                           sizeof(WideInfo) + 64;
+                           sizeof(WideInfo) + tree_bytes + 64 * sizeof(TreeNode) + 4 * 66 + 64;
     if (gpuqo_b200_device_memory_mb > 0 && bytes > ((uint64_t)gpuqo_b200_device_memory_mb << 20)) {
         err = "the sparse exact DP needs " + std::to_string(bytes >> 20) + " MB of device memory; "
               "gpuqo_b200_device_memory_mb allows " + std::to_string(gpuqo_b200_device_memory_mb);
@@ -749,6 +1125,33 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
             off_fks += j;
         }
     }
+    // the plain-class table (the pair selectivities of gpuqo_row_estimation.cuh
+    // :26-88 for a two-member class, both orientations)
+    std::vector<float4> h_pair(std::max<size_t>(n_ec, 1), make_float4(0.f, 0.f, 0.f, 0.f));
+    for (size_t e = 0; e < n_ec; e++) {
+        if (__builtin_popcountll(h_relids[e]) != 2) continue;
+        const int off_s = (int)(h_off[e] >> 16), off_f = (int)(h_off[e] & 0xFFFFu);
+        const int x = __builtin_ctzll(h_relids[e]), y = 63 - __builtin_clzll(h_relids[e]);
+        const bool fk_xy = (h_fks[off_f] >> y) & 1ull;       // member x's key matches y
+        const bool fk_yx = (h_fks[off_f + 1] >> x) & 1ull;   // member y's key matches x
+        const float sel = info.ec_sels[off_s];
+        bool plain = true;
+        for (int j = 0; j < 2; j++) {
+            const DevVar &dv = h_vars[off_f + j];
+            plain = plain && (dv.flags & (1u | kVarMcvRatio)) == 0u && (dv.flags & kVarNoDistinct) != 0u &&
+                    dv.mcvfreq == 0.0f;
+        }
+        float4 &pe = h_pair[e];
+        pe.x = fk_xy ? hw.fksel[y] : (fk_yx ? hw.fksel[x] : sel);
+        pe.y = fk_yx ? hw.fksel[x] : (fk_xy ? hw.fksel[y] : sel);
+        uint32_t flag = plain ? 1u : 0u;
+        std::memcpy(&pe.z, &flag, 4);
+    }
+    std::vector<uint64_t> t_sub, t_before, t_anc;
+    std::vector<uint8_t> t_par;
+    if (tree) tree_tables(adj, t_sub, t_before, t_anc, t_par);
+    std::vector<uint64_t> singles(n);
+    for (int i = 0; i < n; i++) singles[i] = 1ull << i;
     int rc = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -758,12 +1161,15 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     float *d_sels = nullptr;
     DevVar *d_vars = nullptr;
     unsigned long long *d_keys = nullptr, *d_sets = nullptr, *d_left = nullptr, *d_pairs = nullptr;
-    float4 *d_memo = nullptr;
-    unsigned *d_err = nullptr;
-    std::vector<float4> h_memo;
-    std::vector<uint64_t> h_left;
-    unsigned h_err = 0;
+    unsigned long long *d_tsub = nullptr, *d_tbefore = nullptr, *d_tanc = nullptr;
+    uint8_t *d_tpar = nullptr;
+    float4 *d_memo = nullptr, *d_pair = nullptr;
+    unsigned *d_err = nullptr;     // [0] error flag, [1 .. n] sets listed per level (trees)
+    TreeNode *d_nodes = nullptr;
+    int *d_nn = nullptr;
+    std::vector<unsigned> h_err(n + 2, 0u);
     unsigned long long h_pairs = 0, h_work = 0;
+    int h_nn = 0;
     uint32_t launches = 0;
     float ms = 0.f;
     int sm_count = 148, dev = 0;
@@ -778,19 +1184,34 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     CKW(cudaMalloc(&d_sels, std::max<size_t>(n_sels, 1) * 4));
     CKW(cudaMalloc(&d_fks, std::max<size_t>(n_fks, 1) * 8));
     CKW(cudaMalloc(&d_vars, std::max<size_t>(n_fks, 1) * sizeof(DevVar)));
+    CKW(cudaMalloc(&d_pair, h_pair.size() * sizeof(float4)));
     CKW(cudaMalloc(&d_keys, cap * 8));
     CKW(cudaMalloc(&d_slot, cap * 4));
     CKW(cudaMalloc(&d_sets, (size_t)total * 8));
     CKW(cudaMalloc(&d_memo, (size_t)total * sizeof(float4)));
     CKW(cudaMalloc(&d_left, (size_t)total * 8));
     CKW(cudaMalloc(&d_pairs, 16));   // [0] evaluated pairs, [1] the work bound
-    CKW(cudaMalloc(&d_err, 4));
+    CKW(cudaMalloc(&d_err, (size_t)(n + 2) * 4));
+    CKW(cudaMalloc(&d_nodes, 128 * sizeof(TreeNode)));
+    CKW(cudaMalloc(&d_nn, sizeof(int)));
+    if (tree) {
+        CKW(cudaMalloc(&d_tsub, (size_t)n * n * 8));
+        CKW(cudaMalloc(&d_tbefore, (size_t)n * n * 8));
+        CKW(cudaMalloc(&d_tanc, (size_t)n * n * 8));
+        CKW(cudaMalloc(&d_tpar, (size_t)n * n));
+        CKW(cudaMemcpyAsync(d_tsub, t_sub.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice, stream));
+        CKW(cudaMemcpyAsync(d_tbefore, t_before.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice, stream));
+        CKW(cudaMemcpyAsync(d_tanc, t_anc.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice, stream));
+        CKW(cudaMemcpyAsync(d_tpar, t_par.data(), (size_t)n * n, cudaMemcpyHostToDevice, stream));
+    }
     hw.ec_relids = d_relids;
     hw.ec_off = d_off;
     hw.sels = d_sels;
     hw.fks = d_fks;
     hw.vars = d_vars;
+    hw.pair = d_pair;
     CKW(cudaMemcpyAsync(d_info, &hw, sizeof(WideInfo), cudaMemcpyHostToDevice, stream));
+    CKW(cudaMemcpyAsync(d_pair, h_pair.data(), h_pair.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
     if (n_ec) {
         CKW(cudaMemcpyAsync(d_relids, h_relids.data(), n_ec * 8, cudaMemcpyHostToDevice, stream));
         CKW(cudaMemcpyAsync(d_off, h_off.data(), n_ec * 4, cudaMemcpyHostToDevice, stream));
@@ -800,121 +1221,120 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         CKW(cudaMemcpyAsync(d_fks, h_fks.data(), n_fks * 8, cudaMemcpyHostToDevice, stream));
         CKW(cudaMemcpyAsync(d_vars, h_vars.data(), n_fks * sizeof(DevVar), cudaMemcpyHostToDevice, stream));
     }
-    CKW(cudaMemcpyAsync(d_sets, all.data(), (size_t)total * 8, cudaMemcpyHostToDevice, stream));
+    if (tree) CKW(cudaMemcpyAsync(d_sets, singles.data(), (size_t)n * 8, cudaMemcpyHostToDevice, stream));
+    else CKW(cudaMemcpyAsync(d_sets, all.data(), (size_t)total * 8, cudaMemcpyHostToDevice, stream));
     CKW(cudaMemsetAsync(d_keys, 0, cap * 8, stream));
     CKW(cudaMemsetAsync(d_pairs, 0, 16, stream));
-    CKW(cudaMemsetAsync(d_err, 0, 4, stream));
+    CKW(cudaMemsetAsync(d_err, 0, (size_t)(n + 2) * 4, stream));
     {
         WideTable t{d_keys, d_slot, cap_log2};
+        const int index_order = mode == kModeDpsub ? 1 : 0;
+        auto grid_for = [&](uint64_t threads) {
+            return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count * 8, (threads + 255) / 256));
+        };
         CKW(cudaEventRecord(ev0, stream));
-        const uint32_t ib = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8, (total + 255) / 256);
-        k_wide_insert<<<ib, 256, 0, stream>>>(t, d_sets, total, d_err);
-        k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
         CKW(cudaFuncSetAttribute(k_wide_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvalSmem));
-        launches += 2;
-        // refuse before the levels when the DP would evaluate too many splits
-        // (a large biconnected block that is not a cycle); a cactus graph
-        // cannot: every block of a connected set lies in a block of the graph,
-        // so its blocks are bridges and whole cycles, at most 63 * 62 splits
-        if (!cactus) {
-            k_wide_work<<<ib, 256, 0, stream>>>(d_info, d_sets, total, d_pairs + 1);
-            launches++;
+        if (tree) {
+            // level 1, then per level: list level k + 1 into the table, evaluate it
+            const WideTree tt{d_tsub, d_tbefore, d_tanc, d_tpar};
+            k_wide_insert<<<1, 64, 0, stream>>>(t, d_sets, 0u, (uint32_t)n, d_err);
+            k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
+            launches += 2;
+            for (int k = 1; k < n; k++) {
+                const uint32_t first = lvl_off[k - 1], count = lvl_off[k] - lvl_off[k - 1];
+                const uint32_t nfirst = lvl_off[k], ncount = lvl_off[k + 1] - lvl_off[k];
+                k_wide_tree_enum<<<grid_for(count), 256, 0, stream>>>(d_info, t, d_sets, first, count, nfirst,
+                                                                     ncount, d_err + k + 1, d_err);
+                const int E = k;   // split edges of a (k + 1)-set
+                int G = 1;
+                while (G < E && G < 32) G <<= 1;
+                k_wide_eval_tree<<<grid_for((uint64_t)ncount * (uint64_t)G), kWideBlock, kWideInfoBytes, stream>>>(
+                    d_info, t, tt, d_sets, nfirst, ncount, k + 1, G, index_order, d_memo, d_left, d_pairs, d_err);
+                launches += 2;
+                CKW(cudaGetLastError());
+            }
+        } else {
+            k_wide_insert<<<grid_for(total), 256, 0, stream>>>(t, d_sets, 0u, total, d_err);
+            k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
+            launches += 2;
+            // refuse before the levels when the DP would evaluate too many splits
+            // (a large biconnected block that is not a cycle); a cactus graph
+            // cannot: every block of a connected set lies in a block of the graph,
+            // so its blocks are bridges and whole cycles, at most 63 * 62 splits
+            if (!cactus) {
+                k_wide_work<<<grid_for(total), 256, 0, stream>>>(d_info, d_sets, total, d_pairs + 1);
+                launches++;
+                CKW(cudaGetLastError());
+                CKW(cudaMemcpyAsync(&h_work, d_pairs + 1, 8, cudaMemcpyDeviceToHost, stream));
+                CKW(cudaStreamSynchronize(stream));
+            }
             CKW(cudaGetLastError());
-            CKW(cudaMemcpyAsync(&h_work, d_pairs + 1, 8, cudaMemcpyDeviceToHost, stream));
-            CKW(cudaStreamSynchronize(stream));
+            if (h_work > kWideMaxTotal) {
+                err = "the sparse exact DP would evaluate more than " + std::to_string(h_work) +
+                      " candidate splits (a large biconnected block that is not a cycle; the bound is 2^35, 2^24 "
+                      "per set): use IDP";
+                rc = GPUQO_B200_ERR_TOO_LARGE;
+                goto done;
+            }
+            for (int k = 2; k <= n; k++) {
+                const uint32_t first = lvl_off[k - 1], count = lvl_off[k] - lvl_off[k - 1];
+                if (count == 0) continue;
+                launches++;
+                k_wide_eval<<<grid_for((uint64_t)count * 32), kWideBlock, kEvalSmem, stream>>>(
+                    d_info, t, d_sets, first, count, index_order, d_memo, d_left, d_pairs, d_err);
+                CKW(cudaGetLastError());
+            }
         }
+        k_wide_extract<<<1, 32, 0, stream>>>(t, d_memo, d_left, full, n, hw.h.hz_packed ? kWidthMask : 0xFFFFFFFFu,
+                                             d_nodes, d_nn, d_err);
+        launches++;
         CKW(cudaGetLastError());
-        if (h_work > kWideMaxTotal) {
-            err = "the sparse exact DP would evaluate more than " + std::to_string(h_work) +
-                  " candidate splits (a large biconnected block that is not a cycle; the bound is 2^35, 2^24 per "
-                  "set): use IDP";
-            rc = GPUQO_B200_ERR_TOO_LARGE;
-            goto done;
-        }
-        for (int k = 2; k <= n; k++) {
-            const uint32_t first = lvl_off[k - 1], count = lvl_off[k] - lvl_off[k - 1];
-            if (count == 0) continue;
-            launches++;
-            const uint32_t blocks = (uint32_t)std::min<uint64_t>((uint64_t)sm_count * 8,
-                                                                 ((uint64_t)count * 32 + kWideBlock - 1) / kWideBlock);
-            k_wide_eval<<<blocks, kWideBlock, kEvalSmem, stream>>>(d_info, t, d_sets, first, count,
-                                                           mode == kModeDpsub ? 1 : 0, d_memo, d_left, d_pairs,
-                                                           d_err);
-            CKW(cudaGetLastError());
-        }
         CKW(cudaEventRecord(ev1, stream));
     }
-    h_memo.resize(total);
-    h_left.resize(total);
-    CKW(cudaMemcpyAsync(h_memo.data(), d_memo, (size_t)total * sizeof(float4), cudaMemcpyDeviceToHost, stream));
-    CKW(cudaMemcpyAsync(h_left.data(), d_left, (size_t)total * 8, cudaMemcpyDeviceToHost, stream));
-    CKW(cudaMemcpyAsync(&h_err, d_err, 4, cudaMemcpyDeviceToHost, stream));
+    nodes.resize(128);
+    CKW(cudaMemcpyAsync(nodes.data(), d_nodes, 128 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream));
+    CKW(cudaMemcpyAsync(&h_nn, d_nn, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CKW(cudaMemcpyAsync(h_err.data(), d_err, (size_t)(n + 2) * 4, cudaMemcpyDeviceToHost, stream));
     CKW(cudaMemcpyAsync(&h_pairs, d_pairs, 8, cudaMemcpyDeviceToHost, stream));
     CKW(cudaStreamSynchronize(stream));
     CKW(cudaEventElapsedTime(&ms, ev0, ev1));
-    if (h_err) {
-        err = h_err == 3 ? "a connected set with more than 2^24 candidate splits (a dense biconnected block): "
-                           "beyond the sparse exact DP (use IDP)"
-                         : "sparse memo table inconsistent";
-        rc = h_err == 3 ? GPUQO_B200_ERR_TOO_LARGE : GPUQO_B200_ERR_CUDA;
+    if (h_err[0]) {
+        err = h_err[0] == 3 ? "a connected set with more than 2^24 candidate splits (a dense biconnected block): "
+                              "beyond the sparse exact DP (use IDP)"
+                            : "sparse memo table inconsistent";
+        rc = h_err[0] == 3 ? GPUQO_B200_ERR_TOO_LARGE : GPUQO_B200_ERR_CUDA;
         goto done;
     }
-    {
-        // plan: walk the outer sides from the full set (host, sorted slots)
-        auto slot_of = [&](uint64_t s) -> uint32_t {
-            const int k = __builtin_popcountll(s);
-            auto b = all.begin() + lvl_off[k - 1], e = all.begin() + lvl_off[k];
-            return (uint32_t)(std::lower_bound(b, e, s) - all.begin());
-        };
-        const uint32_t wmask = hw.h.hz_packed ? kWidthMask : 0xFFFFFFFFu;
-        nodes.clear();
-        std::vector<std::pair<uint64_t, std::pair<int, int>>> stack;   // set, (parent, side)
-        stack.push_back({full, {-1, 0}});
-        while (!stack.empty() && nodes.size() < 2 * (size_t)n) {
-            const auto it = stack.back();
-            stack.pop_back();
-            const uint64_t s = it.first;
-            const uint32_t sl = slot_of(s);
-            const float4 v = h_memo[sl];
-            TreeNode t;
-            t.set = s;
-            t.left = t.right = -1;
-            t.rows = v.x;
-            t.startup = v.y;
-            t.total = v.z;
-            uint32_t wb;
-            std::memcpy(&wb, &v.w, 4);
-            t.width = (int32_t)(wb & wmask);
-            const int me = (int)nodes.size();
-            nodes.push_back(t);
-            if (it.second.first >= 0) {
-                if (it.second.second == 0) nodes[(size_t)it.second.first].left = me;
-                else nodes[(size_t)it.second.first].right = me;
-            }
-            const uint64_t l = h_left[sl] & s;
-            if (__builtin_popcountll(s) > 1 && l != 0 && l != s) {
-                stack.push_back({s ^ l, {me, 1}});
-                stack.push_back({l, {me, 0}});
+    if (tree) {
+        for (int k = 2; k <= n; k++) {
+            if (h_err[k] != lvl_off[k] - lvl_off[k - 1]) {
+                err = "tree enumeration listed " + std::to_string(h_err[k]) + " sets of " + std::to_string(k) +
+                      " relations where " + std::to_string(lvl_off[k] - lvl_off[k - 1]) + " exist";
+                rc = GPUQO_B200_ERR_CUDA;
+                goto done;
             }
         }
-        if (nodes.size() != 2 * (size_t)n - 1) {
-            err = "plan extraction produced " + std::to_string(nodes.size()) + " nodes";
-            rc = GPUQO_B200_ERR_CUDA;
-            goto done;
-        }
-        st.connected_sets += total - (uint32_t)n;
-        st.evaluated_pairs += h_pairs;
-        st.memo_bytes = std::max<uint64_t>(st.memo_bytes, bytes);
-        st.device_ms += ms;
-        st.kernel_launches += launches;
     }
+    if (h_nn != 2 * n - 1) {
+        err = "plan extraction produced " + std::to_string(h_nn) + " nodes";
+        rc = GPUQO_B200_ERR_CUDA;
+        goto done;
+    }
+    nodes.resize((size_t)h_nn);
+    st.connected_sets += total - (uint32_t)n;
+    st.evaluated_pairs += h_pairs;
+    st.memo_bytes = std::max<uint64_t>(st.memo_bytes, bytes);
+    st.device_ms += ms;
+    st.kernel_launches += launches;
 done:
+    if (rc) nodes.clear();
     cudaFree(d_info);
     cudaFree(d_relids);
     cudaFree(d_off);
     cudaFree(d_sels);
     cudaFree(d_fks);
     cudaFree(d_vars);
+    cudaFree(d_pair);
     cudaFree(d_keys);
     cudaFree(d_slot);
     cudaFree(d_sets);
@@ -922,6 +1342,12 @@ done:
     cudaFree(d_left);
     cudaFree(d_pairs);
     cudaFree(d_err);
+    cudaFree(d_nodes);
+    cudaFree(d_nn);
+    cudaFree(d_tsub);
+    cudaFree(d_tbefore);
+    cudaFree(d_tanc);
+    cudaFree(d_tpar);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);

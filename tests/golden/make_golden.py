@@ -132,7 +132,10 @@ def wide_cases():
             ("wide_lollipop40", query.lollipop(40, 4), DPCCP, 0, 1),
             ("wide_lollipop63_rich", query.lollipop(63, 7, rich=True), DPCCP, 0, 1),
             ("wide_ring_path40", query.ring_path(40, 3), DPCCP, 0, 1),
-            ("wide_ring_path36_rich", query.ring_path(36, 10, rich=True), DPCCP, 0, 1)]
+            ("wide_ring_path36_rich", query.ring_path(36, 10, rich=True), DPCCP, 0, 1),
+            # the snowflake workload beyond the dense memo: 1.2 M and 2.4 M connected sets
+            ("wide_snowflake32", query.snowflake(32, 1), DPCCP, 0, 1),
+            ("wide_snowflake34", query.snowflake(34, 5), DPCCP, 0, 1)]
 
 
 def tree_json(t):

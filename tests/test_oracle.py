@@ -85,7 +85,9 @@ def test_sparse_driver_matches_golden(sparse_from):
         assert same_tree(tree, c["expected"]), (c["tag"], c["name"], c["algorithm"])
 
 
-WIDE = load_golden("wide_cases.jsonl")
+# the snowflakes of 32 and 34 relations (1.2 M and 2.4 M connected sets) take
+# the oracle minutes; the GPU tests compare them
+WIDE = [c for c in load_golden("wide_cases.jsonl") if not c["tag"].startswith("wide_snowflake")]
 
 
 @pytest.mark.parametrize("case", WIDE, ids=[c["tag"] for c in WIDE])
