@@ -129,11 +129,17 @@ typedef struct QueryTreeC {
  *   (GPUQO_CPU_DPSUB, GPUQO_CPU_DPSUB_BICC and their parallel/DPE variants)
  *   return the same plans as the reference's CPU engines; they are served by
  *   the same GPU kernels (plain DPsub for *_DPSUB, MPDP for *_BICC*).
- *   Other codes (DPsize, DPccp, heuristics) are outside this library's
- *   scope and return NULL with a message, as the reference does for
- *   unsupported combinations (gpuqo_main_internal.cu:75-78).
+ *   GPUQO_DPSIZE, GPUQO_CPU_DPSIZE and GPUQO_DPE_DPSIZE return the plans of
+ *   the reference's cpu_dpsize (up to 31 relations).  Other codes (DPccp,
+ *   heuristics) are outside this library's scope and return NULL with a
+ *   message, as the reference does for unsupported combinations
+ *   (gpuqo_main_internal.cu:75-78).
+ * Exact DP: up to 31 relations on a dense memo; DPsub and MPDP of 32 to 63
+ *   relations on a sparse memo over the connected sets
+ *   (gpuqo_b200_sparse_from_rels).
  * IDP: when 1 < gpuqo_idp_n_iters < n_rels, gpuqo_idp_type selects IDP2
- *   (gpuqo_idp.cu:260) or UnionDP (gpuqo_dpdp_union.cu:448) over the GPU DP.
+ *   (gpuqo_idp.cu:260) or UnionDP (gpuqo_dpdp_union.cu:448) over the GPU DP;
+ *   sub-problems of up to 63 relations.
  *
  * The input is borrowed.  The returned tree and every id Bitmapset are
  * palloc'd (inside Postgres: the caller's memory context; standalone: the
