@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <string>
 #include <unordered_set>
 #include <vector>
@@ -66,6 +67,11 @@ struct WideInfo {
     // variables carry no statistics and no index: bucket size 0.1, MCV
     // frequency 0); w unused
     const float4 *pair;
+    // a tree whose classes all have two members on an edge (at most 64
+    // classes): edge_cls[v] = the classes on the edge between v and its
+    // parent in the tree rooted at relation 0
+    int edge_masked;
+    uint64_t edge_cls[64];
 };
 constexpr size_t kWideInfoBytes = (sizeof(WideInfo) + 15) & ~size_t(15);
 
@@ -299,8 +305,20 @@ __device__ float ec_selectivity64(const WideInfo &w, int i, uint64_t ec, uint64_
     return w.sels[off_sels + il * size - il * (il + 1) / 2 + (ir - il - 1)];
 }
 
-// join_eval_t's general path (every class, in class order) on 64-bit sets
-__device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, uint64_t R, const RelVal &r) {
+// join_eval_t's general path on 64-bit sets, the classes in class order:
+// every class, or (MASKED) only the classes in cmask, which must hold every
+// class with a member on each side (a tree whose classes all sit on edges:
+// the classes of the split edge)
+template <bool MASKED>
+__device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, uint64_t R, const RelVal &r,
+                              uint64_t cmask = 0ull) {
+    auto for_classes = [&](auto &&body) {
+        if (MASKED) {
+            for (uint64_t m = cmask; m; m &= m - 1ull) body(lowest_idx64(m));
+        } else {
+            for (int i = 0; i < w.n_ec; i++) body(i);
+        }
+    };
     const DevHeader &h = w.h;
     const bool inner_single = (R & (R - 1ull)) == 0ull;
     Htsz hz;
@@ -314,10 +332,10 @@ __device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, ui
     float sel = 1.0f, per_tuple = 0.0f, bucketsize = 1.0f, mcvfreq = 1.0f;
     int n_quals = 0;
     bool inner_unique = false, any_index = false;
-    for (int i = 0; i < w.n_ec; i++) {
+    for_classes([&](int i) {
         const uint64_t ec = w.ec_relids[i];
         const uint64_t ml = ec & L, mr = ec & R;
-        if (!ml || !mr) continue;
+        if (!ml || !mr) return;
         const float4 pf = __ldg(w.pair + i);
         if (__float_as_uint(pf.z) != 0u) {
             // a plain class: what the general steps below compute for it
@@ -326,7 +344,7 @@ __device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, ui
             n_quals++;
             if (bucketsize > 0.1f) bucketsize = 0.1f;
             if (mcvfreq > 0.0f) mcvfreq = 0.0f;
-            continue;
+            return;
         }
         sel *= ec_selectivity64(w, i, ec, ml, mr);
         per_tuple += h.cpu_operator_cost;
@@ -345,7 +363,7 @@ __device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, ui
             if (bucketsize > this_bs) bucketsize = this_bs;
             if (mcvfreq > v.mcvfreq) mcvfreq = v.mcvfreq;
         }
-    }
+    });
     RelVal out;
     const float rows = sel * l.rows * r.rows;
     out.rows = rows > 1.0f ? roundf(rows) : 1.0f;
@@ -367,19 +385,19 @@ __device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, ui
     }
     if (any_index && !((w.composite >> lowest_idx64(R)) & 1ull)) {
         extra.indexed_join_quals = true;
-        for (int i = 0; i < w.n_ec; i++) {
+        for_classes([&](int i) {
             const uint64_t ec = w.ec_relids[i];
             const uint64_t ml = ec & L, mr = ec & R;
-            if (!ml || !mr) continue;
+            if (!ml || !mr) return;
             const int off_fks = (int)(w.ec_off[i] & 0xFFFFu);
             const DevVar v = w.vars[off_fks + __popcll((lowest64(mr) - 1ull) & ec)];
-            if (!(v.flags & 1u)) continue;
+            if (!(v.flags & 1u)) return;
             cost_nestloop(h, l, v.idx_rows, v.idx_startup, v.idx_total, extra, per_tuple, s, t);
             if (t < min_t) {
                 min_s = s;
                 min_t = t;
             }
-        }
+        });
     }
     out.startup = min_s;
     out.total = min_t;
@@ -489,7 +507,7 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval(const WideInfo *__rest
             if (index_order) key = dpsub_index64(L, S);
             const RelVal l = wide_rel(memo, wide_lookup(t, L, err), w.h.hz_packed);
             const RelVal r = wide_rel(memo, wide_lookup(t, R, err), w.h.hz_packed);
-            const RelVal out = join_eval_w(w, L, l, R, r);
+            const RelVal out = join_eval_w<false>(w, L, l, R, r);
             const bool nan = isnan(out.total);
             pairs++;
             if (key < first_k) {
@@ -739,8 +757,15 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval_tree(const WideInfo *_
             }
             const RelVal lv = wide_rel(memo, wide_lookup(t, L0, err), w.h.hz_packed);
             const RelVal rv = wide_rel(memo, wide_lookup(t, R0, err), w.h.hz_packed);
-            update(k0, L0, join_eval_w(w, L0, lv, R0, rv));
-            update(k1, R0, join_eval_w(w, R0, rv, L0, lv));
+            if (w.edge_masked) {
+                const int child0 = ((__ldg(tt.anc + v) >> p) & 1ull) ? v : p;   // w.r.t. relation 0
+                const uint64_t cm = w.edge_cls[child0];
+                update(k0, L0, join_eval_w<true>(w, L0, lv, R0, rv, cm));
+                update(k1, R0, join_eval_w<true>(w, R0, rv, L0, lv, cm));
+            } else {
+                update(k0, L0, join_eval_w<false>(w, L0, lv, R0, rv));
+                update(k1, R0, join_eval_w<false>(w, R0, rv, L0, lv));
+            }
             pairs += 2;
         }
         // group minimum of (cost, index) and of the first index (butterfly
@@ -893,6 +918,35 @@ static bool is_cactus(const std::vector<uint64_t> &adj) {
     return ok;
 }
 
+// Device state of the sparse DP, kept per device across calls: grow-only
+// buffers, a stream and two events.  One sparse DP at a time per device
+// (its mutex); the buffers stay allocated for the next call, as the dense
+// engine's arenas do.
+struct WideArena {
+    std::mutex mu;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void *buf[24] = {};
+    size_t cap[24] = {};
+};
+static WideArena g_wide_arena[64];
+
+static cudaError_t arena_get(WideArena &a, int idx, size_t bytes, void **out) {
+    if (a.cap[idx] < bytes) {
+        if (a.buf[idx]) cudaFree(a.buf[idx]);
+        a.buf[idx] = nullptr;
+        a.cap[idx] = 0;
+        const cudaError_t e = cudaMalloc(&a.buf[idx], bytes);
+        if (e != cudaSuccess) {
+            a.buf[idx] = nullptr;
+            return e;
+        }
+        a.cap[idx] = bytes;
+    }
+    *out = a.buf[idx];
+    return cudaSuccess;
+}
+
 // Connected sets of a tree per size (index 1..n), counted without listing
 // them: g_v(x) = x * prod over v's children c of (1 + g_c(x)) counts the sets
 // whose relation nearest the root is v; doubles, exact below 2^53.
@@ -1038,18 +1092,43 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
             all.insert(all.end(), cur.begin(), cur.end());
             lvl_off.push_back((uint32_t)all.size());
             if (k == n) break;
-            std::unordered_set<uint64_t> next;
-            next.reserve(cur.size() * 4);
+            // level k + 1, deduplicated in a flat open-addressing set (0 is
+            // never a set), doubled when half full
+            std::vector<uint64_t> table(64, 0ull), next;
+            size_t used = 0;
+            auto slot_of = [](uint64_t key, size_t mask) {
+                return (size_t)((key * 0x9E3779B97F4A7C15ull) >> 32) & mask;
+            };
+            auto add = [&](uint64_t key) {
+                if (2 * (used + 1) > table.size()) {
+                    std::vector<uint64_t> bigger(table.size() * 2, 0ull);
+                    for (uint64_t kk : table) {
+                        if (!kk) continue;
+                        size_t j = slot_of(kk, bigger.size() - 1);
+                        while (bigger[j]) j = (j + 1) & (bigger.size() - 1);
+                        bigger[j] = kk;
+                    }
+                    table.swap(bigger);
+                }
+                size_t j = slot_of(key, table.size() - 1);
+                while (table[j]) {
+                    if (table[j] == key) return;
+                    j = (j + 1) & (table.size() - 1);
+                }
+                table[j] = key;
+                used++;
+                next.push_back(key);
+            };
             for (uint64_t S : cur) {
                 uint64_t N = 0;
                 for (uint64_t x = S; x; x &= x - 1ull) N |= adj[__builtin_ctzll(x)];
                 N &= ~S;
                 for (; N; N &= N - 1ull) {
-                    next.insert(S | (N & (0ull - N)));
+                    add(S | (N & (0ull - N)));
                     if (all.size() + next.size() > cap_sets) return too_many();
                 }
             }
-            cur.assign(next.begin(), next.end());
+            cur.swap(next);
         }
         if (all.back() != full) {
             err = "query graph is not connected";
@@ -1149,7 +1228,26 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     }
     std::vector<uint64_t> t_sub, t_before, t_anc;
     std::vector<uint8_t> t_par;
-    if (tree) tree_tables(adj, t_sub, t_before, t_anc, t_par);
+    if (tree) {
+        tree_tables(adj, t_sub, t_before, t_anc, t_par);
+        bool masked = n_ec <= 64;
+        for (size_t e = 0; masked && e < n_ec; e++) {
+            const uint64_t rr = h_relids[e];
+            if (__builtin_popcountll(rr) != 2) {
+                masked = false;
+                break;
+            }
+            const int a = __builtin_ctzll(rr), b = 63 - __builtin_clzll(rr);
+            if (!((adj[a] >> b) & 1ull)) {
+                masked = false;   // a class between relations that are not adjacent
+                break;
+            }
+            const int child0 = ((t_anc[(size_t)b] >> a) & 1ull) ? b : a;   // row 0: ancestors w.r.t. relation 0
+            hw.edge_cls[child0] |= 1ull << e;
+        }
+        hw.edge_masked = masked ? 1 : 0;
+        if (!masked) std::memset(hw.edge_cls, 0, sizeof(hw.edge_cls));
+    }
     std::vector<uint64_t> singles(n);
     for (int i = 0; i < n; i++) singles[i] = 1ull << i;
     int rc = 0;
@@ -1175,35 +1273,46 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     int sm_count = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
-    CKW(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    CKW(cudaEventCreate(&ev0));
-    CKW(cudaEventCreate(&ev1));
-    CKW(cudaMalloc(&d_info, sizeof(WideInfo)));
-    CKW(cudaMalloc(&d_relids, std::max<size_t>(n_ec, 1) * 8));
-    CKW(cudaMalloc(&d_off, std::max<size_t>(n_ec, 1) * 4));
-    CKW(cudaMalloc(&d_sels, std::max<size_t>(n_sels, 1) * 4));
-    CKW(cudaMalloc(&d_fks, std::max<size_t>(n_fks, 1) * 8));
-    CKW(cudaMalloc(&d_vars, std::max<size_t>(n_fks, 1) * sizeof(DevVar)));
-    CKW(cudaMalloc(&d_pair, h_pair.size() * sizeof(float4)));
-    CKW(cudaMalloc(&d_keys, cap * 8));
-    CKW(cudaMalloc(&d_slot, cap * 4));
-    CKW(cudaMalloc(&d_sets, (size_t)total * 8));
-    CKW(cudaMalloc(&d_memo, (size_t)total * sizeof(float4)));
-    CKW(cudaMalloc(&d_left, (size_t)total * 8));
-    CKW(cudaMalloc(&d_pairs, 16));   // [0] evaluated pairs, [1] the work bound
-    CKW(cudaMalloc(&d_err, (size_t)(n + 2) * 4));
-    CKW(cudaMalloc(&d_nodes, 128 * sizeof(TreeNode)));
-    CKW(cudaMalloc(&d_nn, sizeof(int)));
+    if (dev < 0 || dev >= 64) {
+        err = "device ordinal " + std::to_string(dev) + " beyond the sparse DP's device table";
+        return GPUQO_B200_ERR_ARGS;
+    }
+    WideArena &A = g_wide_arena[dev];
+    std::lock_guard<std::mutex> arena_lock(A.mu);
+    if (!A.stream) CKW(cudaStreamCreateWithFlags(&A.stream, cudaStreamNonBlocking));
+    if (!A.ev0) CKW(cudaEventCreate(&A.ev0));
+    if (!A.ev1) CKW(cudaEventCreate(&A.ev1));
+    stream = A.stream;
+    ev0 = A.ev0;
+    ev1 = A.ev1;
+#define ARENA(i, ptr, bytes) CKW(arena_get(A, i, (size_t)(bytes), reinterpret_cast<void **>(&(ptr))))
+    ARENA(0, d_info, sizeof(WideInfo));
+    ARENA(1, d_relids, std::max<size_t>(n_ec, 1) * 8);
+    ARENA(2, d_off, std::max<size_t>(n_ec, 1) * 4);
+    ARENA(3, d_sels, std::max<size_t>(n_sels, 1) * 4);
+    ARENA(4, d_fks, std::max<size_t>(n_fks, 1) * 8);
+    ARENA(5, d_vars, std::max<size_t>(n_fks, 1) * sizeof(DevVar));
+    ARENA(6, d_pair, h_pair.size() * sizeof(float4));
+    ARENA(7, d_keys, cap * 8);
+    ARENA(8, d_slot, cap * 4);
+    ARENA(9, d_sets, (size_t)total * 8);
+    ARENA(10, d_memo, (size_t)total * sizeof(float4));
+    ARENA(11, d_left, (size_t)total * 8);
+    ARENA(12, d_pairs, 16);   // [0] evaluated pairs, [1] the work bound
+    ARENA(13, d_err, (size_t)(n + 2) * 4);
+    ARENA(14, d_nodes, 128 * sizeof(TreeNode));
+    ARENA(15, d_nn, sizeof(int));
     if (tree) {
-        CKW(cudaMalloc(&d_tsub, (size_t)n * n * 8));
-        CKW(cudaMalloc(&d_tbefore, (size_t)n * n * 8));
-        CKW(cudaMalloc(&d_tanc, (size_t)n * n * 8));
-        CKW(cudaMalloc(&d_tpar, (size_t)n * n));
+        ARENA(16, d_tsub, (size_t)n * n * 8);
+        ARENA(17, d_tbefore, (size_t)n * n * 8);
+        ARENA(18, d_tanc, (size_t)n * n * 8);
+        ARENA(19, d_tpar, (size_t)n * n);
         CKW(cudaMemcpyAsync(d_tsub, t_sub.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice, stream));
         CKW(cudaMemcpyAsync(d_tbefore, t_before.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice, stream));
         CKW(cudaMemcpyAsync(d_tanc, t_anc.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice, stream));
         CKW(cudaMemcpyAsync(d_tpar, t_par.data(), (size_t)n * n, cudaMemcpyHostToDevice, stream));
     }
+#undef ARENA
     hw.ec_relids = d_relids;
     hw.ec_off = d_off;
     hw.sels = d_sels;
@@ -1245,9 +1354,13 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
                 const uint32_t nfirst = lvl_off[k], ncount = lvl_off[k + 1] - lvl_off[k];
                 k_wide_tree_enum<<<grid_for(count), 256, 0, stream>>>(d_info, t, d_sets, first, count, nfirst,
                                                                      ncount, d_err + k + 1, d_err);
+                // lanes per set: as few as keep about two warps' worth of sets
+                // per resident warp slot (a lane walks its set's edges one after
+                // the other: fewer warp rounds per set), up to one lane per edge
                 const int E = k;   // split edges of a (k + 1)-set
+                const uint64_t want_lanes = (uint64_t)sm_count * 24u * 32u * 2u;
                 int G = 1;
-                while (G < E && G < 32) G <<= 1;
+                while (G < E && G < 32 && (uint64_t)ncount * (uint64_t)G < want_lanes) G <<= 1;
                 k_wide_eval_tree<<<grid_for((uint64_t)ncount * (uint64_t)G), kWideBlock, kWideInfoBytes, stream>>>(
                     d_info, t, tt, d_sets, nfirst, ncount, k + 1, G, index_order, d_memo, d_left, d_pairs, d_err);
                 launches += 2;
@@ -1328,29 +1441,7 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     st.kernel_launches += launches;
 done:
     if (rc) nodes.clear();
-    cudaFree(d_info);
-    cudaFree(d_relids);
-    cudaFree(d_off);
-    cudaFree(d_sels);
-    cudaFree(d_fks);
-    cudaFree(d_vars);
-    cudaFree(d_pair);
-    cudaFree(d_keys);
-    cudaFree(d_slot);
-    cudaFree(d_sets);
-    cudaFree(d_memo);
-    cudaFree(d_left);
-    cudaFree(d_pairs);
-    cudaFree(d_err);
-    cudaFree(d_nodes);
-    cudaFree(d_nn);
-    cudaFree(d_tsub);
-    cudaFree(d_tbefore);
-    cudaFree(d_tanc);
-    cudaFree(d_tpar);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (stream) cudaStreamDestroy(stream);
+    // device buffers, stream and events stay in the device's arena
     return rc;
 }
 
