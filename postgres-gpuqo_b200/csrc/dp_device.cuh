@@ -434,10 +434,26 @@ __device__ __forceinline__ RelVal join_eval_t(const DevInfoView &d, uint32_t L, 
         uint32_t ml = ec & L, mr = ec & R;
         if (!ml || !mr) continue;
         // MASKED: a two-member class with one member on each side; its
-        // ec_selectivity for this orientation is tabulated in the header
-        sel *= MASKED ? h.edge_sel[ml > mr ? 1 : 0][i] : ec_selectivity(d, i, ec, ml, mr);
+        // ec_selectivity for this orientation is tabulated in the header.  A
+        // plain class (DevInfoView::plain) takes its pair selectivity, and its
+        // inner member's variable would give bucket size 0.1 and MCV
+        // frequency 0 without an index: set directly, the member not read.
+        const bool plain = (d.plain[i >> 5] >> (i & 31)) & 1u;
+        if (MASKED) {
+            sel *= h.edge_sel[ml > mr ? 1 : 0][i];
+        } else if (plain) {
+            const float2 ps = *reinterpret_cast<const float2 *>(d.pair_sel + 2 * i);
+            sel *= (lowest(ec) & L) ? ps.x : ps.y;
+        } else {
+            sel *= ec_selectivity(d, i, ec, ml, mr);
+        }
         per_tuple += h.cpu_operator_cost;
         n_quals++;
+        if (plain) {
+            if (bucketsize > 0.1f) bucketsize = 0.1f;
+            if (mcvfreq > 0.0f) mcvfreq = 0.0f;
+            continue;
+        }
         int off_fks = (int)(d.ec_off[i] & 0xFFFFu);
         uint32_t m = mr;
         bool first = true;
