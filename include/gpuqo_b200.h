@@ -253,6 +253,13 @@ extern int gpuqo_b200_device_memory_mb;
  * above 63 keeps the default. */
 extern int gpuqo_b200_sparse_from_rels;
 
+/* Connected sets the host lists for a sparse-memo DP of a graph that is not
+ * a tree before it hands the listing to the device (level by level, the
+ * device table deduplicating; the arrays are then sized for the sparse memo's
+ * whole capacity).  0 (default): 65536.  Trees are always listed on the
+ * device.  Plans do not depend on it. */
+extern int gpuqo_b200_sparse_host_list;
+
 /*
  * Device-resident timing of the exact DP of one query (< 32 relations, no
  * IDP): the planner info is converted and uploaded once, then the captured DP

@@ -20,6 +20,7 @@
 //     split in cpu_dpsub's subset order (gpuqo_cpu_dpsub.cu:32-78), which
 //     selects the same first strict minimum over the valid pairs only.
 // The plan is read back from the memo on the host.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,6 +39,7 @@
 #include "host_info.h"
 
 extern "C" int gpuqo_b200_device_memory_mb;
+extern "C" int gpuqo_b200_sparse_host_list;
 
 namespace gqb {
 
@@ -815,6 +817,56 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval_tree(const WideInfo *_
     if (lane == 0 && pairs) atomicAdd(pairs_out, pairs);
 }
 
+// level k + 1 of any graph from level k, listed on the device: every
+// extension of a set by one neighbour is offered to the table, and the thread
+// whose atomicCAS claims the key appends the set (so each connected set is
+// listed once, whichever of its subsets offered it first).  Indices from
+// out_first on; an index at or beyond out_cap raises err 6 instead of writing.
+__global__ void __launch_bounds__(256) k_wide_list_ext(const WideInfo *__restrict__ wi, WideTable t,
+                                                       unsigned long long *__restrict__ sets, uint32_t first,
+                                                       uint32_t count, uint32_t out_first, uint32_t out_cap,
+                                                       unsigned *__restrict__ out_n, unsigned *__restrict__ err) {
+    namespace cg = cooperative_groups;
+    __shared__ unsigned long long adj[64];
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) adj[i] = wi->adj[i];
+    __syncthreads();
+    const uint32_t cap = 1u << t.cap_log2;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint64_t S = sets[first + i];
+        uint64_t N = 0ull;
+        for (uint64_t x = S; x; x &= x - 1ull) N |= adj[lowest_idx64(x)];
+        N &= ~S;
+        for (; N; N &= N - 1ull) {
+            const unsigned long long T = S | lowest64(N);
+            uint32_t pos = wide_hash(T, t.cap_log2);
+            bool done = false;
+            for (uint32_t probe = 0; probe < cap && !done; probe++) {
+                const unsigned long long old = atomicCAS(t.keys + pos, 0ull, T);
+                if (old == 0ull) {
+                    // claimed: append (one counter update per group of claimers)
+                    cg::coalesced_group g = cg::coalesced_threads();
+                    unsigned base = 0;
+                    if (g.thread_rank() == 0) base = atomicAdd(out_n, g.size());
+                    base = g.shfl(base, 0);
+                    const uint32_t idx = out_first + base + g.thread_rank();
+                    if (idx < out_cap) {
+                        sets[idx] = T;
+                        t.slot[pos] = idx;
+                    } else {
+                        atomicExch(err, 6u);
+                    }
+                    done = true;
+                } else if (old == T) {
+                    done = true;   // listed already
+                } else {
+                    pos = (pos + 1u) & (cap - 1u);
+                }
+            }
+            if (!done) atomicExch(err, 1u);
+        }
+    }
+}
+
 // the plan, walked from the full set by one thread (at most 2n - 1 nodes)
 __global__ void k_wide_extract(WideTable t, const float4 *__restrict__ memo,
                                const unsigned long long *__restrict__ memo_left, uint64_t full, int n,
@@ -1072,6 +1124,8 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
     // on the device level by level (k_wide_tree_enum); other graphs' are
     // listed on the host by extension with one neighbour, deduplicated.
     const bool tree = degree_sum == 2 * (n - 1);
+    const uint64_t kHostListMax = gpuqo_b200_sparse_host_list > 0 ? (uint64_t)gpuqo_b200_sparse_host_list : (1ull << 16);
+    bool dev_list = false;   // a general graph whose levels the device lists
     std::vector<uint64_t> all;
     std::vector<uint32_t> lvl_off(1, 0);
     if (tree) {
@@ -1085,10 +1139,23 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         if (tot > (double)cap_sets) return too_many();
         for (int k = 1; k <= n; k++) lvl_off.push_back(lvl_off.back() + (uint32_t)cnt[k]);
     } else {
+        // the host lists up to kHostListMax sets; beyond that the device lists
+        // the levels itself (k_wide_list_ext) into arrays of cap_sets entries
+        const uint64_t host_max = std::min<uint64_t>(cap_sets, kHostListMax);
+        auto over = [&]() -> int {
+            if (host_max < cap_sets) {
+                dev_list = true;
+                return 0;
+            }
+            return (int)too_many();
+        };
         std::vector<uint64_t> cur;
         for (int i = 0; i < n; i++) cur.push_back(1ull << i);
-        for (int k = 1; k <= n; k++) {
-            if (all.size() + cur.size() > cap_sets) return too_many();
+        for (int k = 1; k <= n && !dev_list; k++) {
+            if (all.size() + cur.size() > host_max) {
+                if (int rc = over()) return rc;
+                break;
+            }
             all.insert(all.end(), cur.begin(), cur.end());
             lvl_off.push_back((uint32_t)all.size());
             if (k == n) break;
@@ -1119,24 +1186,33 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
                 used++;
                 next.push_back(key);
             };
-            for (uint64_t S : cur) {
+            for (size_t q = 0; q < cur.size() && !dev_list; q++) {
+                const uint64_t S = cur[q];
                 uint64_t N = 0;
                 for (uint64_t x = S; x; x &= x - 1ull) N |= adj[__builtin_ctzll(x)];
                 N &= ~S;
-                for (; N; N &= N - 1ull) {
+                for (; N && !dev_list; N &= N - 1ull) {
                     add(S | (N & (0ull - N)));
-                    if (all.size() + next.size() > cap_sets) return too_many();
+                    if (all.size() + next.size() > host_max)
+                        if (int rc = over()) return rc;
                 }
             }
             cur.swap(next);
         }
-        if (all.back() != full) {
+        if (dev_list) {
+            all.clear();
+            for (int i = 0; i < n; i++) all.push_back(1ull << i);
+            lvl_off.assign({0u, (uint32_t)n});
+        } else if (all.back() != full) {
             err = "query graph is not connected";
             return GPUQO_B200_ERR_ARGS;
         }
     }
     const bool cactus = tree || is_cactus(adj);
-    const uint32_t total = lvl_off[n];
+    // entries of the set, memo and left arrays (the listed total, or the cap
+    // when the device lists)
+    const uint32_t total = dev_list ? (uint32_t)cap_sets : lvl_off[n];
+    uint32_t listed = dev_list ? (uint32_t)n : total;
     uint32_t cap_log2 = 1;
     while ((1ull << cap_log2) < 2ull * total) cap_log2++;
     const uint64_t cap = 1ull << cap_log2;
@@ -1331,7 +1407,7 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         CKW(cudaMemcpyAsync(d_vars, h_vars.data(), n_fks * sizeof(DevVar), cudaMemcpyHostToDevice, stream));
     }
     if (tree) CKW(cudaMemcpyAsync(d_sets, singles.data(), (size_t)n * 8, cudaMemcpyHostToDevice, stream));
-    else CKW(cudaMemcpyAsync(d_sets, all.data(), (size_t)total * 8, cudaMemcpyHostToDevice, stream));
+    else CKW(cudaMemcpyAsync(d_sets, all.data(), all.size() * 8, cudaMemcpyHostToDevice, stream));
     CKW(cudaMemsetAsync(d_keys, 0, cap * 8, stream));
     CKW(cudaMemsetAsync(d_pairs, 0, 16, stream));
     CKW(cudaMemsetAsync(d_err, 0, (size_t)(n + 2) * 4, stream));
@@ -1365,6 +1441,60 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
                     d_info, t, tt, d_sets, nfirst, ncount, k + 1, G, index_order, d_memo, d_left, d_pairs, d_err);
                 launches += 2;
                 CKW(cudaGetLastError());
+            }
+        } else if (dev_list) {
+            // level 1, then per level: list level k + 1 on the device (the table
+            // deduplicates), read its size back, check the work bound (graphs
+            // that are not cacti), evaluate it
+            k_wide_insert<<<1, 64, 0, stream>>>(t, d_sets, 0u, (uint32_t)n, d_err);
+            k_wide_base<<<1, 64, 0, stream>>>(d_info, t, d_memo, d_left, d_err);
+            launches += 2;
+            uint32_t first = 0, count = (uint32_t)n;
+            for (int k = 1; k < n; k++) {
+                k_wide_list_ext<<<grid_for(count), 256, 0, stream>>>(d_info, t, d_sets, first, count, listed,
+                                                                    total, d_err + k + 1, d_err);
+                launches++;
+                CKW(cudaGetLastError());
+                unsigned got = 0, flag = 0;
+                CKW(cudaMemcpyAsync(&got, d_err + k + 1, 4, cudaMemcpyDeviceToHost, stream));
+                CKW(cudaMemcpyAsync(&flag, d_err, 4, cudaMemcpyDeviceToHost, stream));
+                CKW(cudaStreamSynchronize(stream));
+                if (flag == 6u || (uint64_t)listed + got > (uint64_t)total) {
+                    rc = too_many();
+                    goto done;
+                }
+                if (flag) {
+                    err = "sparse memo table inconsistent while listing";
+                    rc = GPUQO_B200_ERR_CUDA;
+                    goto done;
+                }
+                first = listed;
+                count = got;
+                listed += got;
+                if (count == 0) break;
+                if (!cactus) {
+                    k_wide_work<<<grid_for(count), 256, 0, stream>>>(d_info, d_sets + first, count, d_pairs + 1);
+                    launches++;
+                    CKW(cudaGetLastError());
+                    CKW(cudaMemcpyAsync(&h_work, d_pairs + 1, 8, cudaMemcpyDeviceToHost, stream));
+                    CKW(cudaStreamSynchronize(stream));
+                    if (h_work > kWideMaxTotal) {
+                        err = "the sparse exact DP would evaluate more than " + std::to_string(h_work) +
+                              " candidate splits (a large biconnected block that is not a cycle; the bound is 2^35, "
+                              "2^24 per set): use IDP";
+                        rc = GPUQO_B200_ERR_TOO_LARGE;
+                        goto done;
+                    }
+                }
+                k_wide_eval<<<grid_for((uint64_t)count * 32), kWideBlock, kEvalSmem, stream>>>(
+                    d_info, t, d_sets, first, count, index_order, d_memo, d_left, d_pairs, d_err);
+                launches++;
+                CKW(cudaGetLastError());
+            }
+            if (count != 1u) {
+                err = "query graph is not connected";
+                rc = GPUQO_B200_ERR_ARGS;
+                goto done;
             }
         } else {
             k_wide_insert<<<grid_for(total), 256, 0, stream>>>(t, d_sets, 0u, total, d_err);
@@ -1434,7 +1564,7 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         goto done;
     }
     nodes.resize((size_t)h_nn);
-    st.connected_sets += total - (uint32_t)n;
+    st.connected_sets += listed - (uint32_t)n;
     st.evaluated_pairs += h_pairs;
     st.memo_bytes = std::max<uint64_t>(st.memo_bytes, bytes);
     st.device_ms += ms;

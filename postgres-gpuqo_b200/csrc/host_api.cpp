@@ -86,6 +86,7 @@ int gpuqo_b200_barrier_poll_limit = 0;
 int gpuqo_b200_device_memory_mb = 0;
 int gpuqo_b200_devices = 1;
 int gpuqo_b200_sparse_from_rels = 32;
+int gpuqo_b200_sparse_host_list = 0;
 }
 
 namespace gqb {

@@ -42,6 +42,7 @@ def knob():
     yield lambda name, v: capi.set_int(L, name, v)
     capi.set_int(L, "gpuqo_b200_sparse_from_rels", 32)
     capi.set_int(L, "gpuqo_b200_device_memory_mb", 0)
+    capi.set_int(L, "gpuqo_b200_sparse_host_list", 0)
 
 
 def _run(q, alg, **kw):
@@ -136,6 +137,79 @@ def _ladder(n_rungs, seed):
     pairs = ([(i, i + 1) for i in range(n_rungs - 1)] + [(n_rungs + i, n_rungs + i + 1) for i in range(n_rungs - 1)] +
              [(i, n_rungs + i) for i in range(n_rungs)])
     return _assemble(f"ladder{n}_s{seed}", n, lrows, [8] * n, _key_edges(pairs, lrows), rng)
+
+
+def _equalized(q, rows):
+    """The same graph with identical relations and identical plain classes:
+    most splits of a set cost exactly the same, so the plan is decided by the
+    tie order alone.  With 100 rows and selectivity 0.01 every join keeps 100
+    rows; with 1000 the estimates overflow to inf and the costs to inf and
+    NaN (the reference's NaN rule decides)."""
+    from gpuqo_b200.query import EqClass, VarInfo
+    q.rows = [float(rows)] * q.n
+    q.tuples = [float(rows)] * q.n
+    q.startup = [0.0] * q.n
+    q.total = [18.0] * q.n
+    q.width = [8] * q.n
+    q.eq_classes = [EqClass(list(e.members), [0.01] * len(e.sels), [[] for _ in e.members],
+                            [VarInfo() for _ in e.members]) for e in q.eq_classes]
+    q.name = f"equal{rows}_" + q.name
+    return q
+
+
+@pytest.mark.parametrize("rows", [100, 1000])
+@pytest.mark.parametrize("alg", [3, 5])
+@pytest.mark.parametrize("make", [lambda: query.key_chain(40, 31), lambda: query.key_cycle(36, 32),
+                                  lambda: query.lollipop(42, 33), lambda: query.ring_path(38, 34)],
+                         ids=["chain40", "cycle36", "lollipop42", "ring_path38"])
+def test_wide_ties_follow_the_reference_order(make, alg, rows):
+    """32 to 63 relations where nearly every split ties: tree path (chain),
+    cycle arcs, blocks joined by bridges; the oracle's plan bit for bit."""
+    q = _equalized(make(), rows)
+    r = _run(q, alg)
+    assert r.error == 0, r.error
+    want, _ = harness.run_port(q, alg)
+    assert same_tree(r.tree, want), (q.name, alg)
+
+
+@pytest.mark.parametrize("alg", [3, 5])
+@pytest.mark.parametrize("case", [c for c in WIDE if c["tag"] in ("wide_key_cycle48_rich", "wide_lollipop63_rich",
+                                                                     "wide_ring_path40", "wide_ring_path36_rich")],
+                         ids=lambda c: c["tag"])
+def test_device_listing_of_general_graphs(case, alg, knob):
+    """Graphs with cycles list their connected sets on the host up to
+    gpuqo_b200_sparse_host_list sets and on the device beyond; with the limit
+    at 1 every level is listed on the device: the oracle's plan bit for bit."""
+    q = case["query"]
+    knob("gpuqo_b200_sparse_host_list", 1)
+    r = _run(q, alg)
+    assert r.error == 0, r.error
+    assert r.stats["connected_sets"] == len_connected_sets(q) - q.n
+    want, _ = harness.run_port(q, alg)
+    assert same_tree(r.tree, want), (q.name, alg)
+
+
+def len_connected_sets(q):
+    adj = [0] * q.n
+    for i, e in enumerate(q.edges):
+        for j in e:
+            adj[i] |= 1 << j
+    cur = {1 << i for i in range(q.n)}
+    total = len(cur)
+    while cur:
+        nxt = set()
+        for S in cur:
+            N, x = 0, S
+            while x:
+                N |= adj[(x & -x).bit_length() - 1]
+                x &= x - 1
+            N &= ~S
+            while N:
+                nxt.add(S | (N & -N))
+                N &= N - 1
+        total += len(nxt)
+        cur = nxt
+    return total
 
 
 def test_tree_path_matches_dense_memo(knob):
