@@ -74,6 +74,10 @@ struct WideInfo {
     // parent in the tree rooted at relation 0
     int edge_masked;
     uint64_t edge_cls[64];
+    // at most 64 classes: rel_cls[v] = the classes with a member v; a split
+    // (L, R) matches the classes in (OR over L) & (OR over R)
+    int rel_masked;
+    uint64_t rel_cls[64];
 };
 constexpr size_t kWideInfoBytes = (sizeof(WideInfo) + 15) & ~size_t(15);
 
@@ -309,8 +313,9 @@ __device__ float ec_selectivity64(const WideInfo &w, int i, uint64_t ec, uint64_
 
 // join_eval_t's general path on 64-bit sets, the classes in class order:
 // every class, or (MASKED) only the classes in cmask, which must hold every
-// class with a member on each side (a tree whose classes all sit on edges:
-// the classes of the split edge)
+// class with a member on each side (the classes of the split edge of a tree
+// whose classes all sit on edges, or the intersection of the sides' class
+// masks)
 template <bool MASKED>
 __device__ RelVal join_eval_w(const WideInfo &w, uint64_t L, const RelVal &l, uint64_t R, const RelVal &r,
                               uint64_t cmask = 0ull) {
@@ -509,7 +514,15 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval(const WideInfo *__rest
             if (index_order) key = dpsub_index64(L, S);
             const RelVal l = wide_rel(memo, wide_lookup(t, L, err), w.h.hz_packed);
             const RelVal r = wide_rel(memo, wide_lookup(t, R, err), w.h.hz_packed);
-            const RelVal out = join_eval_w<false>(w, L, l, R, r);
+            RelVal out;
+            if (w.rel_masked) {
+                uint64_t cl = 0ull, cr = 0ull;
+                for (uint64_t x = L; x; x &= x - 1ull) cl |= w.rel_cls[lowest_idx64(x)];
+                for (uint64_t x = R; x; x &= x - 1ull) cr |= w.rel_cls[lowest_idx64(x)];
+                out = join_eval_w<true>(w, L, l, R, r, cl & cr);
+            } else {
+                out = join_eval_w<false>(w, L, l, R, r);
+            }
             const bool nan = isnan(out.total);
             pairs++;
             if (key < first_k) {
@@ -764,6 +777,12 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_eval_tree(const WideInfo *_
                 const uint64_t cm = w.edge_cls[child0];
                 update(k0, L0, join_eval_w<true>(w, L0, lv, R0, rv, cm));
                 update(k1, R0, join_eval_w<true>(w, R0, rv, L0, lv, cm));
+            } else if (w.rel_masked) {
+                uint64_t cl = 0ull, cr = 0ull;
+                for (uint64_t x = L0; x; x &= x - 1ull) cl |= w.rel_cls[lowest_idx64(x)];
+                for (uint64_t x = R0; x; x &= x - 1ull) cr |= w.rel_cls[lowest_idx64(x)];
+                update(k0, L0, join_eval_w<true>(w, L0, lv, R0, rv, cl & cr));
+                update(k1, R0, join_eval_w<true>(w, R0, rv, L0, lv, cl & cr));
             } else {
                 update(k0, L0, join_eval_w<false>(w, L0, lv, R0, rv));
                 update(k1, R0, join_eval_w<false>(w, R0, rv, L0, lv));
@@ -1301,6 +1320,11 @@ int engine_run_wide(const HostInfo &info, DpMode mode, std::vector<TreeNode> &no
         pe.y = fk_yx ? hw.fksel[x] : (fk_xy ? hw.fksel[y] : sel);
         uint32_t flag = plain ? 1u : 0u;
         std::memcpy(&pe.z, &flag, 4);
+    }
+    if (n_ec <= 64) {
+        hw.rel_masked = 1;
+        for (size_t e = 0; e < n_ec; e++)
+            for (uint64_t m = h_relids[e]; m; m &= m - 1ull) hw.rel_cls[__builtin_ctzll(m)] |= 1ull << e;
     }
     std::vector<uint64_t> t_sub, t_before, t_anc;
     std::vector<uint8_t> t_par;
