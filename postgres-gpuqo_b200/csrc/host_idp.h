@@ -11,7 +11,7 @@
 
 namespace gqb {
 
-// Exact DP of one (remapped, at most 31-relation) sub-problem.
+// Exact DP of one (remapped, at most 63-relation) sub-problem.
 using SubSolver = std::function<int(const HostInfo &, DpMode, std::vector<TreeNode> &, std::string &)>;
 
 // A planning request: BFS relabel, IDP2 / UnionDP (1 < idp_n_iters < n) or one
@@ -30,7 +30,7 @@ void planner_free(PlannerHandle *p);
 // Entry used by gpuqo_run when 1 < gpuqo_idp_n_iters < n_rels, when the
 // query has 64 or more relations, or when gpuqo_spanning_tree_enable is set:
 // the planner on dynamic bitsets (spanning tree, BFS relabel, IDP2 / UnionDP
-// or one exact DP of at most 31 relations).
+// or one exact DP of at most 63 relations).
 QueryTreeC *run_planned(int algorithm, GpuqoPlannerInfoC *info);
 
 void set_error(int code, const std::string &msg);
