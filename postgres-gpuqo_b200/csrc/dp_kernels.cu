@@ -3358,6 +3358,20 @@ struct BatchEngine {
     BatchOvf ovf{};                              // overflow list of kb_dp
     uint64_t cap_ovf = 0;
     void *flush = nullptr;                       // L2 flush buffer (device-resident timing only)
+    // pinned staging of a wave: planner infos and descriptors in, plans and
+    // counters out (grown on demand; the copies are truly asynchronous)
+    unsigned char *h_in = nullptr, *h_out = nullptr;
+    size_t cap_h_in = 0, cap_h_out = 0;
+
+    static int grow_pinned(unsigned char *&p, size_t &cap, size_t bytes, std::string &err) {
+        if (bytes <= cap) return 0;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        CK(cudaMallocHost(&p, bytes));
+        cap = bytes;
+        return 0;
+    }
 
     int init(std::string &err) {
         if (stream) return 0;
@@ -3553,41 +3567,61 @@ struct BatchEngine {
             CK(cudaMalloc(&tree_n, nq * sizeof(int)));
             cap_q = nq;
         }
-        std::vector<uint32_t> hblob(words, 0u);
-        for (int q = 0; q < nq; q++) std::copy(wb[q]->begin(), wb[q]->end(), hblob.begin() + hq[q].blob_off);
-        CK(cudaMemcpyAsync(blobs, hblob.data(), words * 4, cudaMemcpyHostToDevice, stream));
-        CK(cudaMemcpyAsync(qs, hq.data(), nq * sizeof(BatchQ), cudaMemcpyHostToDevice, stream));
+        // stage the planner infos and the descriptors in pinned memory (the
+        // previous wave's copies ended with its synchronisation)
+        const size_t in_blob = (size_t)words * 4, in_q = (size_t)nq * sizeof(BatchQ);
+        if (int rc = grow_pinned(h_in, cap_h_in, in_blob + in_q, err)) return rc;
+        uint32_t *hblob = reinterpret_cast<uint32_t *>(h_in);
+        for (int q = 0; q < nq; q++) {
+            const size_t len = wb[q]->size(), padded = (len + 3) & ~(size_t)3;
+            std::memcpy(hblob + hq[q].blob_off, wb[q]->data(), len * 4);
+            std::memset(hblob + hq[q].blob_off + len, 0, (padded - len) * 4);
+        }
+        std::memcpy(h_in + in_blob, hq.data(), in_q);
+        CK(cudaMemcpyAsync(blobs, hblob, in_blob, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(qs, h_in + in_blob, in_q, cudaMemcpyHostToDevice, stream));
+        // plans and counters come back into pinned memory, with the barrier
+        // words, in one synchronisation
+        const size_t o_tree = 0, o_n = o_tree + (size_t)nq * 64 * sizeof(TreeNode),
+                     o_lvl = (o_n + (size_t)nq * sizeof(int) + 15) & ~(size_t)15,
+                     o_glob = o_lvl + 33 * sizeof(LevelCounters), o_end = o_glob + sizeof(GlobalCounters);
+        if (int rc = grow_pinned(h_out, cap_h_out, o_end, err)) return rc;
+        auto download = [&]() -> int {
+            CK(cudaMemcpyAsync(h_out + o_tree, tree, (size_t)nq * 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(h_out + o_n, tree_n, nq * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(h_out + o_lvl, lvl, 33 * sizeof(LevelCounters), cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(h_out + o_glob, glob, sizeof(GlobalCounters), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            CK(cudaGetLastError());
+            return 0;
+        };
         uint32_t kernels = 1;
         CK(cudaEventRecord(ev0, stream));
         bool persistent = enqueue_persistent(nq, maxn, seen_words, tree_only);
         CK(cudaGetLastError());
-        if (persistent) {
-            CK(cudaMemcpyAsync(h_bar, bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
-            CK(cudaStreamSynchronize(stream));
-            CK(cudaGetLastError());
-            if (h_bar[2] != 0u) {   // barrier timed out: rerun with per-level launches
-                persistent = false;
-                barrier_timed_out = true;   // and use them until gpuqo_b200_reset_persistent
-                st.barrier_timeouts++;
-                CK(cudaEventRecord(ev0, stream));
-            }
-        }
+        if (persistent) CK(cudaMemcpyAsync(h_bar, bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
         if (!persistent) {
             ovf.cap = 0u;
             kernels = enqueue_levels(nq, maxn, seen_words);
         }
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev1, stream));
-        std::vector<TreeNode> htree((size_t)nq * 64);
-        std::vector<int> hn(nq);
-        std::vector<LevelCounters> hl(33);
-        GlobalCounters hg;
-        CK(cudaMemcpyAsync(htree.data(), tree, (size_t)nq * 64 * sizeof(TreeNode), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(hn.data(), tree_n, nq * sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(hl.data(), lvl, 33 * sizeof(LevelCounters), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(&hg, glob, sizeof(GlobalCounters), cudaMemcpyDeviceToHost, stream));
-        CK(cudaStreamSynchronize(stream));
-        CK(cudaGetLastError());
+        if (int rc = download()) return rc;
+        if (persistent && h_bar[2] != 0u) {   // barrier timed out: rerun with per-level launches
+            persistent = false;
+            barrier_timed_out = true;           // and use them until gpuqo_b200_reset_persistent
+            st.barrier_timeouts++;
+            CK(cudaEventRecord(ev0, stream));
+            ovf.cap = 0u;
+            kernels = enqueue_levels(nq, maxn, seen_words);
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(ev1, stream));
+            if (int rc = download()) return rc;
+        }
+        const TreeNode *htree = reinterpret_cast<const TreeNode *>(h_out + o_tree);
+        const int *hn = reinterpret_cast<const int *>(h_out + o_n);
+        const LevelCounters *hl = reinterpret_cast<const LevelCounters *>(h_out + o_lvl);
+        const GlobalCounters &hg = *reinterpret_cast<const GlobalCounters *>(h_out + o_glob);
         float fms = 0.f;
         CK(cudaEventElapsedTime(&fms, ev0, ev1));
         ms = fms;
@@ -3603,7 +3637,7 @@ struct BatchEngine {
                 err = "batched plan extraction produced " + std::to_string(hn[q]) + " nodes";
                 return GPUQO_B200_ERR_CUDA;
             }
-            out[q].assign(htree.begin() + (size_t)q * 64, htree.begin() + (size_t)q * 64 + std::max(hn[q], 0));
+            out[q].assign(htree + (size_t)q * 64, htree + (size_t)q * 64 + std::max(hn[q], 0));
         }
         for (int k = 2; k <= maxn; k++) st.connected_sets += hl[k].n_sets;
         st.evaluated_pairs += hg.evaluated_pairs;
