@@ -389,6 +389,14 @@ int gpuqo_b200_get_tuning(GpuqoB200Tuning *out);
  * NaN crossovers: GPUQO_B200_ERR_ARGS. */
 int gpuqo_b200_set_tuning(const GpuqoB200Tuning *in);
 
+/* Batching window of the planner service's schedulers, in microseconds
+ * (default 100): when sub-problems are pending but some of the lane's running
+ * planners are between two sub-problems, the scheduler waits up to this long
+ * for them before it starts the wave (a wave costs about the same device time
+ * for a few sub-problems as for many).  0 starts every wave at once.  Plans
+ * do not depend on it. */
+extern int gpuqo_b200_server_batch_window_us;
+
 int gpuqo_b200_server_start(int max_inflight, int wave_memory_mb);
 int gpuqo_b200_server_submit(int gpuqo_algorithm, GpuqoPlannerInfoC *info, uint64_t *ticket);
 int gpuqo_b200_server_wait(uint64_t ticket, QueryTreeC **out, double *latency_ms);

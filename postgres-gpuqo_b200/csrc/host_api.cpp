@@ -87,6 +87,7 @@ int gpuqo_b200_device_memory_mb = 0;
 int gpuqo_b200_devices = 1;
 int gpuqo_b200_sparse_from_rels = 32;
 int gpuqo_b200_sparse_host_list = 0;
+int gpuqo_b200_server_batch_window_us = 100;
 }
 
 namespace gqb {

@@ -44,6 +44,8 @@ extern "C" int gpuqo_idp_type;
 extern "C" bool gpuqo_dpsub_bicc_enable;
 extern "C" bool gpuqo_dpsub_ccc_enable;
 
+extern "C" int gpuqo_b200_server_batch_window_us;
+
 namespace gqb {
 
 void set_error(int code, const std::string &msg);
@@ -80,6 +82,7 @@ struct DevLane {
     std::condition_variable cv;
     std::thread th;
     int load = 0;                      // requests given to this lane and not finished
+    int active = 0;                    // of those, planners running (not queued for a slot)
 };
 
 // the lane for a new request: the one with the fewest requests in flight
@@ -164,6 +167,16 @@ public:
                 ln.cv.wait(lk, [&] { return stopping || !pending.empty(); });
                 if (open) starved_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_wait).count();
                 if (stopping && pending.empty()) return;
+                // batching window: planners of this lane that are between two
+                // sub-problems (running, nothing pending) usually submit their
+                // next one within tens of microseconds; a wave costs about the
+                // same device time for a few sub-problems as for many, so wait
+                // up to gpuqo_b200_server_batch_window_us for them
+                if (gpuqo_b200_server_batch_window_us > 0) {
+                    const Clock::time_point until =
+                        Clock::now() + std::chrono::microseconds(gpuqo_b200_server_batch_window_us);
+                    ln.cv.wait_until(lk, until, [&] { return stopping || (int)pending.size() >= ln.active; });
+                }
                 // admit pending sub-problems while the wave's memory fits
                 uint64_t bytes = 0;
                 while (!pending.empty()) {
@@ -223,6 +236,7 @@ public:
     void launch(Request *r) {
         r->started = true;
         running++;
+        lanes[(size_t)r->lane]->active++;
         r->th = std::thread([this, r] {
             cudaSetDevice(lanes[(size_t)r->lane]->device);
             std::string err;
@@ -234,6 +248,8 @@ public:
             r->done = true;
             running--;
             lanes[(size_t)r->lane]->load--;
+            lanes[(size_t)r->lane]->active--;
+            lanes[(size_t)r->lane]->cv.notify_one();   // one planner fewer to wait for
             completed++;
             if (!waiting.empty()) {
                 Request *nx = waiting.front();
