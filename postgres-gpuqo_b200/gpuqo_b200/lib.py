@@ -245,14 +245,21 @@ class Server:
             raise RuntimeError(f"gpuqo_b200_server_submit: {rc}")
         return t.value
 
-    def wait(self, ticket: int):
+    def wait_raw(self, ticket: int):
+        """gpuqo_b200_server_wait as it returns: (status, the QueryTreeC
+        pointer or NULL, latency in ms); the caller frees the tree with
+        gpuqo_b200_free_query_tree."""
         out = C.POINTER(capi.QueryTreeC)()
         lat = C.c_double(0.0)
         rc = self.lib.gpuqo_b200_server_wait(ticket, C.byref(out), C.byref(lat))
+        return rc, out, lat.value
+
+    def wait(self, ticket: int):
+        rc, out, lat = self.wait_raw(ticket)
         tree = capi.tree_to_py(out) if (rc == 0 and out) else None
         if out:
             self.lib.gpuqo_b200_free_query_tree(C.cast(out, C.c_void_p))
-        return rc, tree, lat.value
+        return rc, tree, lat
 
     def cancel(self, ticket: int) -> int:
         """Cancel one request (gpuqo_b200_server_cancel); returns the status."""
