@@ -33,7 +33,8 @@ Printed (rank 0, one JSON line):
            through gpuqo_b200_run_batch against gpuqo_run one query per call,
            queries per second and a bit-for-bit plan comparison;
   served - IDP2 and UnionDP (k=25) snowflake queries of 30..1000 relations
-           arriving as a Poisson stream at 1x and 4x the plain capacity into
+           arriving as a Poisson stream at 1x and 4x the plain capacity
+           (UnionDP also 8x and 16x) into
            the continuous-batching service: queries/s, p50/p99 latency,
            against one-at-a-time gpuqo_run served first-in first-out under
            the same arrivals (a worker thread, measured).
@@ -466,7 +467,8 @@ def served_section(n_req=192, seed=5):
     capi.set_int(L, "gpuqo_idp_n_iters", 25)
     builders = [capi.PlannerInfoBuilder(q) for q in qs]
     out = {"workload": f"{n_req} snowflake queries, relation counts log-uniform in [30,1000], gpuqo_idp_n_iters=25 "
-                       f"over MPDP, Poisson arrivals at 1x and 4x the plain capacity", "by_idp_type": {}}
+                       f"over MPDP, Poisson arrivals at 1x and 4x the plain capacity (UnionDP, which keeps "
+                       f"up with 4x, also at 8x and 16x)", "by_idp_type": {}}
     for idp_type, tag in ((capi.GPUQO_IDP2, "idp2"), (capi.GPUQO_UNION, "union")):
         capi.set_int(L, "gpuqo_idp_type", idp_type)
         r = L.gpuqo_run(capi.GPUQO_DPSUB, builders[0].pointer())   # warm-up
@@ -480,7 +482,7 @@ def served_section(n_req=192, seed=5):
             L.gpuqo_b200_free_query_tree(C.cast(r, C.c_void_p))
         plain_qps = n_req / sum(svc)
         res_t = {"plain_qps": plain_qps, "plain_mean_service_ms": 1e3 * sum(svc) / n_req, "rates": []}
-        for mult in (1.0, 4.0):
+        for mult in ((1.0, 4.0) if tag == "idp2" else (1.0, 4.0, 8.0, 16.0)):
             rate = plain_qps * mult
             arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
             # plain arm, measured: one worker thread takes the requests in
