@@ -1202,7 +1202,10 @@ __device__ __forceinline__ void extract_plan(const float4 *memo, const uint32_t 
 // chosen per query from its connected sets per level, the total over the
 // relation count (Tuning::single_narrow_level_sets,
 // Tuning::single_wide_level_sets)
-template <int MINB>
+// MASKED: every class of the query is a two-member class on a tree edge
+// (DevHeader::ec_masked), a separate kernel so that each carries only the
+// evaluation paths its queries take
+template <int MINB, bool MASKED>
 __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__restrict__ blob, uint32_t blob_words,
                                                        const uint32_t *__restrict__ binom_g, float4 *__restrict__ memo,
                                                        uint32_t *__restrict__ memo_left, uint32_t *__restrict__ setsA,
@@ -1225,7 +1228,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
     uint32_t *st = stage + warp * 64;
     const uint32_t gwarp = blockIdx.x * kWarpsPerBlock + warp;
     const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
-    const bool masked = d.h->ec_masked != 0u;
     unsigned long long pairs = 0;
     unsigned epoch = 0;   // grid barriers passed (thread 0)
     // the pipelined candidate loop needs the registers of the 2- and 3-blocks
@@ -1253,14 +1255,11 @@ __global__ void __launch_bounds__(kBlock, MINB) k_dp_tree(const uint32_t *__rest
         while (G < max_group && (uint64_t)count * (uint64_t)G < (uint64_t)target_lanes) G <<= 1;
         G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
         if (G == 2) {
-            if (masked) tree_groups<2, true, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
-            else tree_groups<2, false, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
+            tree_groups<2, MASKED, kPipe>(d, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs);
         } else if (G == 8) {
-            if (masked) tree_groups<8, true, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
-            else tree_groups<8, false, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
+            tree_groups<8, MASKED, kPipe>(d, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs);
         } else {
-            if (masked) tree_groups<32, true, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
-            else tree_groups<32, false, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
+            tree_groups<32, MASKED, kPipe>(d, gwarp, nwarps, cur, count, k, memo, memo_left, pairs);
         }
         if (!grid_barrier<true>(bar, epoch, max_polls)) return;
     }
@@ -2033,10 +2032,14 @@ public:
             const Tuning &tu = g_tuning[device];
             minb = per_level <= tu.single_narrow_level_sets ? 2 : (per_level > tu.single_wide_level_sets ? 4 : 3);
         }
-        const void *fn = minb == 4   ? (const void *)k_dp_tree<4>
-                         : minb == 2 ? (const void *)k_dp_tree<2>
-                                     : (const void *)k_dp_tree<3>;
-        const size_t key = smem * 8u + (size_t)minb;
+        const bool masked = reinterpret_cast<const DevHeader *>(h_blob)->ec_masked != 0u;
+        const void *fn = masked ? (minb == 4   ? (const void *)k_dp_tree<4, true>
+                                   : minb == 2 ? (const void *)k_dp_tree<2, true>
+                                               : (const void *)k_dp_tree<3, true>)
+                                : (minb == 4   ? (const void *)k_dp_tree<4, false>
+                                   : minb == 2 ? (const void *)k_dp_tree<2, false>
+                                               : (const void *)k_dp_tree<3, false>);
+        const size_t key = smem * 16u + (size_t)minb * 2u + (masked ? 1u : 0u);
         auto cb = coop_blocks.find(key);
         if (cb == coop_blocks.end()) {
             int blocks = 0, dev_coop = 0, occ = 0;
