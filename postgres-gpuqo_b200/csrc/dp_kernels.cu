@@ -2891,7 +2891,10 @@ __device__ __forceinline__ void tree_cand(const DevHeader &h, uint32_t S, int a,
     }
 }
 
-template <int G, bool TREE_ONLY>
+// ALL_MASKED (with TREE_ONLY): every query of the wave has only two-member
+// classes on tree edges (DevHeader::ec_masked), so the general class pass
+// is not compiled in
+template <int G, bool TREE_ONLY, bool ALL_MASKED = false>
 __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *blobs, uint32_t first, uint32_t stride,
                                              const unsigned long long *items, uint32_t count, int k, float4 *memo_all,
                                              uint32_t *memo_left_all, unsigned long long &pairs,
@@ -2915,7 +2918,7 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
         float4 *memo = memo_all + Q.memo_off;
         uint32_t *memo_left = memo_left_all + Q.memo_off;
         const bool tree = has && (TREE_ONLY || h.tree_mode != 0u);
-        const bool masked = tree && h.ec_masked != 0u;
+        const bool masked = ALL_MASKED || (tree && h.ec_masked != 0u);
         uint32_t P = 0;
         B.nb = 0;
         if (has) {
@@ -2971,7 +2974,8 @@ __device__ __forceinline__ void batch_groups(const BatchQ *qs, const uint32_t *b
             }
             if (valid) {
                 RelVal l = load_rel(memo, L, d.h->hz_packed), r = load_rel(memo, R, d.h->hz_packed);
-                RelVal out = masked ? join_eval_t<true>(d, L, l, R, r, ecm) : join_eval_t<false>(d, L, l, R, r, 0u);
+                RelVal out = (ALL_MASKED || masked) ? join_eval_t<true>(d, L, l, R, r, ecm)
+                                                    : join_eval_t<false>(d, L, l, R, r, 0u);
                 best_update(best, p, L, out);
             }
         }
@@ -3171,7 +3175,7 @@ __global__ void kb_extract(const BatchQ *__restrict__ qs, int nq, const uint32_t
 // extracted (one thread per query) after the last level.  The grid barrier
 // is bounded (grid_barrier); on timeout the host reruns the wave with
 // per-level launches.
-template <bool TREE_ONLY>
+template <bool TREE_ONLY, bool ALL_MASKED = false>
 __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ *__restrict__ qs, int nq, int maxn,
                                                    const uint32_t *__restrict__ blobs, float4 *__restrict__ memo,
                                                    uint32_t *__restrict__ memo_left, uint32_t *__restrict__ seen,
@@ -3236,11 +3240,14 @@ __global__ void __launch_bounds__(kBlock, TREE_ONLY ? 3 : 2) kb_dp(const BatchQ 
         G = G <= 2 ? 2 : (G <= 8 ? 8 : 32);
         LevelCounters *lk = lvl + k;
         if (G == 2)
-            batch_groups<2, TREE_ONLY>(qs, blobs, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left, pairs, ovf, lk);
+            batch_groups<2, TREE_ONLY, ALL_MASKED>(qs, blobs, gwarp * 16, nwarps * 16, cur, count, k, memo, memo_left,
+                                                   pairs, ovf, lk);
         else if (G == 8)
-            batch_groups<8, TREE_ONLY>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left, pairs, ovf, lk);
+            batch_groups<8, TREE_ONLY, ALL_MASKED>(qs, blobs, gwarp * 4, nwarps * 4, cur, count, k, memo, memo_left,
+                                                   pairs, ovf, lk);
         else
-            batch_groups<32, TREE_ONLY>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs, ovf, lk);
+            batch_groups<32, TREE_ONLY, ALL_MASKED>(qs, blobs, gwarp, nwarps, cur, count, k, memo, memo_left, pairs,
+                                                    ovf, lk);
         if (!grid_barrier<false>(bar, epoch, max_polls)) return;
         if (TREE_ONLY) continue;   // tree sets have 2(k - 1) candidates: never an overflow
         // overflow sets of level k: the counter is final after the barrier, so
@@ -3357,6 +3364,7 @@ struct BatchEngine {
     unsigned *bar = nullptr, *h_bar = nullptr;   // grid barrier words of kb_dp (device, pinned copy)
     int coop_grid = -1;                          // co-resident blocks of kb_dp<false> (0: no cooperative launch)
     int coop_grid_tree = -1;                     // co-resident blocks of kb_dp<true>
+    int coop_grid_masked = -1;                   // co-resident blocks of kb_dp<true, true>
     bool barrier_timed_out = false;              // a grid barrier of kb_dp gave up: per-level launches until reset
     BatchOvf ovf{};                              // overflow list of kb_dp
     uint64_t cap_ovf = 0;
@@ -3387,13 +3395,15 @@ struct BatchEngine {
         CK(cudaMalloc(&glob, sizeof(GlobalCounters)));
         CK(cudaMalloc(&bar, 4 * sizeof(unsigned)));
         CK(cudaMallocHost(&h_bar, 4 * sizeof(unsigned)));
-        int dev_coop = 0, occ = 0, occ_tree = 0;
+        int dev_coop = 0, occ = 0, occ_tree = 0, occ_masked = 0;
         cudaDeviceGetAttribute(&dev_coop, cudaDevAttrCooperativeLaunch, device);
-        coop_grid = coop_grid_tree = 0;
+        coop_grid = coop_grid_tree = coop_grid_masked = 0;
         if (dev_coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb_dp<false>, kBlock, 0) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tree, kb_dp<true>, kBlock, 0) == cudaSuccess) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_tree, kb_dp<true>, kBlock, 0) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_masked, kb_dp<true, true>, kBlock, 0) == cudaSuccess) {
             coop_grid = occ * sm_count;
             coop_grid_tree = occ_tree * sm_count;
+            coop_grid_masked = occ_masked * sm_count;
         }
         cudaGetLastError();
         return 0;
@@ -3422,9 +3432,11 @@ struct BatchEngine {
     }
 
     // the wave as one cooperative launch of kb_dp (kb_dp<true> when every query
-    // is tree-shaped); false when it could not start
-    bool enqueue_persistent(int nq, int maxn, uint64_t seen_words, bool tree_only) {
-        const int grid = tree_only ? coop_grid_tree : coop_grid;
+    // is tree-shaped, kb_dp<true, true> when every class of every query is also
+    // a two-member class on a tree edge); false when it could not start
+    bool enqueue_persistent(int nq, int maxn, uint64_t seen_words, bool tree_only, bool all_masked) {
+        const bool masked = tree_only && all_masked;
+        const int grid = masked ? coop_grid_masked : (tree_only ? coop_grid_tree : coop_grid);
         if (grid <= 0 || gpuqo_b200_persistent == 0 || barrier_timed_out) return false;
         cudaMemsetAsync(lvl, 0, 33 * sizeof(LevelCounters), stream);
         cudaMemsetAsync(glob, 0, sizeof(GlobalCounters), stream);
@@ -3434,10 +3446,11 @@ struct BatchEngine {
         unsigned poll_limit = (unsigned)std::max(0, gpuqo_b200_barrier_poll_limit);
         void *args[] = {&qs, &nq, &maxn, &blobs, &memo, &memo_left, &seen, &listA, &listB,
                         &lvl, &glob, &tree, &tree_n, &bar, &target_lanes, &ovf, &poll_limit};
-        const void *fn = tree_only ? (const void *)kb_dp<true> : (const void *)kb_dp<false>;
+        const void *fn = masked ? (const void *)kb_dp<true, true>
+                                : (tree_only ? (const void *)kb_dp<true> : (const void *)kb_dp<false>);
         if (cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, stream) != cudaSuccess) {
             cudaGetLastError();
-            coop_grid = coop_grid_tree = 0;
+            coop_grid = coop_grid_tree = coop_grid_masked = 0;
             return false;
         }
         return true;
@@ -3513,7 +3526,7 @@ struct BatchEngine {
         std::vector<BatchQ> hq(nq);
         uint64_t slots = 0, words = 0, seen_words = 0, items = 0, base = 0, ovf_need = 0;
         int maxn = 0;
-        bool tree_only = true;
+        bool tree_only = true, all_masked = true;
         for (int q = 0; q < nq; q++) {
             const DevHeader *h = reinterpret_cast<const DevHeader *>(wb[q]->data());
             const int n = h->n;
@@ -3530,6 +3543,7 @@ struct BatchEngine {
             maxn = std::max(maxn, n);
             if (batch_needs_ovf(*wb[q])) ovf_need += max_level_sets(n);
             tree_only = tree_only && h->tree_mode != 0u;
+            all_masked = all_masked && h->ec_masked != 0u;
         }
         items = std::max(items, base);
         ovf_need = std::min(ovf_need, kBatchOvfCap);
@@ -3600,7 +3614,7 @@ struct BatchEngine {
         };
         uint32_t kernels = 1;
         CK(cudaEventRecord(ev0, stream));
-        bool persistent = enqueue_persistent(nq, maxn, seen_words, tree_only);
+        bool persistent = enqueue_persistent(nq, maxn, seen_words, tree_only, all_masked);
         CK(cudaGetLastError());
         if (persistent) CK(cudaMemcpyAsync(h_bar, bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
         if (!persistent) {
