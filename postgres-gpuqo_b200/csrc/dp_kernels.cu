@@ -3899,8 +3899,10 @@ int engine_autotune(const std::vector<std::vector<uint32_t>> &blobs, double &sin
         }
         sets.push_back(cs);
         level_sets.push_back(cs / h->n);
-        narrow_wins.push_back(t[0] < t[1]);
-        wide_wins.push_back(t[2] < t[1]);
+        // each variant against the best of the other two, so that the
+        // crossovers give the fastest of the three at every measured size
+        narrow_wins.push_back(t[0] < std::min(t[1], t[2]));
+        wide_wins.push_back(t[2] < std::min(t[0], t[1]));
         single_wins.push_back(std::min(t[0], std::min(t[1], t[2])) < wms / m);
     }
     single_narrow_level_sets = crossover_below(level_sets, narrow_wins);

@@ -35,6 +35,12 @@ class Stats(C.Structure):
 
 _lib = None
 
+# GUC variables whose values load() records as the library was loaded, before
+# any caller changed them (boot_gucs)
+_BOOT_INTS = ("gpuqo_n_parallel", "gpuqo_dpsub_filter_threshold", "gpuqo_idp_type", "gpuqo_idp_n_iters")
+_BOOT_BOOLS = ("gpuqo_dpsub_ccc_enable", "gpuqo_dpsub_bicc_enable", "gpuqo_dpsub_csg_enable")
+boot_gucs = {}
+
 
 def load():
     """Load the product library (raises OSError when it has not been built)."""
@@ -43,6 +49,10 @@ def load():
         if not os.path.exists(LIB_PATH):
             raise OSError(f"{LIB_PATH} is missing; build it with `make -C postgres-gpuqo_b200`")
         lib = C.CDLL(LIB_PATH, mode=C.RTLD_LOCAL)
+        for name in _BOOT_INTS:
+            boot_gucs[name] = C.c_int.in_dll(lib, name).value
+        for name in _BOOT_BOOLS:
+            boot_gucs[name] = C.c_bool.in_dll(lib, name).value
         capi.bind_gpuqo_run(lib)
         lib.gpuqo_b200_free_query_tree.argtypes = [C.c_void_p]
         lib.gpuqo_b200_free_query_tree.restype = None

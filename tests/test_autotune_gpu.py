@@ -21,11 +21,15 @@ def _plans():
 
 def test_autotune_installs_crossovers_without_changing_plans():
     before = _plans()
-    t = lib.autotune()
-    assert t["tuned"] == 1 and t["tune_ms"] > 0.0
-    for k in ("single_narrow_level_sets", "single_wide_level_sets", "batch_single_sets"):
-        assert t[k] >= 0.0
-    assert lib.get_tuning() == t
-    after = _plans()
-    for a, b in zip(before[0] + before[1], after[0] + after[1]):
-        assert same_tree(a, b)
+    try:
+        t = lib.autotune()
+        assert t["tuned"] == 1 and t["tune_ms"] > 0.0
+        for k in ("single_narrow_level_sets", "single_wide_level_sets", "batch_single_sets"):
+            assert t[k] >= 0.0
+        assert lib.get_tuning() == t
+        after = _plans()
+        for a, b in zip(before[0] + before[1], after[0] + after[1]):
+            assert same_tree(a, b)
+    finally:
+        # the built-in crossovers again, for the tests after this one
+        lib.set_tuning(16384.0, 1e30, float(1 << 20), tuned=0)

@@ -18,13 +18,19 @@ def test_library_exports_declared_symbols():
 
 
 def test_guc_boot_values():
-    l = lib.load()
-    # boot values of src/backend/utils/misc/guc.c
-    assert capi.get_int(l, "gpuqo_n_parallel") == 10240
-    assert capi.get_int(l, "gpuqo_dpsub_filter_threshold") == 16
-    assert capi.get_int(l, "gpuqo_idp_type") == capi.GPUQO_IDP2
-    assert C.c_bool.in_dll(l, "gpuqo_dpsub_ccc_enable").value is True
-    assert C.c_bool.in_dll(l, "gpuqo_dpsub_bicc_enable").value is False
+    """The values the library's GUC variables hold as it is loaded (recorded
+    by lib.load(), so that tests run before this one in the same process and
+    changing them do not matter): the boot values of
+    src/backend/utils/misc/guc.c."""
+    lib.load()
+    b = lib.boot_gucs
+    assert b["gpuqo_n_parallel"] == 10240
+    assert b["gpuqo_dpsub_filter_threshold"] == 16
+    assert b["gpuqo_idp_type"] == capi.GPUQO_IDP2
+    assert b["gpuqo_idp_n_iters"] == 0
+    assert b["gpuqo_dpsub_ccc_enable"] is True
+    assert b["gpuqo_dpsub_bicc_enable"] is False
+    assert b["gpuqo_dpsub_csg_enable"] is True
 
 
 def test_struct_layouts_match_reference():
